@@ -1,0 +1,229 @@
+/*
+ * shinobi_b200 -- C ABI of the B200-native (sm_100a) grid ray-tracing path:
+ * sort-based uniform and two-level grid construction, 3D-DDA traversal with a
+ * watertight ray/triangle test, camera / ambient-occlusion ray generation and
+ * the wavefront path tracer with stream compaction.
+ *
+ * Conventions
+ *  - every call returns shn_status; shn_ctx_last_error() gives a message;
+ *  - pointers named d_* are device pointers owned by the caller; objects
+ *    created by shn_*_create are owned by the library and released by the
+ *    matching shn_*_destroy;
+ *  - "stream" is a cudaStream_t (NULL = legacy default stream); all work of a
+ *    call is ordered on it and calls return without synchronising unless a
+ *    size must come back to the host (documented per call);
+ *  - no global textures or __constant__ state: several grids and scenes may
+ *    be alive and used concurrently from different streams; a ctx serialises
+ *    its own bookkeeping with an internal lock.
+ *
+ * Reference interfaces replaced (jckarter/shinobi, paths within that tree):
+ *  - FaceSoup<frame>::upload / uploadVertices      -> shn_scene_create / shn_scene_update_vertices
+ *      (src/Control/Structure/FaceSoup.h:171-339)
+ *  - FastSimpleGridBuilder::init/build/rebuild     -> shn_grid_build (SHN_GRID_UNIFORM)
+ *      (src/Control/Algorithm/FastSimpleGridBuilder.h:59-452)
+ *  - FastTwoLevelGridBuilder::init/build/rebuild   -> shn_grid_build (SHN_GRID_TWO_LEVEL)
+ *      (src/Control/Algorithm/FastTwoLevelGridBuilder.h:61-740)
+ *  - UniformGridTraverser / TwoLevelGridTraverser  -> shn_trace_closest
+ *      (src/Control/Algorithm/SimpleGridTraverser.h:274-401,
+ *       src/Control/Algorithm/TwoLevelGridTraverser.h:445-671)
+ *  - *ShadowTraverser                               -> shn_trace_any
+ *      (src/Control/Algorithm/SimpleGridTraverser.h:405-469,
+ *       src/Control/Algorithm/TwoLevelGridTraverser.h:677-828)
+ *  - trace<RegularPrimaryRayGenerator,...>          -> shn_trace_primary
+ *      (src/Engine/RayTracingKernels.h:37-136, src/Engine/RayGenerators.h:36-61)
+ *  - DirectIlluminationIntegrator::shade occlusion  -> shn_trace_ao
+ *      (src/Integrator/DirectIlluminationIntegrator.h:254-315)
+ *  - SimplePathTracer / render megakernel           -> shn_pt_render
+ *      (src/Integrator/SimplePathTracer.hpp:65-241, src/Shinobi.h:152-230)
+ *  - InclusiveScan / ExclusiveScan / Sort           -> shn_exclusive_scan_u32 / shn_sort_keys_u64
+ *      (src/Utils/Scan.h:35-68, src/Utils/Sort.h:33-48)
+ *  - chag::pp::compact (present, unused by the ref) -> shn_compact_u32
+ *      (src/Utils/chag/pp/compact.cuh:52-90)
+ */
+#ifndef SHINOBI_B200_H
+#define SHINOBI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SHN_ABI_VERSION 1u
+#define SHN_MISS 0xFFFFFFFFu
+
+typedef enum shn_status {
+  SHN_OK = 0,
+  SHN_ERR_INVALID = 1,      /* bad argument, size beyond a stated maximum, non-finite input */
+  SHN_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+  SHN_ERR_OOM = 3,          /* device allocation failed */
+  SHN_ERR_TIMEOUT = 4,      /* a bounded device-side wait gave up (result is not valid) */
+  SHN_ERR_BUDGET = 5,       /* the context's HBM budget would be exceeded */
+  SHN_ERR_NOT_BUILT = 6,    /* grid used before a successful build */
+  SHN_ERR_BUSY = 7,         /* server queue full / request not finished */
+  SHN_ERR_CANCELLED = 8     /* server request cancelled */
+} shn_status;
+
+typedef struct shn_ctx shn_ctx;
+typedef struct shn_scene shn_scene;
+typedef struct shn_grid shn_grid;
+
+/* ---- context -------------------------------------------------------------
+ * One per device.  hbm_budget_bytes = 0 means no limit.  Device memory of
+ * scenes, grids and build workspaces comes from a stream-ordered pool that
+ * the context owns. */
+shn_status shn_ctx_create(int device, uint64_t hbm_budget_bytes, shn_ctx** out);
+void shn_ctx_destroy(shn_ctx* ctx);
+const char* shn_status_string(shn_status s);
+const char* shn_ctx_last_error(const shn_ctx* ctx);
+shn_status shn_ctx_memory(const shn_ctx* ctx, uint64_t* used_bytes, uint64_t* budget_bytes);
+uint32_t shn_abi_version(void);
+
+/* ---- scene (FaceSoup) ----------------------------------------------------- */
+#define SHN_MEM_HOST 0u
+#define SHN_MEM_DEVICE 1u
+/* vtx_xyz: nv float xyz triples; idx: nt uint32 index triples.  mem says
+ * whether both pointers are host or device memory.  Host input is validated
+ * (finite vertices, indices < nv); device input is copied as is.  Blocks
+ * until the bounds are known on the host (one small read-back for device
+ * input). */
+shn_status shn_scene_create(shn_ctx* ctx, const float* vtx_xyz, uint32_t nv, const uint32_t* idx,
+                            uint32_t nt, uint32_t mem, void* stream, shn_scene** out);
+/* Replace vertex positions (same counts); recomputes bounds. */
+shn_status shn_scene_update_vertices(shn_scene* s, const float* vtx_xyz, uint32_t nv, uint32_t mem,
+                                     void* stream);
+shn_status shn_scene_bounds(const shn_scene* s, float out_min_max[6]);
+uint32_t shn_scene_num_triangles(const shn_scene* s);
+void shn_scene_destroy(shn_scene* s);
+
+/* ---- grid build ------------------------------------------------------------ */
+#define SHN_GRID_UNIFORM 0u
+#define SHN_GRID_TWO_LEVEL 1u
+
+typedef struct shn_grid_params {
+  uint32_t kind;            /* SHN_GRID_UNIFORM or SHN_GRID_TWO_LEVEL */
+  float lambda;             /* cells per triangle of the (top) grid: res = diag*cbrt(lambda*N/V) */
+  int32_t top_divisor;      /* integer divisor applied to that resolution (reference two-level: 6) */
+  int32_t min_res;          /* lower clamp per axis after the divisor (reference two-level: 2) */
+  float lambda_leaf;        /* two-level: leaf cells per reference in a top cell (reference: 1.2) */
+  uint32_t leaf_threshold;  /* two-level: top cells with <= this many references stay one leaf (16) */
+  int32_t res[3];           /* if all > 0: use this resolution instead of the lambda rule */
+} shn_grid_params;
+
+/* Reference defaults: uniform lambda=5; two-level lambda=5, divisor 6, min 2,
+ * lambda_leaf 1.2, threshold 16 (src/Control/Algorithm/GridBuilder.h:48,
+ * src/Control/Algorithm/FastTwoLevelGridBuilder.h:87-102,
+ * src/Control/Algorithm/TwoLevelBuildKernels.h:49,73). */
+void shn_grid_params_default(uint32_t kind, shn_grid_params* p);
+
+typedef struct shn_grid_info {
+  uint32_t kind;
+  int32_t res[3];
+  float bounds[6];
+  float cell_size[3];
+  uint64_t num_cells;      /* uniform cells, or top cells */
+  uint64_t num_top_refs;   /* two-level: (top cell, tri) pairs */
+  uint64_t num_leaves;     /* two-level: leaf cells */
+  uint64_t num_refs;       /* entries of indices[] (the reference array) */
+  uint64_t device_bytes;   /* grid-owned device memory */
+  float build_ms;          /* device time of the last build (CUDA events) */
+} shn_grid_info;
+
+shn_status shn_grid_create(shn_ctx* ctx, shn_grid** out);
+/* Builds (or rebuilds) the grid over the scene on stream.  Synchronises the
+ * stream up to twice (uniform) / four times (two-level) to size buffers from
+ * device-side counts, as the reference does. */
+shn_status shn_grid_build(shn_grid* g, const shn_scene* s, const shn_grid_params* p, void* stream);
+shn_status shn_grid_get_info(const shn_grid* g, shn_grid_info* out);
+/* Copies the grid to host buffers (any may be NULL): cells = 2*num_cells
+ * uint32 (uniform: [begin,end) ranges; two-level: cell words in the
+ * TwoLevelGridCell layout), leaves = 2*num_leaves, indices = num_refs,
+ * top_pairs = num_top_refs sorted (cell<<32 | tri) keys (two-level) or
+ * num_refs (uniform).  Synchronises. */
+shn_status shn_grid_export(const shn_grid* g, uint32_t* cells, uint32_t* leaves, uint32_t* indices,
+                           uint64_t* top_pairs);
+void shn_grid_destroy(shn_grid* g);
+
+/* ---- traversal -------------------------------------------------------------- */
+typedef struct shn_rays {
+  const float *ox, *oy, *oz;  /* device SoA origins */
+  const float *dx, *dy, *dz;  /* device SoA directions (need not be unit length) */
+  const float* tmax;          /* device; NULL = FLT_MAX */
+} shn_rays;
+
+typedef struct shn_hits {
+  uint32_t* tri;  /* device; SHN_MISS when nothing was hit */
+  float* t;       /* device; tmax when nothing was hit */
+  float* u;       /* device, may be NULL: barycentric weight of vertex 1 */
+  float* v;       /* device, may be NULL: barycentric weight of vertex 2 */
+} shn_hits;
+
+/* Closest hit with t in (1e-5, tmax). */
+shn_status shn_trace_closest(const shn_grid* g, const shn_rays* rays, uint32_t n, shn_hits* hits,
+                             void* stream);
+/* Any hit with t in (1e-5, tmax): occluded[i] = 1 if blocked, else 0. */
+shn_status shn_trace_any(const shn_grid* g, const shn_rays* rays, uint32_t n, uint8_t* d_occluded,
+                         void* stream);
+
+typedef struct shn_camera {
+  float eye[3], forward[3], up[3];
+  float fov_deg;            /* vertical opening angle */
+  uint32_t res_x, res_y;
+} shn_camera;
+
+/* Pinhole primary rays (Camera + RegularPixelSampler<1,1>, generated in the
+ * kernel) traced for closest hit; hits are pixel-major (res_x*res_y). */
+shn_status shn_trace_primary(const shn_grid* g, const shn_camera* cam, uint32_t image_id,
+                             shn_hits* hits, void* stream);
+
+/* Ambient occlusion from primary hits: spp cosine-distributed any-hit rays
+ * of length `length` per hit pixel, origin offset `offset` along the facing
+ * normal, Philox4x32-10 stream (pixel, sample) keyed by seed.  d_ao[p] =
+ * fraction of unoccluded samples (1 for pixels without a primary hit).
+ * If d_num_rays != NULL it receives the number of AO rays traced (device). */
+shn_status shn_trace_ao(const shn_grid* g, const shn_camera* cam, const shn_hits* primary,
+                        uint32_t spp, float length, float offset, uint32_t seed, float* d_ao,
+                        uint32_t* d_num_rays, void* stream);
+
+/* ---- path tracer --------------------------------------------------------------- */
+typedef struct shn_pt_params {
+  uint32_t spp;              /* samples per pixel */
+  uint32_t max_depth;        /* bounces (path segments) per sample */
+  uint32_t rr_depth;         /* Russian roulette from this depth on */
+  float albedo;              /* diffuse albedo of every surface */
+  float light_pos[3];        /* area light: corner, two edges, emitted radiance */
+  float light_e1[3];
+  float light_e2[3];
+  float light_radiance[3];
+  float background[3];
+  float offset;              /* ray origin offset along the normal */
+  uint32_t seed;
+} shn_pt_params;
+
+void shn_pt_params_default(shn_pt_params* p);
+/* Wavefront path tracer: camera rays -> extend -> shade/next-event -> compact
+ * after each bounce.  d_image: res_x*res_y*3 floats (mean radiance).  If
+ * d_stats != NULL it receives per-bounce live-path counts (max_depth+1 uint32). */
+shn_status shn_pt_render(const shn_grid* g, const shn_scene* s, const shn_camera* cam,
+                         const shn_pt_params* p, float* d_image, uint32_t* d_stats, void* stream);
+
+/* ---- parallel primitives ------------------------------------------------------- */
+/* d_out[0..n] = exclusive prefix sums of d_in[0..n-1], d_out[n] = total.
+ * Single-pass decoupled look-back.  n < 2^31. */
+shn_status shn_exclusive_scan_u32(shn_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t n,
+                                  void* stream);
+/* Stable compaction: d_out_idx[0..m) = indices i with d_flags[i] != 0, in
+ * order; *d_count = m (device). */
+shn_status shn_compact_u32(shn_ctx* ctx, const uint32_t* d_flags, uint32_t n, uint32_t* d_out_idx,
+                           uint32_t* d_count, void* stream);
+/* Stable LSD radix sort of 64-bit keys on bits [lo_bit, hi_bit) (8-bit
+ * digits, one onesweep pass per digit).  d_tmp has n entries; the sorted
+ * keys end in d_keys.  n < 2^30. */
+shn_status shn_sort_keys_u64(shn_ctx* ctx, uint64_t* d_keys, uint64_t* d_tmp, uint32_t n,
+                             uint32_t lo_bit, uint32_t hi_bit, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SHINOBI_B200_H */

@@ -1,0 +1,274 @@
+"""Oracle (test infrastructure only).
+
+Python bindings for ``liboracle.so`` -- the CPU restatement of Shinobi's
+grid build, DDA traversal and ray generation -- and for ``_ref/`` -- the
+reference's own host-compilable code compiled in place.  Only ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` import
+this package; the product never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libshinobi_ref.so")
+MISS = 0xFFFFFFFF
+
+_lib = None
+_ref = None
+
+
+def build(force: bool = False) -> None:
+    """Compile the oracle (and the reference checker when its tree is present)."""
+    args = ["make", "-C", HERE]
+    if force:
+        args.insert(1, "-B")
+    subprocess.run(args, check=True, stdout=subprocess.DEVNULL)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _u32(a):
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(os.path.join(HERE, "oracle.cpp")):
+            build()
+        L = C.CDLL(LIB)
+        vp, u32, i32, f32 = C.c_void_p, C.c_uint32, C.c_int, C.c_float
+        L.orc_bounds.argtypes = [vp, vp, u32, vp]
+        L.orc_resolution.argtypes = [u32, vp, f32, i32, i32, vp]
+        L.orc_build_uniform.argtypes = [vp, u32, vp, u32, vp, vp]
+        L.orc_build_uniform.restype = vp
+        L.orc_build_two_level.argtypes = [vp, u32, vp, u32, vp, vp, f32, u32]
+        L.orc_build_two_level.restype = vp
+        L.orc_grid_free.argtypes = [vp]
+        L.orc_grid_info.argtypes = [vp, vp]
+        for nm in ("orc_grid_cells", "orc_grid_leaves", "orc_grid_indices", "orc_grid_top_pairs"):
+            getattr(L, nm).argtypes = [vp]
+            getattr(L, nm).restype = vp
+        L.orc_num_threads.restype = i32
+        L.orc_set_threads.argtypes = [i32]
+        L.orc_trace_closest.argtypes = [vp] + [vp] * 7 + [u32] + [vp] * 5
+        L.orc_trace_any.argtypes = [vp] + [vp] * 7 + [u32, vp, vp]
+        L.orc_trace_brute.argtypes = [vp, vp, u32] + [vp] * 6 + [u32, vp, vp]
+        L.orc_t_fp64.argtypes = [vp, vp, vp] + [vp] * 6 + [u32, vp]
+        L.orc_sincos_2pi.argtypes = [vp, u32, vp, vp]
+        L.orc_philox.argtypes = [vp, u32, u32, u32, vp]
+        L.orc_camera.argtypes = [vp, vp, vp, f32, u32, u32, vp]
+        L.orc_primary_rays.argtypes = [vp, u32, u32, u32, vp, vp, vp]
+        L.orc_ao_rays.argtypes = [vp, vp] + [vp] * 8 + [u32, u32, u32, f32] + [vp] * 7
+        L.orc_ao_rays.restype = u32
+        L.orc_compact.argtypes = [vp, u32, vp]
+        L.orc_compact.restype = u32
+        _lib = L
+    return _lib
+
+
+def ref_lib():
+    """The reference's own code compiled in place, or None when it was not built here."""
+    global _ref
+    if _ref is None and os.path.exists(REF_LIB):
+        R = C.CDLL(REF_LIB)
+        vp, u32, i32, f32 = C.c_void_p, C.c_uint32, C.c_int, C.c_float
+        R.ref_host_build.argtypes = [vp, u32, vp, u32, i32, i32, i32, vp, vp]
+        R.ref_host_build.restype = vp
+        R.ref_host_build_copy.argtypes = [vp, vp, vp, vp]
+        R.ref_host_build_free.argtypes = [vp]
+        R.ref_camera.argtypes = [vp, vp, vp, f32, u32, u32, vp]
+        R.ref_primary_dirs.argtypes = [vp, u32, u32, u32, vp, u32, vp]
+        R.ref_mt_closest.argtypes = [vp, vp, u32, vp, vp, u32, vp, vp]
+        R.ref_cosine_sample.argtypes = [vp, vp, u32, vp]
+        R.ref_cell_word.argtypes = [u32, u32, u32, i32, u32, vp]
+        _ref = R
+    return _ref
+
+
+def bounds(vtx, idx) -> np.ndarray:
+    vtx, idx = _f32(vtx), _u32(idx)
+    out = np.zeros(6, np.float32)
+    lib().orc_bounds(_p(vtx), _p(idx), idx.shape[0], _p(out))
+    return out
+
+
+def resolution(nt: int, b, lam: float, divisor: int = 1, min_res: int = 1) -> np.ndarray:
+    b = _f32(b)
+    out = np.zeros(3, np.int32)
+    lib().orc_resolution(nt, _p(b), lam, divisor, min_res, _p(out))
+    return out
+
+
+@dataclass
+class Grid:
+    kind: int
+    res: np.ndarray
+    bounds: np.ndarray
+    cells: np.ndarray       # (C, 2) uint32: ranges (uniform) or cell words (two-level)
+    leaves: np.ndarray      # (L, 2) uint32 (two-level)
+    indices: np.ndarray     # (K,) uint32
+    top_pairs: np.ndarray   # sorted (cell<<32 | tri) uint64
+    handle: object = None
+
+    def __del__(self):
+        if self.handle:
+            lib().orc_grid_free(self.handle)
+            self.handle = None
+
+
+def _wrap(h, kind, res, b) -> Grid:
+    L = lib()
+    info = np.zeros(8, np.uint64)
+    L.orc_grid_info(h, _p(info))
+    nc, nk, nl, ntp = int(info[1]), int(info[2]), int(info[3]), int(info[4])
+
+    def arr(ptr, n, dt):
+        if n == 0:
+            return np.zeros(0, dt)
+        return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(np.ctypeslib.as_ctypes_type(dt))), (n,)).copy()
+
+    cells = arr(L.orc_grid_cells(h), 2 * nc, np.uint32).reshape(-1, 2)
+    leaves = arr(L.orc_grid_leaves(h), 2 * nl, np.uint32).reshape(-1, 2)
+    indices = arr(L.orc_grid_indices(h), nk, np.uint32)
+    tp = arr(L.orc_grid_top_pairs(h), ntp, np.uint64)
+    return Grid(kind, np.asarray(res, np.int32), np.asarray(b, np.float32), cells, leaves, indices, tp, h)
+
+
+def build_uniform(vtx, idx, b, res) -> Grid:
+    vtx, idx, b = _f32(vtx), _u32(idx), _f32(b)
+    r = np.ascontiguousarray(res, np.int32)
+    h = lib().orc_build_uniform(_p(vtx), vtx.shape[0], _p(idx), idx.shape[0], _p(b), _p(r))
+    return _wrap(h, 0, r, b)
+
+
+def build_two_level(vtx, idx, b, res, lambda_leaf: float, leaf_threshold: int = 16) -> Grid:
+    vtx, idx, b = _f32(vtx), _u32(idx), _f32(b)
+    r = np.ascontiguousarray(res, np.int32)
+    h = lib().orc_build_two_level(_p(vtx), vtx.shape[0], _p(idx), idx.shape[0], _p(b), _p(r),
+                                  lambda_leaf, leaf_threshold)
+    return _wrap(h, 1, r, b)
+
+
+def trace_closest(g: Grid, org, dirs, tmax=None):
+    """Returns (tri, t, u, v, stats[steps, tests])."""
+    org, dirs = _f32(org), _f32(dirs)
+    n = org.shape[0]
+    ox, oy, oz = (np.ascontiguousarray(org[:, k]) for k in range(3))
+    dx, dy, dz = (np.ascontiguousarray(dirs[:, k]) for k in range(3))
+    tm = _f32(tmax) if tmax is not None else None
+    tri = np.zeros(n, np.uint32)
+    t = np.zeros(n, np.float32)
+    u = np.zeros(n, np.float32)
+    v = np.zeros(n, np.float32)
+    st = np.zeros(2, np.uint64)
+    lib().orc_trace_closest(g.handle, _p(ox), _p(oy), _p(oz), _p(dx), _p(dy), _p(dz), _p(tm), n,
+                            _p(tri), _p(t), _p(u), _p(v), _p(st))
+    return tri, t, u, v, st
+
+
+def trace_any(g: Grid, org, dirs, tmax):
+    org, dirs = _f32(org), _f32(dirs)
+    n = org.shape[0]
+    ox, oy, oz = (np.ascontiguousarray(org[:, k]) for k in range(3))
+    dx, dy, dz = (np.ascontiguousarray(dirs[:, k]) for k in range(3))
+    tm = _f32(tmax)
+    occ = np.zeros(n, np.uint8)
+    st = np.zeros(2, np.uint64)
+    lib().orc_trace_any(g.handle, _p(ox), _p(oy), _p(oz), _p(dx), _p(dy), _p(dz), _p(tm), n,
+                        _p(occ), _p(st))
+    return occ, st
+
+
+def trace_brute(vtx, idx, org, dirs):
+    vtx, idx, org, dirs = _f32(vtx), _u32(idx), _f32(org), _f32(dirs)
+    n = org.shape[0]
+    cols = [np.ascontiguousarray(org[:, k]) for k in range(3)] + [np.ascontiguousarray(dirs[:, k]) for k in range(3)]
+    tri = np.zeros(n, np.uint32)
+    t = np.zeros(n, np.float32)
+    lib().orc_trace_brute(_p(vtx), _p(idx), idx.shape[0], *[_p(c) for c in cols], n, _p(tri), _p(t))
+    return tri, t
+
+
+def t_fp64(vtx, idx, tri, org, dirs) -> np.ndarray:
+    vtx, idx, tri, org, dirs = _f32(vtx), _u32(idx), _u32(tri), _f32(org), _f32(dirs)
+    n = org.shape[0]
+    cols = [np.ascontiguousarray(org[:, k]) for k in range(3)] + [np.ascontiguousarray(dirs[:, k]) for k in range(3)]
+    out = np.zeros(n, np.float64)
+    lib().orc_t_fp64(_p(vtx), _p(idx), _p(tri), *[_p(c) for c in cols], n, _p(out))
+    return out
+
+
+def sincos_2pi(u):
+    u = _f32(u)
+    s = np.zeros_like(u)
+    c = np.zeros_like(u)
+    lib().orc_sincos_2pi(_p(u), u.size, _p(s), _p(c))
+    return s, c
+
+
+def philox(ctr, k0: int, k1: int) -> np.ndarray:
+    ctr = _u32(ctr).reshape(-1, 4)
+    out = np.zeros_like(ctr)
+    lib().orc_philox(_p(ctr), ctr.shape[0], k0, k1, _p(out))
+    return out
+
+
+def camera(cam) -> np.ndarray:
+    out = np.zeros(9, np.float32)
+    lib().orc_camera(_p(_f32(cam.eye)), _p(_f32(cam.forward)), _p(_f32(cam.up)), cam.fov_deg,
+                     cam.res_x, cam.res_y, _p(out))
+    return out
+
+
+def primary_rays(cam, image_id: int = 0):
+    """(org (n,3), dir (n,3)) of the camera's primary rays, pixel-major."""
+    c = camera(cam)
+    n = cam.res_x * cam.res_y
+    dx, dy, dz = (np.zeros(n, np.float32) for _ in range(3))
+    lib().orc_primary_rays(_p(c), cam.res_x, cam.res_y, image_id, _p(dx), _p(dy), _p(dz))
+    org = np.tile(_f32(cam.eye), (n, 1))
+    return org, np.stack([dx, dy, dz], axis=1)
+
+
+def ao_rays(vtx, idx, org, dirs, tri, t, spp: int, seed: int, offset: float):
+    """AO rays from primary hits; returns (org, dir, pixel) for hit pixels only."""
+    vtx, idx, org, dirs, tri, t = _f32(vtx), _u32(idx), _f32(org), _f32(dirs), _u32(tri), _f32(t)
+    n = org.shape[0]
+    m_max = int(np.count_nonzero(tri != MISS)) * spp
+    outs = [np.zeros(m_max, np.float32) for _ in range(6)] + [np.zeros(m_max, np.uint32)]
+    cols = [np.ascontiguousarray(org[:, k]) for k in range(3)] + [np.ascontiguousarray(dirs[:, k]) for k in range(3)]
+    m = lib().orc_ao_rays(_p(vtx), _p(idx), *[_p(c) for c in cols], _p(tri), _p(t), n, spp, seed,
+                          offset, *[_p(o) for o in outs])
+    assert m == m_max
+    ro = np.stack(outs[0:3], axis=1)
+    rd = np.stack(outs[3:6], axis=1)
+    return ro, rd, outs[6]
+
+
+def compact(flags) -> np.ndarray:
+    flags = _u32(flags)
+    out = np.zeros(flags.size, np.uint32)
+    m = lib().orc_compact(_p(flags), flags.size, _p(out))
+    return out[:m]
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(n)
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()

@@ -1,0 +1,53 @@
+/* Oracle (test infrastructure only): CPU restatement of Shinobi's grid
+ * build, DDA traversal and ray generation.  Used as the checker by the
+ * tests, the smoke check and the bench's CPU baseline; never by the product. */
+#ifndef SHINOBI_ORACLE_H
+#define SHINOBI_ORACLE_H
+#include <stdint.h>
+
+typedef struct orc_grid orc_grid;
+
+void orc_bounds(const float* vtx, const uint32_t* idx, uint32_t nt, float out[6]);
+void orc_resolution(uint32_t nt, const float bounds[6], float lambda, int divisor, int min_res,
+                    int out[3]);
+orc_grid* orc_build_uniform(const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                            const float bounds[6], const int res[3]);
+orc_grid* orc_build_two_level(const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                              const float bounds[6], const int res[3], float lambda_leaf,
+                              uint32_t leaf_threshold);
+void orc_grid_free(orc_grid* g);
+void orc_grid_info(const orc_grid* g, uint64_t out[8]);
+const uint32_t* orc_grid_cells(const orc_grid* g);
+const uint32_t* orc_grid_leaves(const orc_grid* g);
+const uint32_t* orc_grid_indices(const orc_grid* g);
+const uint64_t* orc_grid_top_pairs(const orc_grid* g);
+
+int orc_num_threads(void);
+void orc_set_threads(int n);
+void orc_trace_closest(const orc_grid* g, const float* ox, const float* oy, const float* oz,
+                       const float* dx, const float* dy, const float* dz, const float* tmax,
+                       uint32_t n, uint32_t* tri, float* t, float* u, float* v, uint64_t* stats);
+void orc_trace_any(const orc_grid* g, const float* ox, const float* oy, const float* oz,
+                   const float* dx, const float* dy, const float* dz, const float* tmax, uint32_t n,
+                   uint8_t* occluded, uint64_t* stats);
+void orc_trace_brute(const float* vtx, const uint32_t* idx, uint32_t nt, const float* ox,
+                     const float* oy, const float* oz, const float* dx, const float* dy,
+                     const float* dz, uint32_t n, uint32_t* tri, float* t);
+void orc_t_fp64(const float* vtx, const uint32_t* idx, const uint32_t* tri, const float* ox,
+                const float* oy, const float* oz, const float* dx, const float* dy, const float* dz,
+                uint32_t n, double* t64);
+
+void orc_sincos_2pi(const float* u, uint32_t n, float* s, float* c);
+void orc_philox(const uint32_t* ctr, uint32_t n, uint32_t k0, uint32_t k1, uint32_t* out);
+void orc_camera(const float eye[3], const float fwd[3], const float up[3], float fov_deg,
+                uint32_t resx, uint32_t resy, float out[9]);
+void orc_primary_rays(const float cam[9], uint32_t resx, uint32_t resy, uint32_t image_id,
+                      float* dx, float* dy, float* dz);
+uint32_t orc_ao_rays(const float* vtx, const uint32_t* idx, const float* ox, const float* oy,
+                     const float* oz, const float* dx, const float* dy, const float* dz,
+                     const uint32_t* tri, const float* t, uint32_t n, uint32_t spp, uint32_t seed,
+                     float offset, float* rox, float* roy, float* roz, float* rdx, float* rdy,
+                     float* rdz, uint32_t* rpix);
+uint32_t orc_compact(const uint32_t* flags, uint32_t n, uint32_t* out);
+
+#endif

@@ -1,0 +1,319 @@
+"""shinobi_b200: B200-native grid ray tracing (Python bindings of the C ABI).
+
+The compute path lives in ``libshinobi_b200.so`` (hand-written sm_100a CUDA
+behind the C ABI of ``include/shinobi_b200.h``).  This module is a thin
+ctypes binding for tests, the benchmark and Python users; torch is used only
+to hold device buffers and streams.  There is no CPU fallback: every call
+goes to the CUDA library and raises ``ShinobiError`` on failure.
+
+Names follow the reference's operator surface: a ``FaceSoup`` holds the
+triangles (FaceSoup<frame>), ``Grid.build`` plays FastSimpleGridBuilder /
+FastTwoLevelGridBuilder, ``Grid.trace_*`` play the grid traversers with the
+intersector, and ``Grid.trace_primary`` / ``Grid.trace_ao`` the ray
+generators with the trace<> kernel.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from ._abi import (SHN_GRID_TWO_LEVEL, SHN_GRID_UNIFORM, SHN_MEM_DEVICE, SHN_MEM_HOST, SHN_MISS,
+                   GridInfo, GridParams)
+
+__all__ = ["ShinobiError", "Context", "FaceSoup", "Grid", "grid_params", "SHN_MISS",
+           "SHN_GRID_UNIFORM", "SHN_GRID_TWO_LEVEL", "exclusive_scan", "compact", "sort_keys",
+           "camera_struct", "default_context"]
+
+
+class ShinobiError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        self.status = status
+        super().__init__(f"{_abi.STATUS.get(status, status)}: {msg}")
+
+
+def _torch():
+    import torch  # noqa: PLC0415  (torch is plumbing: device buffers and streams)
+    return torch
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream(stream):
+    torch = _torch()
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+class Context:
+    """One library context (device, stream-ordered memory pool, HBM budget)."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        self.lib = _abi.load()
+        h = C.c_void_p()
+        st = self.lib.shn_ctx_create(device, hbm_budget_bytes, C.byref(h))
+        if st != 0:
+            raise ShinobiError(st, "shn_ctx_create")
+        self.handle = h
+        self.device = device
+
+    def check(self, st: int, what: str):
+        if st != 0:
+            msg = self.lib.shn_ctx_last_error(self.handle)
+            raise ShinobiError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def memory(self):
+        used, budget = C.c_uint64(), C.c_uint64()
+        self.check(self.lib.shn_ctx_memory(self.handle, C.byref(used), C.byref(budget)), "memory")
+        return used.value, budget.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.shn_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+class FaceSoup:
+    """Triangle storage on the device (FaceSoup::upload / uploadVertices)."""
+
+    def __init__(self, vertices, indices, ctx: Context | None = None, stream=None):
+        self.ctx = ctx or default_context()
+        lib = self.ctx.lib
+        h = C.c_void_p()
+        if isinstance(vertices, np.ndarray):
+            v = np.ascontiguousarray(vertices, np.float32)
+            i = np.ascontiguousarray(indices, np.uint32)
+            st = lib.shn_scene_create(self.ctx.handle, v.ctypes.data_as(C.c_void_p), v.shape[0],
+                                      i.ctypes.data_as(C.c_void_p), i.shape[0], SHN_MEM_HOST,
+                                      _stream(stream), C.byref(h))
+        else:
+            v, i = vertices.contiguous(), indices.contiguous()
+            st = lib.shn_scene_create(self.ctx.handle, _ptr(v), v.shape[0], _ptr(i), i.shape[0],
+                                      SHN_MEM_DEVICE, _stream(stream), C.byref(h))
+        self.ctx.check(st, "shn_scene_create")
+        self.handle = h
+        self.num_triangles = int(indices.shape[0])
+        self.num_vertices = int(vertices.shape[0])
+
+    def update_vertices(self, vertices, stream=None):
+        lib = self.ctx.lib
+        if isinstance(vertices, np.ndarray):
+            v = np.ascontiguousarray(vertices, np.float32)
+            st = lib.shn_scene_update_vertices(self.handle, v.ctypes.data_as(C.c_void_p), v.shape[0],
+                                               SHN_MEM_HOST, _stream(stream))
+        else:
+            v = vertices.contiguous()
+            st = lib.shn_scene_update_vertices(self.handle, _ptr(v), v.shape[0], SHN_MEM_DEVICE,
+                                               _stream(stream))
+        self.ctx.check(st, "shn_scene_update_vertices")
+
+    @property
+    def bounds(self) -> np.ndarray:
+        out = (C.c_float * 6)()
+        self.ctx.check(self.ctx.lib.shn_scene_bounds(self.handle, out), "bounds")
+        return np.array(out[:], np.float32)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx.lib.shn_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def grid_params(kind: int = SHN_GRID_UNIFORM, lambda_: float | None = None, top_divisor=None,
+                min_res=None, lambda_leaf=None, leaf_threshold=None, res=None) -> GridParams:
+    p = GridParams()
+    _abi.load().shn_grid_params_default(kind, C.byref(p))
+    if lambda_ is not None:
+        p.lambda_ = lambda_
+    if top_divisor is not None:
+        p.top_divisor = top_divisor
+    if min_res is not None:
+        p.min_res = min_res
+    if lambda_leaf is not None:
+        p.lambda_leaf = lambda_leaf
+    if leaf_threshold is not None:
+        p.leaf_threshold = leaf_threshold
+    if res is not None:
+        for k in range(3):
+            p.res[k] = int(res[k])
+    return p
+
+
+def camera_struct(cam) -> _abi.Camera:
+    c = _abi.Camera()
+    for k in range(3):
+        c.eye[k] = cam.eye[k]
+        c.forward[k] = cam.forward[k]
+        c.up[k] = cam.up[k]
+    c.fov_deg = cam.fov_deg
+    c.res_x = cam.res_x
+    c.res_y = cam.res_y
+    return c
+
+
+@dataclass
+class HitBuffers:
+    tri: object
+    t: object
+    u: object
+    v: object
+
+    def struct(self) -> _abi.Hits:
+        return _abi.Hits(_ptr(self.tri), _ptr(self.t), _ptr(self.u), _ptr(self.v))
+
+
+def alloc_hits(n: int, device="cuda", uv: bool = True) -> HitBuffers:
+    torch = _torch()
+    return HitBuffers(torch.empty(n, dtype=torch.int32, device=device),
+                      torch.empty(n, dtype=torch.float32, device=device),
+                      torch.empty(n, dtype=torch.float32, device=device) if uv else None,
+                      torch.empty(n, dtype=torch.float32, device=device) if uv else None)
+
+
+class Grid:
+    """Uniform or two-level grid over a FaceSoup (build + traversal)."""
+
+    def __init__(self, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.shn_grid_create(self.ctx.handle, C.byref(h)), "shn_grid_create")
+        self.handle = h
+        self.scene = None
+
+    def build(self, scene: FaceSoup, params: GridParams, stream=None) -> "Grid":
+        self.ctx.check(self.ctx.lib.shn_grid_build(self.handle, scene.handle, C.byref(params),
+                                                   _stream(stream)), "shn_grid_build")
+        self.scene = scene  # the grid reads the scene's triangles for AO frames
+        return self
+
+    def info(self) -> GridInfo:
+        inf = GridInfo()
+        self.ctx.check(self.ctx.lib.shn_grid_get_info(self.handle, C.byref(inf)), "shn_grid_get_info")
+        return inf
+
+    def export(self):
+        """-> dict(cells (C,2), leaves (L,2), indices (K,), top_pairs) as numpy uint arrays."""
+        inf = self.info()
+        cells = np.zeros((inf.num_cells, 2), np.uint32)
+        leaves = np.zeros((inf.num_leaves, 2), np.uint32)
+        indices = np.zeros(inf.num_refs, np.uint32)
+        ntp = inf.num_top_refs if inf.kind == SHN_GRID_TWO_LEVEL else inf.num_refs
+        top = np.zeros(ntp, np.uint64)
+        self.ctx.check(self.ctx.lib.shn_grid_export(
+            self.handle, cells.ctypes.data_as(C.c_void_p), leaves.ctypes.data_as(C.c_void_p),
+            indices.ctypes.data_as(C.c_void_p), top.ctypes.data_as(C.c_void_p)), "shn_grid_export")
+        return {"cells": cells, "leaves": leaves, "indices": indices, "top_pairs": top,
+                "res": np.array(inf.res[:], np.int32), "bounds": np.array(inf.bounds[:], np.float32)}
+
+    @staticmethod
+    def _rays(org, dirs, tmax):
+        cols = [org[:, k].contiguous() for k in range(3)] + [dirs[:, k].contiguous() for k in range(3)]
+        r = _abi.Rays(*[_ptr(c) for c in cols], _ptr(tmax.contiguous()) if tmax is not None else None)
+        return r, cols
+
+    def trace_closest(self, org, dirs, tmax=None, out: HitBuffers | None = None, stream=None) -> HitBuffers:
+        n = org.shape[0]
+        out = out or alloc_hits(n, org.device)
+        r, keep = self._rays(org, dirs, tmax)
+        h = out.struct()
+        self.ctx.check(self.ctx.lib.shn_trace_closest(self.handle, C.byref(r), n, C.byref(h),
+                                                      _stream(stream)), "shn_trace_closest")
+        return out
+
+    def trace_any(self, org, dirs, tmax, out=None, stream=None):
+        torch = _torch()
+        n = org.shape[0]
+        out = out if out is not None else torch.empty(n, dtype=torch.uint8, device=org.device)
+        r, keep = self._rays(org, dirs, tmax)
+        self.ctx.check(self.ctx.lib.shn_trace_any(self.handle, C.byref(r), n, _ptr(out),
+                                                  _stream(stream)), "shn_trace_any")
+        return out
+
+    def trace_primary(self, cam, image_id: int = 0, out: HitBuffers | None = None, stream=None) -> HitBuffers:
+        n = cam.res_x * cam.res_y
+        out = out or alloc_hits(n)
+        c = camera_struct(cam)
+        h = out.struct()
+        self.ctx.check(self.ctx.lib.shn_trace_primary(self.handle, C.byref(c), image_id, C.byref(h),
+                                                      _stream(stream)), "shn_trace_primary")
+        return out
+
+    def trace_ao(self, cam, primary: HitBuffers, spp: int, length: float, offset: float, seed: int,
+                 out=None, num_rays=None, stream=None):
+        torch = _torch()
+        n = cam.res_x * cam.res_y
+        out = out if out is not None else torch.empty(n, dtype=torch.float32, device="cuda")
+        c = camera_struct(cam)
+        h = primary.struct()
+        self.ctx.check(self.ctx.lib.shn_trace_ao(self.handle, C.byref(c), C.byref(h), spp, length,
+                                                 offset, seed, _ptr(out), _ptr(num_rays),
+                                                 _stream(stream)), "shn_trace_ao")
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx.lib.shn_grid_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def exclusive_scan(x, ctx: Context | None = None, stream=None):
+    """uint32 exclusive scan; returns n+1 values (last = total)."""
+    torch = _torch()
+    ctx = ctx or default_context()
+    out = torch.empty(x.numel() + 1, dtype=torch.int32, device=x.device)
+    ctx.check(ctx.lib.shn_exclusive_scan_u32(ctx.handle, _ptr(x), _ptr(out), x.numel(), _stream(stream)),
+              "shn_exclusive_scan_u32")
+    return out
+
+
+def compact(flags, ctx: Context | None = None, stream=None):
+    torch = _torch()
+    ctx = ctx or default_context()
+    out = torch.empty(max(1, flags.numel()), dtype=torch.int32, device=flags.device)
+    cnt = torch.zeros(1, dtype=torch.int32, device=flags.device)
+    ctx.check(ctx.lib.shn_compact_u32(ctx.handle, _ptr(flags), flags.numel(), _ptr(out), _ptr(cnt),
+                                      _stream(stream)), "shn_compact_u32")
+    return out[: int(cnt.item())]
+
+
+def sort_keys(keys, lo_bit: int, hi_bit: int, ctx: Context | None = None, stream=None):
+    """In-place stable radix sort of int64 keys on bits [lo_bit, hi_bit)."""
+    torch = _torch()
+    ctx = ctx or default_context()
+    tmp = torch.empty_like(keys)
+    ctx.check(ctx.lib.shn_sort_keys_u64(ctx.handle, _ptr(keys), _ptr(tmp), keys.numel(), lo_bit, hi_bit,
+                                        _stream(stream)), "shn_sort_keys_u64")
+    return keys

@@ -1,0 +1,104 @@
+"""ctypes declarations of the C ABI in include/shinobi_b200.h."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import build as _build
+
+vp = C.c_void_p
+u32 = C.c_uint32
+u64 = C.c_uint64
+i32 = C.c_int
+f32 = C.c_float
+
+STATUS = {
+    0: "SHN_OK", 1: "SHN_ERR_INVALID", 2: "SHN_ERR_CUDA", 3: "SHN_ERR_OOM", 4: "SHN_ERR_TIMEOUT",
+    5: "SHN_ERR_BUDGET", 6: "SHN_ERR_NOT_BUILT", 7: "SHN_ERR_BUSY", 8: "SHN_ERR_CANCELLED",
+}
+
+SHN_MISS = 0xFFFFFFFF
+SHN_MEM_HOST = 0
+SHN_MEM_DEVICE = 1
+SHN_GRID_UNIFORM = 0
+SHN_GRID_TWO_LEVEL = 1
+
+
+class GridParams(C.Structure):
+    _fields_ = [("kind", u32), ("lambda_", f32), ("top_divisor", i32), ("min_res", i32),
+                ("lambda_leaf", f32), ("leaf_threshold", u32), ("res", i32 * 3)]
+
+
+class GridInfo(C.Structure):
+    _fields_ = [("kind", u32), ("res", i32 * 3), ("bounds", f32 * 6), ("cell_size", f32 * 3),
+                ("num_cells", u64), ("num_top_refs", u64), ("num_leaves", u64), ("num_refs", u64),
+                ("device_bytes", u64), ("build_ms", f32)]
+
+
+class Rays(C.Structure):
+    _fields_ = [("ox", vp), ("oy", vp), ("oz", vp), ("dx", vp), ("dy", vp), ("dz", vp), ("tmax", vp)]
+
+
+class Hits(C.Structure):
+    _fields_ = [("tri", vp), ("t", vp), ("u", vp), ("v", vp)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("eye", f32 * 3), ("forward", f32 * 3), ("up", f32 * 3), ("fov_deg", f32),
+                ("res_x", u32), ("res_y", u32)]
+
+
+class PtParams(C.Structure):
+    _fields_ = [("spp", u32), ("max_depth", u32), ("rr_depth", u32), ("albedo", f32),
+                ("light_pos", f32 * 3), ("light_e1", f32 * 3), ("light_e2", f32 * 3),
+                ("light_radiance", f32 * 3), ("background", f32 * 3), ("offset", f32), ("seed", u32)]
+
+
+# name -> (argtypes, restype)
+SIGNATURES = {
+    "shn_abi_version": ([], u32),
+    "shn_status_string": ([i32], C.c_char_p),
+    "shn_ctx_create": ([i32, u64, C.POINTER(vp)], i32),
+    "shn_ctx_destroy": ([vp], None),
+    "shn_ctx_last_error": ([vp], C.c_char_p),
+    "shn_ctx_memory": ([vp, C.POINTER(u64), C.POINTER(u64)], i32),
+    "shn_scene_create": ([vp, vp, u32, vp, u32, u32, vp, C.POINTER(vp)], i32),
+    "shn_scene_update_vertices": ([vp, vp, u32, u32, vp], i32),
+    "shn_scene_bounds": ([vp, C.POINTER(f32)], i32),
+    "shn_scene_num_triangles": ([vp], u32),
+    "shn_scene_destroy": ([vp], None),
+    "shn_grid_params_default": ([u32, C.POINTER(GridParams)], None),
+    "shn_grid_create": ([vp, C.POINTER(vp)], i32),
+    "shn_grid_build": ([vp, vp, C.POINTER(GridParams), vp], i32),
+    "shn_grid_get_info": ([vp, C.POINTER(GridInfo)], i32),
+    "shn_grid_export": ([vp, vp, vp, vp, vp], i32),
+    "shn_grid_destroy": ([vp], None),
+    "shn_trace_closest": ([vp, C.POINTER(Rays), u32, C.POINTER(Hits), vp], i32),
+    "shn_trace_any": ([vp, C.POINTER(Rays), u32, vp, vp], i32),
+    "shn_trace_primary": ([vp, C.POINTER(Camera), u32, C.POINTER(Hits), vp], i32),
+    "shn_trace_ao": ([vp, C.POINTER(Camera), C.POINTER(Hits), u32, f32, f32, u32, vp, vp, vp], i32),
+    "shn_pt_params_default": ([C.POINTER(PtParams)], None),
+    "shn_pt_render": ([vp, vp, C.POINTER(Camera), C.POINTER(PtParams), vp, vp, vp], i32),
+    "shn_exclusive_scan_u32": ([vp, vp, vp, u32, vp], i32),
+    "shn_compact_u32": ([vp, vp, u32, vp, vp, vp], i32),
+    "shn_sort_keys_u64": ([vp, vp, vp, u32, u32, u32, vp], i32),
+}
+
+_lib = None
+
+
+def load(auto_build: bool = True):
+    """Load libshinobi_b200.so (building it first when missing or stale)."""
+    global _lib
+    if _lib is None:
+        if auto_build and _build.stale():
+            _build.build()
+        if not os.path.exists(_build.LIB):
+            raise RuntimeError(f"libshinobi_b200.so not built ({_build.LIB})")
+        lib = C.CDLL(_build.LIB)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = lib
+    return _lib

@@ -1,0 +1,582 @@
+// Sort-based uniform and two-level grid construction for sm_100a.
+//
+// Pipeline (uniform grid, and the top level of the two-level grid):
+//   k_count_scan_tris   exact per-triangle cell counts (bbox range + plane
+//                       test) fused with a decoupled look-back exclusive scan
+//                       -> per-triangle output offsets and the pair total
+//   k_emit_tris         packed (cell << 32 | tri) keys, triangle order
+//   onesweep_sort       stable 8-bit-digit LSD sort on the cell bits
+//   k_ranges            [begin,end) per cell, indices[] and the
+//                       reference-ordered SoA float4 triangle copy
+// Two-level leaf stage:
+//   k_leaf_cells_scan   leaf resolution per top cell fused with the scan of
+//                       leaf-cell counts -> TwoLevelGridCell words
+//   k_leaf_count_scan   exact leaf-cell counts per sorted top pair + scan
+//   k_leaf_emit         (leafId << 32 | tri) keys
+//   onesweep_sort + k_ranges on the leaf keys.
+//
+// The cell arithmetic restates src/Control/Algorithm/FastBuildKernels.h:31-313
+// and src/Control/Algorithm/TwoLevelBuildKernels.h:40-536 operation by
+// operation (see the oracle for the list of canonicalisations); the library
+// is compiled with -fmad=false so the results are bit-identical to it.
+#include <cmath>
+
+#include "internal.h"
+
+namespace shn {
+
+namespace {
+
+constexpr int kScanBlock = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanBlock * kScanItems;
+
+struct TriSoA {
+  const float4* v0;
+  const float4* v1;
+  const float4* v2;
+};
+
+SHN_D void load_tri(const TriSoA& t, uint32_t i, V3& a, V3& b, V3& c) {
+  a = f4v(__ldg(t.v0 + i));
+  b = f4v(__ldg(t.v1 + i));
+  c = f4v(__ldg(t.v2 + i));
+}
+
+SHN_D void tri_bounds(V3 a, V3 b, V3 c, V3& bmin, V3& bmax) {
+  bmin = mk(FLT_MAX, FLT_MAX, FLT_MAX);
+  bmax = mk(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+  bmin = vmin(bmin, a); bmax = vmax(bmax, a);
+  bmin = vmin(bmin, b); bmax = vmax(bmax, b);
+  bmin = vmin(bmin, c); bmax = vmax(bmax, c);
+}
+
+// countRefs / buildUnsortedGrid cell range (FastBuildKernels.h:47-69, 110-133).
+SHN_D void cell_range(V3 a, V3 b, V3 c, const Geom& g, uint32_t lo[3], uint32_t hi[3]) {
+  V3 bmin, bmax;
+  tri_bounds(a, b, c, bmin, bmax);
+  const V3 minf = vmax(mk(0.f, 0.f, 0.f), add(mul(sub(bmin, g.gmin), g.rcpBuild), mk(-kEps, -kEps, -kEps)));
+  const V3 maxf = vmin(sub(g.resf, mk(1.f, 1.f, 1.f)), add(mul(sub(bmax, g.gmin), g.rcpBuild), mk(kEps, kEps, kEps)));
+  lo[0] = (uint32_t)minf.x; lo[1] = (uint32_t)minf.y; lo[2] = (uint32_t)minf.z;
+  hi[0] = (uint32_t)maxf.x; hi[1] = (uint32_t)maxf.y; hi[2] = (uint32_t)maxf.z;
+}
+
+// Cells of one triangle in emission order (z, y, x); plane-distance test when
+// the bbox spans >= 2 cells on every axis (FastBuildKernels.h:137-212).
+template <class F>
+SHN_D void for_each_cell(V3 a, V3 b, V3 c, const Geom& g, F&& emit) {
+  uint32_t lo[3], hi[3];
+  cell_range(a, b, c, g, lo, hi);
+  const uint32_t rx = (uint32_t)g.resf.x;
+  const uint32_t rxy = (uint32_t)(g.resf.x * g.resf.y);
+  if (hi[0] - lo[0] > 0 && hi[1] - lo[1] > 0 && hi[2] - lo[2] > 0) {
+    const V3 n = normalize(cross(sub(b, a), sub(c, a)));
+    const V3 half = muls(g.cs, 0.5f);
+    V3 c0 = mk((float)lo[0], (float)lo[1], (float)lo[2]);
+    c0 = mul(c0, g.cs);
+    c0 = add(add(c0, g.gmin), half);
+    float cz = c0.z - g.cs.z;
+    for (uint32_t z = lo[2]; z <= hi[2]; ++z) {
+      cz += g.cs.z;
+      float cy = c0.y - g.cs.y;
+      for (uint32_t y = lo[1]; y <= hi[1]; ++y) {
+        cy += g.cs.y;
+        float cx = c0.x - g.cs.x;
+        for (uint32_t x = lo[0]; x <= hi[0]; ++x) {
+          cx += g.cs.x;
+          const float d = dot(sub(mk(cx, cy, cz), a), n);
+          const V3 dist = muls(n, d);
+          if (fabsf(dist.x) <= half.x + kEps && fabsf(dist.y) <= half.y + kEps &&
+              fabsf(dist.z) <= half.z + kEps)
+            emit(x + y * rx + z * rxy);
+        }
+      }
+    }
+  } else {
+    for (uint32_t z = lo[2]; z <= hi[2]; ++z)
+      for (uint32_t y = lo[1]; y <= hi[1]; ++y)
+        for (uint32_t x = lo[0]; x <= hi[0]; ++x) emit(x + y * rx + z * rxy);
+  }
+}
+
+// Leaf resolution: largest r with r^3 <= cs_a^3 * lambda * refs / V, clamped
+// to [1, 255] (see the header comment of the oracle for the reasoning).
+SHN_D uint32_t cube_floor(double q) {
+  if (!(q > 0.0)) return 0u;
+  if (__dmul_rn(__dmul_rn(256.0, 256.0), 256.0) <= q) return 256u;
+  uint32_t lo = 0, hi = 256;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    const double m = (double)mid;
+    if (__dmul_rn(__dmul_rn(m, m), m) <= q) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+SHN_D uint32_t leaf_word(const Geom& g, float lambda, uint32_t refs, uint32_t threshold,
+                         uint32_t* count) {
+  uint32_t r[3] = {1u, 1u, 1u};
+  if (refs > threshold) {
+    const double vol = __dmul_rn(__dmul_rn((double)g.cs.x, (double)g.cs.y), (double)g.cs.z);
+    const double lr = __dmul_rn((double)lambda, (double)refs);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double c = (double)comp(g.cs, a);
+      const double q = __ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(c, c), c), lr), vol);
+      r[a] = min(255u, max(1u, cube_floor(q)));
+    }
+  }
+  *count = r[0] * r[1] * r[2];
+  uint32_t y = (r[0] & 0xFFu) | ((r[1] & 0xFFu) << 8) | ((r[2] & 0xFFu) << 16);
+  if (refs > 0) y |= kNotEmpty;
+  return y;
+}
+
+// Leaf cells of one (top cell, tri) pair in emission order
+// (TwoLevelBuildKernels.h:175-222, 327-451).
+template <class F>
+SHN_D void for_each_leaf(V3 a, V3 b, V3 c, const Geom& g, uint32_t topCell, uint32_t cellY,
+                         uint32_t leafBegin, F&& emit) {
+  const uint32_t rX = (uint32_t)g.res[0], rY = (uint32_t)g.res[1];
+  const uint32_t tx = topCell % rX;
+  const uint32_t ty = (topCell % (rX * rY)) / rX;
+  const uint32_t tz = topCell / (rX * rY);
+  V3 bmin, bmax;
+  tri_bounds(a, b, c, bmin, bmax);
+  const V3 cres = mk((float)(cellY & 0xFFu), (float)((cellY >> 8) & 0xFFu), (float)((cellY >> 16) & 0xFFu));
+  V3 origin;
+  origin.x = (float)tx * g.cs.x + g.gmin.x;
+  origin.y = (float)ty * g.cs.y + g.gmin.y;
+  origin.z = (float)tz * g.cs.z + g.gmin.z;
+  const V3 subRCP = divv(cres, g.cs);
+  const V3 minf = add(mul(sub(bmin, origin), subRCP), mk(-0.001f, -0.001f, -0.001f));
+  const V3 maxf = add(mul(sub(bmax, origin), subRCP), mk(1.001f, 1.001f, 1.001f));
+  int lo[3], hp[3];
+  lo[0] = max(0, (int)minf.x); lo[1] = max(0, (int)minf.y); lo[2] = max(0, (int)minf.z);
+  hp[0] = min((int)cres.x, (int)maxf.x);
+  hp[1] = min((int)cres.y, (int)maxf.y);
+  hp[2] = min((int)cres.z, (int)maxf.z);
+  const uint32_t crx = (uint32_t)cres.x;
+  const uint32_t crxy = (uint32_t)(cres.x * cres.y);
+  if (hp[0] - lo[0] > 1 && hp[1] - lo[1] > 1 && hp[2] - lo[2] > 1) {
+    const V3 n = normalize(cross(sub(b, a), sub(c, a)));
+    const V3 scs = divv(g.cs, cres);
+    V3 c0 = mk((float)lo[0], (float)lo[1], (float)lo[2]);
+    c0 = mul(c0, scs);
+    c0 = add(add(c0, origin), muls(scs, 0.5f));
+    float cz = c0.z - scs.z;
+    for (int z = lo[2]; z < hp[2]; ++z) {
+      cz += scs.z;
+      float cy = c0.y - scs.y;
+      for (int y = lo[1]; y < hp[1]; ++y) {
+        cy += scs.y;
+        float cx = c0.x - scs.x;
+        for (int x = lo[0]; x < hp[0]; ++x) {
+          cx += scs.x;
+          const float d = dot(sub(mk(cx, cy, cz), a), n);
+          const V3 dist = muls(n, d);
+          if (fabsf(dist.x) <= scs.x * 0.5f + kEps && fabsf(dist.y) <= scs.y * 0.5f + kEps &&
+              fabsf(dist.z) <= scs.z * 0.5f + kEps)
+            emit((uint32_t)x + (uint32_t)y * crx + (uint32_t)z * crxy + leafBegin);
+        }
+      }
+    }
+  } else {
+    for (int z = lo[2]; z < hp[2]; ++z)
+      for (int y = lo[1]; y < hp[1]; ++y)
+        for (int x = lo[0]; x < hp[0]; ++x)
+          emit((uint32_t)x + (uint32_t)y * crx + (uint32_t)z * crxy + leafBegin);
+  }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_pack_triangles(const float* __restrict__ vtx, const uint32_t* __restrict__ idx,
+                                 uint32_t nt, float4* __restrict__ tri) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    const uint32_t i0 = idx[3 * (size_t)t], i1 = idx[3 * (size_t)t + 1], i2 = idx[3 * (size_t)t + 2];
+    const float* a = vtx + 3 * (size_t)i0;
+    const float* b = vtx + 3 * (size_t)i1;
+    const float* c = vtx + 3 * (size_t)i2;
+    tri[t] = make_float4(a[0], a[1], a[2], __uint_as_float(t));
+    tri[nt + (size_t)t] = make_float4(b[0], b[1], b[2], 0.f);
+    tri[2 * (size_t)nt + t] = make_float4(c[0], c[1], c[2], 0.f);
+  }
+}
+
+// Order-preserving float <-> uint mapping for atomic min/max of bounds.
+SHN_D uint32_t fkey(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+SHN_HD float fval(uint32_t k) {
+  const uint32_t u = (k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k;
+  float f;
+  memcpy(&f, &u, 4);
+  return f;
+}
+
+__global__ void k_bounds(const float4* __restrict__ tri, uint32_t nt, uint32_t* out6) {
+  V3 mn = mk(FLT_MAX, FLT_MAX, FLT_MAX), mx = mk(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < 3ull * nt;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const V3 p = f4v(tri[i]);
+    mn = vmin(mn, p);
+    mx = vmax(mx, p);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mn.x = fminf(mn.x, __shfl_xor_sync(0xFFFFFFFFu, mn.x, o));
+    mn.y = fminf(mn.y, __shfl_xor_sync(0xFFFFFFFFu, mn.y, o));
+    mn.z = fminf(mn.z, __shfl_xor_sync(0xFFFFFFFFu, mn.z, o));
+    mx.x = fmaxf(mx.x, __shfl_xor_sync(0xFFFFFFFFu, mx.x, o));
+    mx.y = fmaxf(mx.y, __shfl_xor_sync(0xFFFFFFFFu, mx.y, o));
+    mx.z = fmaxf(mx.z, __shfl_xor_sync(0xFFFFFFFFu, mx.z, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(out6 + 0, fkey(mn.x)); atomicMin(out6 + 1, fkey(mn.y)); atomicMin(out6 + 2, fkey(mn.z));
+    atomicMax(out6 + 3, fkey(mx.x)); atomicMax(out6 + 4, fkey(mx.y)); atomicMax(out6 + 5, fkey(mx.z));
+  }
+}
+
+__global__ void k_bounds_decode(uint32_t* io6) {
+  if (threadIdx.x < 6) {
+    const float f = fval(io6[threadIdx.x]);
+    io6[threadIdx.x] = __float_as_uint(f);
+  }
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_count_scan_tris(TriSoA tri, uint32_t nt, Geom g,
+                                                               LookbackState st, uint32_t* offs) {
+  __shared__ TileScanSmem<kScanBlock, kScanItems> sm;
+  tile_scan<kScanBlock, kScanItems>(
+      st, nt, sm,
+      [&](uint32_t i) {
+        V3 a, b, c;
+        load_tri(tri, i, a, b, c);
+        uint32_t cnt = 0;
+        for_each_cell(a, b, c, g, [&](uint32_t) { ++cnt; });
+        return cnt;
+      },
+      [&](uint32_t i, uint32_t ex) { offs[i] = ex; }, offs + nt);
+}
+
+__global__ void k_emit_tris(TriSoA tri, uint32_t nt, Geom g, const uint32_t* __restrict__ offs,
+                            uint64_t* __restrict__ keys) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    V3 a, b, c;
+    load_tri(tri, t, a, b, c);
+    uint32_t o = offs[t];
+    for_each_cell(a, b, c, g, [&](uint32_t cell) { keys[o++] = ((uint64_t)cell << 32) | t; });
+  }
+}
+
+// Cell ranges from sorted keys (prepareCellRanges, FastBuildKernels.h:243-311)
+// plus indices[] and the reference-ordered triangle copy.
+__global__ void k_ranges(const uint64_t* __restrict__ keys, uint32_t n, uint2* __restrict__ ranges,
+                         uint32_t* __restrict__ indices, TriSoA tri, float4* __restrict__ rtri) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    const uint32_t c = (uint32_t)(k >> 32);
+    const uint32_t t = (uint32_t)k;
+    if (i == 0 || (uint32_t)(keys[i - 1] >> 32) != c) ranges[c].x = i;
+    if (i + 1 == n || (uint32_t)(keys[i + 1] >> 32) != c) ranges[c].y = i + 1;
+    if (indices) indices[i] = t;
+    if (rtri) {
+      rtri[i] = __ldg(tri.v0 + t);
+      rtri[(size_t)n + i] = __ldg(tri.v1 + t);
+      rtri[2 * (size_t)n + i] = __ldg(tri.v2 + t);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_leaf_cells_scan(const uint2* __restrict__ top_ranges,
+                                                               uint32_t C, Geom g, float lambda,
+                                                               uint32_t threshold, LookbackState st,
+                                                               uint2* __restrict__ cells,
+                                                               uint32_t* d_total) {
+  __shared__ TileScanSmem<kScanBlock, kScanItems> sm;
+  tile_scan<kScanBlock, kScanItems>(
+      st, C, sm,
+      [&](uint32_t c) {
+        const uint2 r = top_ranges[c];
+        uint32_t cnt;
+        leaf_word(g, lambda, r.y - r.x, threshold, &cnt);
+        return cnt;
+      },
+      [&](uint32_t c, uint32_t ex) {
+        const uint2 r = top_ranges[c];
+        uint32_t cnt;
+        const uint32_t y = leaf_word(g, lambda, r.y - r.x, threshold, &cnt);
+        cells[c] = make_uint2(ex, y);
+      },
+      d_total);
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_leaf_count_scan(TriSoA tri, const uint64_t* __restrict__ top,
+                                                               uint32_t P, Geom g,
+                                                               const uint2* __restrict__ cells,
+                                                               LookbackState st, uint32_t* offs) {
+  __shared__ TileScanSmem<kScanBlock, kScanItems> sm;
+  tile_scan<kScanBlock, kScanItems>(
+      st, P, sm,
+      [&](uint32_t i) {
+        const uint64_t k = top[i];
+        const uint32_t c = (uint32_t)(k >> 32), t = (uint32_t)k;
+        V3 a, b, cc;
+        load_tri(tri, t, a, b, cc);
+        const uint2 w = cells[c];
+        uint32_t cnt = 0;
+        for_each_leaf(a, b, cc, g, c, w.y, w.x, [&](uint32_t) { ++cnt; });
+        return cnt;
+      },
+      [&](uint32_t i, uint32_t ex) { offs[i] = ex; }, offs + P);
+}
+
+__global__ void k_leaf_emit(TriSoA tri, const uint64_t* __restrict__ top, uint32_t P, Geom g,
+                            const uint2* __restrict__ cells, const uint32_t* __restrict__ offs,
+                            uint64_t* __restrict__ keys) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
+    const uint64_t k = top[i];
+    const uint32_t c = (uint32_t)(k >> 32), t = (uint32_t)k;
+    V3 a, b, cc;
+    load_tri(tri, t, a, b, cc);
+    const uint2 w = cells[c];
+    uint32_t o = offs[i];
+    for_each_leaf(a, b, cc, g, c, w.y, w.x,
+                  [&](uint32_t leaf) { keys[o++] = ((uint64_t)leaf << 32) | t; });
+  }
+}
+
+int grid_for(uint64_t n, int block, int max_blocks) {
+  const uint64_t b = (n + block - 1) / block;
+  return (int)std::max<uint64_t>(1, std::min<uint64_t>(b, (uint64_t)max_blocks));
+}
+
+shn_status ensure(shn_grid* g, void** p, size_t* cap, size_t bytes, cudaStream_t st) {
+  if (*cap >= bytes && *p) return SHN_OK;
+  if (*p) dev_free(g->ctx, *p, *cap, st);
+  *p = nullptr;
+  *cap = 0;
+  size_t want = std::max<size_t>(bytes + bytes / 8, 256);
+  cudaError_t e = dev_alloc(g->ctx, p, want, st);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return e == cudaErrorMemoryAllocation ? set_error(g->ctx, SHN_ERR_OOM, "device allocation failed")
+                                          : (e == cudaErrorNotPermitted ? set_error(g->ctx, SHN_ERR_BUDGET, "HBM budget exceeded")
+                                                                        : cuda_status(g->ctx, e, "alloc"));
+  }
+  *cap = want;
+  return SHN_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+Geom make_geom(const float b[6], const int res[3]) {
+  Geom g;
+  g.gmin = mk(b[0], b[1], b[2]);
+  g.gmax = mk(b[3], b[4], b[5]);
+  for (int i = 0; i < 3; ++i) g.res[i] = res[i];
+  g.resf = mk((float)res[0], (float)res[1], (float)res[2]);
+  const V3 diag = sub(g.gmax, g.gmin);
+  g.cs = divv(diag, g.resf);
+  g.rcpBuild = divv(mk(1.f, 1.f, 1.f), g.cs);
+  g.rcpTrav = divv(g.resf, diag);
+  return g;
+}
+
+// GridBuilder::computeResolution (GridBuilder.h:41-62) and the two-level top
+// rule (FastTwoLevelGridBuilder.h:87-102), each axis clamped to [1, 2048].
+void compute_resolution(uint32_t nt, const float b[6], float lambda, int divisor, int min_res,
+                        int out[3]) {
+  V3 diag = sub(mk(b[3], b[4], b[5]), mk(b[0], b[1], b[2]));
+  const float volume = diag.x * diag.y * diag.z;
+  const float magic = powf(lambda * (float)nt / volume, 0.3333333f);
+  diag = muls(diag, magic);
+  const float d[3] = {diag.x, diag.y, diag.z};
+  for (int a = 0; a < 3; ++a) {
+    const float v = d[a];
+    int r = (v >= 2048.f || !(v == v)) ? 2048 : (int)v;
+    if (divisor > 1) r = r / divisor;
+    r = std::max(r, min_res);
+    r = std::min(std::max(r, 1), 2048);
+    out[a] = r;
+  }
+}
+
+void launch_pack_triangles(const float* vtx, const uint32_t* idx, uint32_t nt, float4* tri,
+                           cudaStream_t st) {
+  if (!nt) return;
+  k_pack_triangles<<<grid_for(nt, 256, 148 * 16), 256, 0, st>>>(vtx, idx, nt, tri);
+}
+
+void launch_bounds_reduce(const float4* tri, uint32_t nt, float* d_out6, cudaStream_t st) {
+  uint32_t init[6];
+  for (int i = 0; i < 3; ++i) init[i] = 0xFFFFFFFFu;
+  for (int i = 3; i < 6; ++i) init[i] = 0u;
+  cudaMemcpyAsync(d_out6, init, sizeof(init), cudaMemcpyHostToDevice, st);
+  if (nt) k_bounds<<<grid_for(3ull * nt, 256, 148 * 8), 256, 0, st>>>(tri, nt, (uint32_t*)d_out6);
+  k_bounds_decode<<<1, 32, 0, st>>>((uint32_t*)d_out6);
+}
+
+namespace {
+
+shn_status ensure_buf(shn_grid* g, DevBuf& b, size_t bytes, cudaStream_t st) {
+  return ensure(g, &b.ptr, &b.bytes, bytes, st);
+}
+
+LookbackState scan_state(shn_grid* g, uint64_t n, cudaStream_t st, shn_status* rc) {
+  const size_t tiles = ((size_t)n + kScanTile - 1) / kScanTile;
+  *rc = ensure_buf(g, g->scan, (tiles + 2) * 8, st);
+  uint64_t* status = (uint64_t*)g->scan.ptr;
+  uint32_t* ticket = (uint32_t*)(status + tiles + 1);
+  if (*rc == SHN_OK) cudaMemsetAsync(status, 0, (tiles + 2) * 8, st);
+  return LookbackState{status, ticket, g->d_err};
+}
+
+uint32_t scan_tiles(uint64_t n) { return (uint32_t)std::max<uint64_t>(1, (n + kScanTile - 1) / kScanTile); }
+
+shn_status read_words(shn_grid* g, const uint32_t* d_src[], int k, uint32_t* out,
+                      cudaStream_t st) {
+  for (int i = 0; i < k; ++i)
+    cudaMemcpyAsync(g->h_pinned + i, d_src[i], 4, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(g->h_pinned + 7, g->d_err, 4, cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_status(g->ctx, e, "build sync");
+  if (g->h_pinned[7] != 0u)
+    return set_error(g->ctx, SHN_ERR_TIMEOUT, "a bounded device wait gave up during the build");
+  for (int i = 0; i < k; ++i) out[i] = g->h_pinned[i];
+  return SHN_OK;
+}
+
+shn_status finish(shn_grid* g, cudaStream_t st) {
+  cudaEventRecord(g->ev1, st);
+  const uint32_t* none[1] = {g->d_err};
+  uint32_t dummy;
+  shn_status rc = read_words(g, none, 1, &dummy, st);
+  if (rc) return rc;
+  cudaEventElapsedTime(&g->build_ms, g->ev0, g->ev1);
+  g->built = true;
+  return SHN_OK;
+}
+
+}  // namespace
+
+shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p, cudaStream_t st) {
+  shn_ctx* ctx = g->ctx;
+  const uint32_t nt = s->nt;
+  int res[3];
+  if (p->res[0] > 0 && p->res[1] > 0 && p->res[2] > 0) {
+    for (int i = 0; i < 3; ++i) res[i] = std::min(p->res[i], 2048);
+  } else {
+    compute_resolution(nt, s->bounds, p->lambda, p->top_divisor, p->min_res, res);
+  }
+  const uint64_t C = (uint64_t)res[0] * res[1] * res[2];
+  if (C >= (1ull << 31)) return set_error(ctx, SHN_ERR_INVALID, "grid resolution too large");
+  g->kind = p->kind;
+  g->geom = make_geom(s->bounds, res);
+  g->built = false;
+  g->src_tri = s->tri;
+  g->src_nt = s->nt;
+  if (!g->d_err) {
+    if (cudaMalloc(&g->d_err, 64) != cudaSuccess) return set_error(ctx, SHN_ERR_OOM, "err word");
+    if (cudaMallocHost(&g->h_pinned, 64) != cudaSuccess) return set_error(ctx, SHN_ERR_OOM, "pinned");
+    cudaEventCreate(&g->ev0);
+    cudaEventCreate(&g->ev1);
+  }
+  cudaMemsetAsync(g->d_err, 0, 64, st);
+  cudaEventRecord(g->ev0, st);
+  const TriSoA tri{s->tri, s->tri + nt, s->tri + 2 * (size_t)nt};
+  shn_status rc;
+
+  // ---- counts + offsets ------------------------------------------------------
+  if ((rc = ensure_buf(g, g->offs_tri, ((size_t)nt + 1) * 4, st))) return rc;
+  uint32_t* offs = (uint32_t*)g->offs_tri.ptr;
+  uint32_t P = 0;
+  if (nt) {
+    LookbackState ls = scan_state(g, nt, st, &rc);
+    if (rc) return rc;
+    k_count_scan_tris<<<scan_tiles(nt), kScanBlock, 0, st>>>(tri, nt, g->geom, ls, offs);
+    const uint32_t* src[1] = {offs + nt};
+    if ((rc = read_words(g, src, 1, &P, st))) return rc;
+  }
+  if (P >= (1u << 30)) return set_error(ctx, SHN_ERR_INVALID, "more than 2^30 cell references");
+
+  // ---- emit + sort (uniform grid / top level) ----------------------------------
+  for (int i = 0; i < 2; ++i)
+    if ((rc = ensure_buf(g, g->keys[i], (size_t)std::max<uint32_t>(P, 1) * 8, st))) return rc;
+  if ((rc = ensure_buf(g, g->sortws, sort_workspace_bytes(P), st))) return rc;
+  uint64_t* k0 = (uint64_t*)g->keys[0].ptr;
+  uint64_t* k1 = (uint64_t*)g->keys[1].ptr;
+  if (nt) k_emit_tris<<<grid_for(nt, 256, 148 * 16), 256, 0, st>>>(tri, nt, g->geom, offs, k0);
+  uint64_t* sortedTop =
+      onesweep_sort(k0, k1, P, 32, sort_passes_for(C ? C - 1 : 0), g->sortws.ptr, g->d_err, st);
+  const int topBuf = sortedTop == k0 ? 0 : 1;
+
+  g->num_cells = C;
+  g->num_top_refs = (p->kind == SHN_GRID_TWO_LEVEL) ? P : 0;
+  if ((rc = ensure(g, (void**)&g->cells, &g->cap_cells, C * 8, st))) return rc;
+
+  if (p->kind == SHN_GRID_UNIFORM) {
+    if ((rc = ensure(g, (void**)&g->indices, &g->cap_refs, (size_t)std::max<uint32_t>(P, 1) * 4, st))) return rc;
+    if ((rc = ensure(g, (void**)&g->rtri, &g->cap_rtri, (size_t)std::max<uint32_t>(P, 1) * 48, st))) return rc;
+    cudaMemsetAsync(g->cells, 0, C * 8, st);
+    if (P) k_ranges<<<grid_for(P, 256, 148 * 16), 256, 0, st>>>(sortedTop, P, g->cells, g->indices, tri, g->rtri);
+    g->num_refs = P;
+    g->num_leaves = 0;
+    g->top_pairs = sortedTop;
+    return finish(g, st);
+  }
+
+  // ---- two-level leaf stage ------------------------------------------------------
+  if ((rc = ensure_buf(g, g->top_ranges, C * 8, st))) return rc;
+  uint2* topRanges = (uint2*)g->top_ranges.ptr;
+  cudaMemsetAsync(topRanges, 0, C * 8, st);
+  if (P) k_ranges<<<grid_for(P, 256, 148 * 16), 256, 0, st>>>(sortedTop, P, topRanges, nullptr, tri, nullptr);
+  uint32_t* d_L = g->d_err + 1;
+  {
+    LookbackState ls = scan_state(g, C, st, &rc);
+    if (rc) return rc;
+    k_leaf_cells_scan<<<scan_tiles(C), kScanBlock, 0, st>>>(topRanges, (uint32_t)C, g->geom,
+                                                           p->lambda_leaf, p->leaf_threshold, ls,
+                                                           g->cells, d_L);
+  }
+  if ((rc = ensure_buf(g, g->offs_pair, ((size_t)P + 1) * 4, st))) return rc;
+  uint32_t* pairOffs = (uint32_t*)g->offs_pair.ptr;
+  if (P) {
+    LookbackState ls = scan_state(g, P, st, &rc);
+    if (rc) return rc;
+    k_leaf_count_scan<<<scan_tiles(P), kScanBlock, 0, st>>>(tri, sortedTop, P, g->geom, g->cells, ls,
+                                                           pairOffs);
+  } else {
+    cudaMemsetAsync(pairOffs, 0, 4, st);
+  }
+  uint32_t sizes[2];
+  {
+    const uint32_t* src[2] = {d_L, pairOffs + P};
+    if ((rc = read_words(g, src, 2, sizes, st))) return rc;
+  }
+  const uint32_t Lc = sizes[0], R = sizes[1];
+  if (R >= (1u << 30)) return set_error(ctx, SHN_ERR_INVALID, "more than 2^30 leaf references");
+  const int bA = (topBuf + 1) % 3, bB = (topBuf + 2) % 3;
+  if ((rc = ensure_buf(g, g->keys[bA], (size_t)std::max<uint32_t>(R, 1) * 8, st))) return rc;
+  if ((rc = ensure_buf(g, g->keys[bB], (size_t)std::max<uint32_t>(R, 1) * 8, st))) return rc;
+  if ((rc = ensure_buf(g, g->sortws, sort_workspace_bytes(R), st))) return rc;
+  uint64_t* lk0 = (uint64_t*)g->keys[bA].ptr;
+  uint64_t* lk1 = (uint64_t*)g->keys[bB].ptr;
+  if (P) k_leaf_emit<<<grid_for(P, 256, 148 * 16), 256, 0, st>>>(tri, sortedTop, P, g->geom, g->cells,
+                                                                 pairOffs, lk0);
+  uint64_t* sortedLeaf = onesweep_sort(lk0, lk1, R, 32, sort_passes_for(Lc ? Lc - 1 : 0),
+                                       g->sortws.ptr, g->d_err, st);
+  if ((rc = ensure(g, (void**)&g->leaves, &g->cap_leaves, (size_t)std::max<uint32_t>(Lc, 1) * 8, st))) return rc;
+  if ((rc = ensure(g, (void**)&g->indices, &g->cap_refs, (size_t)std::max<uint32_t>(R, 1) * 4, st))) return rc;
+  if ((rc = ensure(g, (void**)&g->rtri, &g->cap_rtri, (size_t)std::max<uint32_t>(R, 1) * 48, st))) return rc;
+  cudaMemsetAsync(g->leaves, 0, (size_t)Lc * 8, st);
+  if (R) k_ranges<<<grid_for(R, 256, 148 * 16), 256, 0, st>>>(sortedLeaf, R, g->leaves, g->indices, tri, g->rtri);
+  g->num_leaves = Lc;
+  g->num_refs = R;
+  g->top_pairs = sortedTop;
+  return finish(g, st);
+}
+
+}  // namespace shn

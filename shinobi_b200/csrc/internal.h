@@ -1,0 +1,110 @@
+// Host-side internals shared by the translation units of libshinobi_b200.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/shinobi_b200.h"
+#include "common.cuh"
+#include "lookback.cuh"
+
+namespace shn {
+
+// Device buffer from the context's stream-ordered pool.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace shn
+
+struct shn_ctx {
+  int device = 0;
+  int num_sms = 148;
+  uint64_t budget = 0;
+  std::atomic<uint64_t> used{0};
+  cudaMemPool_t pool = nullptr;
+  std::mutex mu;
+  std::string last_error;
+  uint32_t* d_err = nullptr;    // device error word of context-level primitives
+  void* scratch = nullptr;      // small reusable workspace for primitives
+  size_t scratch_bytes = 0;
+};
+
+struct shn_scene {
+  shn_ctx* ctx = nullptr;
+  uint32_t nv = 0, nt = 0;
+  float* vtx = nullptr;      // 3*nv
+  uint32_t* idx = nullptr;   // 3*nt
+  float4* tri = nullptr;     // 3*nt: v0[nt], v1[nt], v2[nt] (w of v0 = tri id bits)
+  float bounds[6] = {0, 0, 0, 0, 0, 0};
+  size_t bytes = 0;
+};
+
+struct shn_grid {
+  shn_ctx* ctx = nullptr;
+  bool built = false;
+  uint32_t kind = 0;
+  shn::Geom geom{};
+  uint64_t num_cells = 0, num_top_refs = 0, num_leaves = 0, num_refs = 0;
+  // results
+  uint2* cells = nullptr;       // uniform ranges / two-level cell words
+  uint2* leaves = nullptr;      // two-level leaf ranges
+  uint32_t* indices = nullptr;  // tri id per reference
+  float4* rtri = nullptr;       // 3*num_refs: reference-ordered v0[], v1[], v2[]
+  uint64_t* top_pairs = nullptr;  // two-level: sorted top pairs; uniform: sorted pairs
+  size_t cap_cells = 0, cap_leaves = 0, cap_refs = 0, cap_rtri = 0;
+  // grow-only build workspace
+  shn::DevBuf offs_tri, offs_pair, scan, top_ranges, keys[3], sortws;
+  uint32_t* d_err = nullptr;
+  uint32_t* h_pinned = nullptr; // pinned host words for size read-backs
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float build_ms = 0.f;
+  size_t bytes = 0;
+  // scene the grid was built over (triangles by id, for shading / AO frames)
+  const float4* src_tri = nullptr;
+  uint32_t src_nt = 0;
+};
+
+namespace shn {
+
+// api.cu
+cudaError_t dev_alloc(shn_ctx* ctx, void** p, size_t bytes, cudaStream_t st);
+void dev_free(shn_ctx* ctx, void* p, size_t bytes, cudaStream_t st);
+shn_status set_error(shn_ctx* ctx, shn_status s, const std::string& msg);
+shn_status cuda_status(shn_ctx* ctx, cudaError_t e, const char* where);
+
+// sort.cu
+size_t sort_workspace_bytes(uint32_t n);
+uint32_t sort_tiles(uint32_t n);
+uint64_t* onesweep_sort(uint64_t* buf0, uint64_t* buf1, uint32_t n, uint32_t lo_bit,
+                        uint32_t passes, void* ws, uint32_t* d_err, cudaStream_t st);
+uint32_t sort_passes_for(uint64_t max_key_value);
+
+// build.cu
+Geom make_geom(const float b[6], const int res[3]);
+void compute_resolution(uint32_t nt, const float b[6], float lambda, int divisor, int min_res,
+                        int out[3]);
+shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p, cudaStream_t st);
+void launch_pack_triangles(const float* vtx, const uint32_t* idx, uint32_t nt, float4* tri,
+                           cudaStream_t st);
+void launch_bounds_reduce(const float4* tri, uint32_t nt, float* d_out6, cudaStream_t st);
+
+// trace.cu
+struct CamView;
+CamView make_camera(const shn_camera* c);
+
+// scan.cu (context-level primitives)
+void launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, void* ws, uint32_t* err,
+                           cudaStream_t st);
+size_t scan_workspace_bytes(uint32_t n);
+void launch_compact(const uint32_t* flags, uint32_t n, uint32_t* out_idx, uint32_t* d_count,
+                    void* ws, uint32_t* err, cudaStream_t st);
+
+}  // namespace shn

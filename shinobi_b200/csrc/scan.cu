@@ -1,0 +1,69 @@
+// Context-level parallel primitives: single-pass exclusive scan and stable
+// stream compaction (decoupled look-back).  Replace the reference's
+// three-level InclusiveScan with a cudaMalloc per call (src/Utils/Scan.cu:124-252),
+// chag::pp::prefix (src/Utils/chag/pp/detail/prefix.cu.inl:59-239) and the
+// unused chag::pp::compact (src/Utils/chag/pp/detail/compact.cu.inl:57-200).
+#include "internal.h"
+
+namespace shn {
+
+namespace {
+constexpr int kBlock = 256;
+constexpr int kItems = 8;
+constexpr int kTile = kBlock * kItems;
+
+__global__ void __launch_bounds__(kBlock) k_exclusive_scan(const uint32_t* __restrict__ in,
+                                                          uint32_t* __restrict__ out, uint32_t n,
+                                                          LookbackState st) {
+  __shared__ TileScanSmem<kBlock, kItems> sm;
+  tile_scan<kBlock, kItems>(
+      st, n, sm, [&](uint32_t i) { return in[i]; }, [&](uint32_t i, uint32_t ex) { out[i] = ex; },
+      out + n);
+}
+
+__global__ void __launch_bounds__(kBlock) k_compact(const uint32_t* __restrict__ flags,
+                                                   uint32_t* __restrict__ out, uint32_t n,
+                                                   uint32_t* d_count, LookbackState st) {
+  __shared__ TileScanSmem<kBlock, kItems> sm;
+  tile_scan<kBlock, kItems>(
+      st, n, sm, [&](uint32_t i) { return flags[i] ? 1u : 0u; },
+      [&](uint32_t i, uint32_t ex) {
+        if (flags[i]) out[ex] = i;
+      },
+      d_count);
+}
+}  // namespace
+
+size_t scan_workspace_bytes(uint32_t n) {
+  const size_t tiles = ((size_t)n + kTile - 1) / kTile;
+  return (tiles + 2) * 8;
+}
+
+static LookbackState prep(void* ws, uint32_t n, uint32_t* err, cudaStream_t st) {
+  const size_t tiles = ((size_t)n + kTile - 1) / kTile;
+  uint64_t* status = (uint64_t*)ws;
+  cudaMemsetAsync(status, 0, (tiles + 2) * 8, st);
+  return LookbackState{status, (uint32_t*)(status + tiles + 1), err};
+}
+
+void launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, void* ws, uint32_t* err,
+                           cudaStream_t st) {
+  if (n == 0) {
+    cudaMemsetAsync(out, 0, 4, st);
+    return;
+  }
+  LookbackState ls = prep(ws, n, err, st);
+  k_exclusive_scan<<<(n + kTile - 1) / kTile, kBlock, 0, st>>>(in, out, n, ls);
+}
+
+void launch_compact(const uint32_t* flags, uint32_t n, uint32_t* out_idx, uint32_t* d_count,
+                    void* ws, uint32_t* err, cudaStream_t st) {
+  if (n == 0) {
+    cudaMemsetAsync(d_count, 0, 4, st);
+    return;
+  }
+  LookbackState ls = prep(ws, n, err, st);
+  k_compact<<<(n + kTile - 1) / kTile, kBlock, 0, st>>>(flags, out_idx, n, d_count, ls);
+}
+
+}  // namespace shn

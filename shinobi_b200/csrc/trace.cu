@@ -1,0 +1,346 @@
+// Persistent, warp-scheduled trace kernels: each warp takes 32 rays at a time
+// from a global atomic pool (the reference's trace<> kernel took 96-ray
+// batches per warp, src/Engine/RayTracingKernels.h:60-100) and traces them to
+// completion.  Variants: SoA rays (closest / any), in-kernel camera rays
+// (RegularPrimaryRayGenerator) and in-kernel ambient-occlusion rays
+// generated from compacted primary hits.
+#include "internal.h"
+#include "trace.cuh"
+
+namespace shn {
+
+namespace {
+
+constexpr int kTraceBlock = 128;
+
+struct RaysView {
+  const float *ox, *oy, *oz, *dx, *dy, *dz, *tmax;
+};
+
+SHN_D bool next_batch(uint32_t* counter, uint32_t n, uint32_t& base) {
+  const int lane = threadIdx.x & 31;
+  uint32_t b = 0;
+  if (lane == 0) b = atomicAdd(counter, 32u);
+  base = __shfl_sync(0xFFFFFFFFu, b, 0);
+  return base < n;
+}
+
+template <int KIND, bool ANY>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_rays(GridView G, RaysView R, uint32_t n,
+                                                            uint32_t* counter, uint32_t* otri,
+                                                            float* ot, float* ou, float* ov,
+                                                            uint8_t* occ) {
+  uint32_t base;
+  while (next_batch(counter, n, base)) {
+    const uint32_t i = base + (threadIdx.x & 31);
+    if (i < n) {
+      const V3 o = mk(R.ox[i], R.oy[i], R.oz[i]);
+      const V3 d = mk(R.dx[i], R.dy[i], R.dz[i]);
+      Hit h{R.tmax ? R.tmax[i] : FLT_MAX, kMiss, 0.f, 0.f};
+      trace_ray<KIND, ANY>(G, o, d, h);
+      if (ANY) {
+        occ[i] = h.tri != kMiss ? 1 : 0;
+      } else {
+        otri[i] = h.tri;
+        ot[i] = h.t;
+        if (ou) ou[i] = h.u;
+        if (ov) ov[i] = h.v;
+      }
+    }
+  }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_camera(GridView G, CamView cam,
+                                                              uint32_t image_id, uint32_t n,
+                                                              uint32_t* counter, uint32_t* otri,
+                                                              float* ot, float* ou, float* ov) {
+  uint32_t base;
+  while (next_batch(counter, n, base)) {
+    const uint32_t i = base + (threadIdx.x & 31);
+    if (i < n) {
+      const V3 d = primary_dir(cam, i, image_id);
+      Hit h{FLT_MAX, kMiss, 0.f, 0.f};
+      trace_ray<KIND, false>(G, cam.eye, d, h);
+      otri[i] = h.tri;
+      ot[i] = h.t;
+      if (ou) ou[i] = h.u;
+      if (ov) ov[i] = h.v;
+    }
+  }
+}
+
+// Compaction of hit pixels: hit_idx[k] = k-th pixel with a hit, pos[p] = its rank.
+__global__ void __launch_bounds__(256) k_compact_hits(const uint32_t* __restrict__ tri, uint32_t n,
+                                                      uint32_t* __restrict__ hit_idx,
+                                                      uint32_t* __restrict__ pos, uint32_t* d_m,
+                                                      LookbackState st) {
+  __shared__ TileScanSmem<256, 8> sm;
+  tile_scan<256, 8>(
+      st, n, sm, [&](uint32_t i) { return tri[i] != kMiss ? 1u : 0u; },
+      [&](uint32_t i, uint32_t ex) {
+        pos[i] = ex;
+        if (tri[i] != kMiss) hit_idx[ex] = i;
+      },
+      d_m);
+}
+
+struct AoParams {
+  CamView cam;
+  uint32_t image_id, spp, seed;
+  float len, offset;
+  const float4* stri;  // scene triangles v0[nt], v1[nt], v2[nt]
+  uint32_t snt;
+};
+
+template <int KIND>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_ao(GridView G, AoParams A,
+                                                          const uint32_t* __restrict__ ptri,
+                                                          const float* __restrict__ pt,
+                                                          const uint32_t* __restrict__ hit_idx,
+                                                          const uint32_t* d_m, uint32_t* counter,
+                                                          uint8_t* __restrict__ occ) {
+  const uint32_t n = (*d_m) * A.spp;
+  uint32_t base;
+  while (next_batch(counter, n, base)) {
+    const uint32_t r = base + (threadIdx.x & 31);
+    if (r < n) {
+      const uint32_t k = r / A.spp, s = r - k * A.spp;
+      const uint32_t p = hit_idx[k];
+      const uint32_t tri = ptri[p];
+      const float t = pt[p];
+      const V3 d = primary_dir(A.cam, p, A.image_id);
+      const V3 v0 = f4v(__ldg(A.stri + tri));
+      const V3 v1 = f4v(__ldg(A.stri + A.snt + tri));
+      const V3 v2 = f4v(__ldg(A.stri + 2 * (size_t)A.snt + tri));
+      const V3 e1 = sub(v1, v0);
+      V3 nn = normalize(cross(e1, sub(v2, v0)));
+      if (dot(nn, d) > 0.f) nn = mk(-nn.x, -nn.y, -nn.z);
+      const V3 tx = normalize(e1);
+      const V3 ty = cross(nn, tx);
+      const V3 hp = add(A.cam.eye, muls(d, t));
+      const V3 o = add(hp, muls(nn, A.offset));
+      const uint4 w = philox4x32(make_uint4(p, s, 0u, 0x414Fu), A.seed, 0u);
+      const float u1 = u01(w.x), u2 = u01(w.y);
+      float sn, cs;
+      sincos_2pi(u1, sn, cs);
+      const float rr = sqrtf(1.f - u2);
+      const float lx = sn * rr, ly = cs * rr, lz = sqrtf(u2);
+      const V3 dir = mk(tx.x * lx + ty.x * ly + nn.x * lz, tx.y * lx + ty.y * ly + nn.y * lz,
+                        tx.z * lx + ty.z * ly + nn.z * lz);
+      Hit h{A.len, kMiss, 0.f, 0.f};
+      trace_ray<KIND, true>(G, o, dir, h);
+      occ[r] = h.tri != kMiss ? 1 : 0;
+    }
+  }
+}
+
+__global__ void k_ao_finalize(const uint32_t* __restrict__ ptri, const uint32_t* __restrict__ pos,
+                              const uint8_t* __restrict__ occ, uint32_t n, uint32_t spp,
+                              const uint32_t* d_m, float* __restrict__ ao, uint32_t* d_num_rays) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p == 0 && d_num_rays) *d_num_rays = (*d_m) * spp;
+  if (p >= n) return;
+  if (ptri[p] == kMiss) {
+    ao[p] = 1.0f;
+    return;
+  }
+  const uint32_t b = pos[p] * spp;
+  uint32_t c = 0;
+  for (uint32_t s = 0; s < spp; ++s) c += occ[b + s];
+  ao[p] = 1.0f - (float)c / (float)spp;
+}
+
+template <class K>
+int persistent_blocks(K kernel, int num_sms) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTraceBlock, 0);
+  return std::max(1, per_sm) * num_sms;
+}
+
+GridView view_of(const shn_grid* g) {
+  GridView v;
+  v.g = g->geom;
+  v.kind = g->kind;
+  v.cells = g->cells;
+  v.leaves = g->leaves;
+  v.rv0 = g->rtri;
+  v.rv1 = g->rtri + g->num_refs;
+  v.rv2 = g->rtri + 2 * g->num_refs;
+  return v;
+}
+
+// Per-call scratch from the context pool, released stream-ordered.
+struct Scratch {
+  shn_ctx* ctx;
+  cudaStream_t st;
+  std::vector<std::pair<void*, size_t>> items;
+  cudaError_t err = cudaSuccess;
+  template <class T>
+  T* get(size_t count) {
+    void* p = nullptr;
+    const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    cudaError_t e = dev_alloc(ctx, &p, bytes, st);
+    if (e != cudaSuccess) {
+      err = e;
+      return nullptr;
+    }
+    items.emplace_back(p, bytes);
+    return (T*)p;
+  }
+  ~Scratch() {
+    for (auto& it : items) dev_free(ctx, it.first, it.second, st);
+  }
+};
+
+shn_status check_launch(shn_ctx* ctx, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? SHN_OK : cuda_status(ctx, e, what);
+}
+
+}  // namespace
+
+CamView make_camera(const shn_camera* c) {
+  // Camera::init (src/Primitive/Camera.h:41-60), host FP32 as in the reference.
+  const float aspect = (float)c->res_x / (float)c->res_y;
+  const V3 f = normalize(mk(c->forward[0], c->forward[1], c->forward[2]));
+  const V3 r = normalize(cross(f, mk(c->up[0], c->up[1], c->up[2])));
+  const V3 u = normalize(cross(f, r));
+  const float ang = c->fov_deg * 3.14159265358979323846f / 180.f;
+  const float tn = tanf(ang / 2.f);
+  const V3 row = muls(muls(muls(r, 2.f), tn), aspect);
+  const V3 col = muls(muls(u, 2.f), tn);
+  CamView v;
+  v.eye = mk(c->eye[0], c->eye[1], c->eye[2]);
+  v.sx = mk(row.x / (float)c->res_x, row.y / (float)c->res_x, row.z / (float)c->res_x);
+  v.sy = mk(col.x / (float)c->res_y, col.y / (float)c->res_y, col.z / (float)c->res_y);
+  v.tl = sub(sub(f, mk(row.x / 2.f, row.y / 2.f, row.z / 2.f)), mk(col.x / 2.f, col.y / 2.f, col.z / 2.f));
+  v.resx = (float)c->res_x;
+  v.res_x = c->res_x;
+  v.res_y = c->res_y;
+  return v;
+}
+
+}  // namespace shn
+
+using namespace shn;
+
+extern "C" {
+
+shn_status shn_trace_closest(const shn_grid* g, const shn_rays* rays, uint32_t n, shn_hits* hits,
+                             void* stream) {
+  if (!g || !rays || !hits) return SHN_ERR_INVALID;
+  if (!g->built) return set_error(g->ctx, SHN_ERR_NOT_BUILT, "grid not built");
+  if (n == 0) return SHN_OK;
+  if (!rays->ox || !rays->oy || !rays->oz || !rays->dx || !rays->dy || !rays->dz || !hits->tri || !hits->t)
+    return set_error(g->ctx, SHN_ERR_INVALID, "null ray or hit array");
+  cudaStream_t st = (cudaStream_t)stream;
+  Scratch S{g->ctx, st};
+  uint32_t* counter = S.get<uint32_t>(1);
+  if (!counter) return set_error(g->ctx, SHN_ERR_OOM, "trace scratch");
+  cudaMemsetAsync(counter, 0, 4, st);
+  const GridView G = view_of(g);
+  const RaysView R{rays->ox, rays->oy, rays->oz, rays->dx, rays->dy, rays->dz, rays->tmax};
+  if (g->kind == SHN_GRID_UNIFORM) {
+    static int blocks = persistent_blocks(k_trace_rays<0, false>, g->ctx->num_sms);
+    k_trace_rays<0, false><<<blocks, kTraceBlock, 0, st>>>(G, R, n, counter, hits->tri, hits->t, hits->u, hits->v, nullptr);
+  } else {
+    static int blocks = persistent_blocks(k_trace_rays<1, false>, g->ctx->num_sms);
+    k_trace_rays<1, false><<<blocks, kTraceBlock, 0, st>>>(G, R, n, counter, hits->tri, hits->t, hits->u, hits->v, nullptr);
+  }
+  return check_launch(g->ctx, "trace_closest");
+}
+
+shn_status shn_trace_any(const shn_grid* g, const shn_rays* rays, uint32_t n, uint8_t* d_occluded,
+                         void* stream) {
+  if (!g || !rays || !d_occluded) return SHN_ERR_INVALID;
+  if (!g->built) return set_error(g->ctx, SHN_ERR_NOT_BUILT, "grid not built");
+  if (n == 0) return SHN_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  Scratch S{g->ctx, st};
+  uint32_t* counter = S.get<uint32_t>(1);
+  if (!counter) return set_error(g->ctx, SHN_ERR_OOM, "trace scratch");
+  cudaMemsetAsync(counter, 0, 4, st);
+  const GridView G = view_of(g);
+  const RaysView R{rays->ox, rays->oy, rays->oz, rays->dx, rays->dy, rays->dz, rays->tmax};
+  if (g->kind == SHN_GRID_UNIFORM) {
+    static int blocks = persistent_blocks(k_trace_rays<0, true>, g->ctx->num_sms);
+    k_trace_rays<0, true><<<blocks, kTraceBlock, 0, st>>>(G, R, n, counter, nullptr, nullptr, nullptr, nullptr, d_occluded);
+  } else {
+    static int blocks = persistent_blocks(k_trace_rays<1, true>, g->ctx->num_sms);
+    k_trace_rays<1, true><<<blocks, kTraceBlock, 0, st>>>(G, R, n, counter, nullptr, nullptr, nullptr, nullptr, d_occluded);
+  }
+  return check_launch(g->ctx, "trace_any");
+}
+
+shn_status shn_trace_primary(const shn_grid* g, const shn_camera* cam, uint32_t image_id,
+                             shn_hits* hits, void* stream) {
+  if (!g || !cam || !hits || !hits->tri || !hits->t) return SHN_ERR_INVALID;
+  if (!g->built) return set_error(g->ctx, SHN_ERR_NOT_BUILT, "grid not built");
+  const uint64_t n64 = (uint64_t)cam->res_x * cam->res_y;
+  if (n64 == 0) return SHN_OK;
+  if (n64 > (1u << 24)) return set_error(g->ctx, SHN_ERR_INVALID, "more than 2^24 pixels");
+  const uint32_t n = (uint32_t)n64;
+  cudaStream_t st = (cudaStream_t)stream;
+  Scratch S{g->ctx, st};
+  uint32_t* counter = S.get<uint32_t>(1);
+  if (!counter) return set_error(g->ctx, SHN_ERR_OOM, "trace scratch");
+  cudaMemsetAsync(counter, 0, 4, st);
+  const GridView G = view_of(g);
+  const CamView C = make_camera(cam);
+  if (g->kind == SHN_GRID_UNIFORM) {
+    static int blocks = persistent_blocks(k_trace_camera<0>, g->ctx->num_sms);
+    k_trace_camera<0><<<blocks, kTraceBlock, 0, st>>>(G, C, image_id, n, counter, hits->tri, hits->t, hits->u, hits->v);
+  } else {
+    static int blocks = persistent_blocks(k_trace_camera<1>, g->ctx->num_sms);
+    k_trace_camera<1><<<blocks, kTraceBlock, 0, st>>>(G, C, image_id, n, counter, hits->tri, hits->t, hits->u, hits->v);
+  }
+  return check_launch(g->ctx, "trace_primary");
+}
+
+shn_status shn_trace_ao(const shn_grid* g, const shn_camera* cam, const shn_hits* primary,
+                        uint32_t spp, float length, float offset, uint32_t seed, float* d_ao,
+                        uint32_t* d_num_rays, void* stream) {
+  if (!g || !cam || !primary || !primary->tri || !primary->t || !d_ao || spp == 0) return SHN_ERR_INVALID;
+  if (!g->built) return set_error(g->ctx, SHN_ERR_NOT_BUILT, "grid not built");
+  if (!g->src_tri) return set_error(g->ctx, SHN_ERR_INVALID, "grid has no scene");
+  const uint64_t n64 = (uint64_t)cam->res_x * cam->res_y;
+  if (n64 == 0) return SHN_OK;
+  if (n64 > (1u << 24) || n64 * spp >= (1ull << 32)) return set_error(g->ctx, SHN_ERR_INVALID, "too many AO rays");
+  const uint32_t n = (uint32_t)n64;
+  cudaStream_t st = (cudaStream_t)stream;
+  Scratch S{g->ctx, st};
+  uint32_t* counter = S.get<uint32_t>(4);
+  uint32_t* hit_idx = S.get<uint32_t>(n);
+  uint32_t* pos = S.get<uint32_t>(n);
+  uint8_t* occ = S.get<uint8_t>((size_t)n * spp);
+  const size_t tiles = (n + 2047) / 2048;
+  uint64_t* status = S.get<uint64_t>(tiles + 2);
+  if (S.err != cudaSuccess) return set_error(g->ctx, SHN_ERR_OOM, "ao scratch");
+  cudaMemsetAsync(counter, 0, 16, st);
+  cudaMemsetAsync(status, 0, (tiles + 2) * 8, st);
+  LookbackState ls{status, (uint32_t*)(status + tiles + 1), g->d_err};
+  uint32_t* d_m = counter + 1;
+  k_compact_hits<<<(unsigned)tiles, 256, 0, st>>>(primary->tri, n, hit_idx, pos, d_m, ls);
+  const GridView G = view_of(g);
+  AoParams A;
+  A.cam = make_camera(cam);
+  A.image_id = 0;
+  A.spp = spp;
+  A.seed = seed;
+  A.len = length;
+  A.offset = offset;
+  A.stri = g->src_tri;
+  A.snt = g->src_nt;
+  if (g->kind == SHN_GRID_UNIFORM) {
+    static int blocks = persistent_blocks(k_trace_ao<0>, g->ctx->num_sms);
+    k_trace_ao<0><<<blocks, kTraceBlock, 0, st>>>(G, A, primary->tri, primary->t, hit_idx, d_m, counter, occ);
+  } else {
+    static int blocks = persistent_blocks(k_trace_ao<1>, g->ctx->num_sms);
+    k_trace_ao<1><<<blocks, kTraceBlock, 0, st>>>(G, A, primary->tri, primary->t, hit_idx, d_m, counter, occ);
+  }
+  k_ao_finalize<<<(n + 255) / 256, 256, 0, st>>>(primary->tri, pos, occ, n, spp, d_m, d_ao, d_num_rays);
+  return check_launch(g->ctx, "trace_ao");
+}
+
+}  // extern "C"

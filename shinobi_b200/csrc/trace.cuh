@@ -1,0 +1,254 @@
+// 3D-DDA traversal of uniform and two-level grids with the watertight
+// ray/triangle test, as device functions shared by the trace, AO and
+// path-tracing kernels.
+//
+// Traversal restates UniformGridTraverser (src/Control/Algorithm/SimpleGridTraverser.h:274-401)
+// and TwoLevelGridTraverser (src/Control/Algorithm/TwoLevelGridTraverser.h:445-671):
+// float cell coordinates, continuation while the best t exceeds the current
+// cell's exit (min of tMax), exit when a coordinate reaches res or -1 within
+// 0.1.  Cell lookups clamp the coordinates like the reference's tex3D did;
+// each DDA level carries a step cap of res.x+res.y+res.z+3.  Any-hit stops at
+// the first hit in (EPS, tmax).
+//
+// Triangles are read from the grid's reference-ordered SoA float4 copy
+// (v0[ref], v1[ref], v2[ref]; v0.w carries the triangle id), so a cell's
+// candidates are contiguous and no indices[] indirection is needed.
+#pragma once
+#include "common.cuh"
+
+namespace shn {
+
+struct GridView {
+  Geom g;
+  uint32_t kind;
+  const uint2* __restrict__ cells;
+  const uint2* __restrict__ leaves;
+  const float4* __restrict__ rv0;
+  const float4* __restrict__ rv1;
+  const float4* __restrict__ rv2;
+};
+
+struct Hit {
+  float t;
+  uint32_t tri;
+  float u, v;
+};
+
+// Watertight ray/triangle test (Woop, Benthin, Wald, JCGT 2(1), 2013).
+struct RayWT {
+  V3 org;
+  int kx, ky, kz;
+  float Sx, Sy, Sz;
+};
+
+SHN_D float sel(int k, V3 v) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+SHN_D RayWT wt_setup(V3 org, V3 d) {
+  RayWT r;
+  r.org = org;
+  const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+  r.kz = (ax > ay) ? ((ax > az) ? 0 : 2) : ((ay > az) ? 1 : 2);
+  r.kx = r.kz + 1 == 3 ? 0 : r.kz + 1;
+  r.ky = r.kx + 1 == 3 ? 0 : r.kx + 1;
+  if (sel(r.kz, d) < 0.f) {
+    const int t = r.kx;
+    r.kx = r.ky;
+    r.ky = t;
+  }
+  const float dz = sel(r.kz, d);
+  r.Sx = sel(r.kx, d) / dz;
+  r.Sy = sel(r.ky, d) / dz;
+  r.Sz = 1.0f / dz;
+  return r;
+}
+
+SHN_D bool wt_test(const RayWT& r, float4 p0, float4 p1, float4 p2, float tmin, float tbest,
+                   float& t, float& u, float& v) {
+  const V3 A = sub(f4v(p0), r.org), B = sub(f4v(p1), r.org), C = sub(f4v(p2), r.org);
+  const float Akz = sel(r.kz, A), Bkz = sel(r.kz, B), Ckz = sel(r.kz, C);
+  const float Ax = sel(r.kx, A) - r.Sx * Akz;
+  const float Ay = sel(r.ky, A) - r.Sy * Akz;
+  const float Bx = sel(r.kx, B) - r.Sx * Bkz;
+  const float By = sel(r.ky, B) - r.Sy * Bkz;
+  const float Cx = sel(r.kx, C) - r.Sx * Ckz;
+  const float Cy = sel(r.ky, C) - r.Sy * Ckz;
+  float U = Cx * By - Cy * Bx;
+  float V = Ax * Cy - Ay * Cx;
+  float W = Bx * Ay - By * Ax;
+  if (U == 0.f || V == 0.f || W == 0.f) {
+    U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+    V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+    W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+  }
+  if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
+  const float det = U + V + W;
+  if (det == 0.f) return false;
+  const float T = U * (r.Sz * Akz) + V * (r.Sz * Bkz) + W * (r.Sz * Ckz);
+  const float tt = T / det;
+  if (!(tt > tmin && tt < tbest)) return false;
+  t = tt;
+  u = V / det;
+  v = W / det;
+  return true;
+}
+
+template <bool ANY>
+SHN_D bool test_range(const GridView& G, const RayWT& r, uint32_t b, uint32_t e, Hit& h) {
+  for (uint32_t it = b; it < e; ++it) {
+    const float4 p0 = __ldg(G.rv0 + it);
+    const float4 p1 = __ldg(G.rv1 + it);
+    const float4 p2 = __ldg(G.rv2 + it);
+    float t, u, v;
+    if (wt_test(r, p0, p1, p2, kEps, h.t, t, u, v)) {
+      h.t = t;
+      h.tri = __float_as_uint(p0.w);
+      h.u = u;
+      h.v = v;
+      if (ANY) return true;
+    }
+  }
+  return false;
+}
+
+SHN_D int min_dim(V3 t) { return (t.x < t.y) ? ((t.x < t.z) ? 0 : 2) : ((t.y < t.z) ? 1 : 2); }
+SHN_D float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
+SHN_D void bump(V3& v, int d, float a) {
+  if (d == 0) v.x += a; else if (d == 1) v.y += a; else v.z += a;
+}
+
+template <bool ANY>
+SHN_D void trace_uniform(const GridView& G, V3 org, V3 dir, Hit& h) {
+  const Geom& g = G.g;
+  const V3 rcp = divv(mk(1.f, 1.f, 1.f), dir);
+  const RayWT w = wt_setup(org, dir);
+  if (!(h.t > 0.f)) return;
+  const V3 t1 = mul(sub(g.gmin, org), rcp);
+  V3 t2 = mul(sub(g.gmax, org), rcp);
+  const V3 tmn = vmin(t1, t2);
+  t2 = vmax(t1, t2);
+  const float tEntry = fmaxf(fmaxf(tmn.x, tmn.y), tmn.z);
+  const float tExit = fminf(fminf(t2.x, t2.y), t2.z);
+  if (tExit <= tEntry || tExit < 0.f) return;
+  const float te = tEntry + kEps;
+  const V3 entry = (tEntry >= 0.f) ? add(org, divv(mk(te, te, te), rcp)) : org;
+  V3 cell = mul(sub(entry, g.gmin), g.rcpTrav);
+  cell = mk(floorf(cell.x), floorf(cell.y), floorf(cell.z));
+  const V3 tmp = mk(rcp.x > 0.f ? 1.f : 0.f, rcp.y > 0.f ? 1.f : 0.f, rcp.z > 0.f ? 1.f : 0.f);
+  V3 tMax = mul(sub(add(mul(add(cell, tmp), g.cs), g.gmin), org), rcp);
+  bool valid = (cell.x != (rcp.x > 0.f ? g.resf.x : -1.f)) && (cell.y != (rcp.y > 0.f ? g.resf.y : -1.f)) &&
+               (cell.z != (rcp.z > 0.f ? g.resf.z : -1.f));
+  const int cap = g.res[0] + g.res[1] + g.res[2] + 3;
+  for (int step = 0; valid && step < cap; ++step) {
+    const uint32_t cx = (uint32_t)clampf(cell.x, 0.f, g.resf.x - 1.f);
+    const uint32_t cy = (uint32_t)clampf(cell.y, 0.f, g.resf.y - 1.f);
+    const uint32_t cz = (uint32_t)clampf(cell.z, 0.f, g.resf.z - 1.f);
+    const uint2 range = __ldg(G.cells + (cx + cy * (uint32_t)g.res[0] + cz * (uint32_t)g.res[0] * (uint32_t)g.res[1]));
+    if (test_range<ANY>(G, w, range.x, range.y, h)) return;
+    valid = h.t > tMax.x || h.t > tMax.y || h.t > tMax.z;
+    if (!valid) break;
+    const int d = min_dim(tMax);
+    const float rd = sel(d, rcp);
+    bump(cell, d, rd > 0.f ? 1.f : -1.f);
+    bump(tMax, d, sel(d, g.cs) * fabsf(rd));
+    const float cd = sel(d, cell);
+    valid = !(fabsf(cd - sel(d, g.resf)) < 0.1f || fabsf(cd + 1.f) < 0.1f);
+  }
+}
+
+template <bool ANY>
+SHN_D void trace_two_level(const GridView& G, V3 org, V3 dir, Hit& h) {
+  const Geom& g = G.g;
+  const V3 rcp = divv(mk(1.f, 1.f, 1.f), dir);
+  const RayWT w = wt_setup(org, dir);
+  if (!(h.t > 0.f)) return;
+  const V3 t1 = mul(sub(g.gmin, org), rcp);
+  V3 t2 = mul(sub(g.gmax, org), rcp);
+  const V3 tmn = vmin(t1, t2);
+  t2 = vmax(t1, t2);
+  float tEntry = fmaxf(fmaxf(tmn.x, tmn.y), tmn.z);
+  const float tExit = fminf(fminf(t2.x, t2.y), t2.z);
+  if (tExit <= tEntry || tExit < 0.f) return;
+  tEntry = fmaxf(0.f, tEntry);
+  const float te = tEntry + kEps;
+  const V3 entry = add(org, divv(mk(te, te, te), rcp));
+  V3 cell = mul(sub(entry, g.gmin), g.rcpTrav);
+  cell = mk(floorf(cell.x), floorf(cell.y), floorf(cell.z));
+  const V3 tmp = mk(rcp.x > 0.f ? 1.f : 0.f, rcp.y > 0.f ? 1.f : 0.f, rcp.z > 0.f ? 1.f : 0.f);
+  V3 tMax = mul(sub(add(mul(add(cell, tmp), g.cs), g.gmin), org), rcp);
+  bool valid = (cell.x != (rcp.x > 0.f ? g.resf.x : -1.f)) && (cell.y != (rcp.y > 0.f ? g.resf.y : -1.f)) &&
+               (cell.z != (rcp.z > 0.f ? g.resf.z : -1.f));
+  const int cap = g.res[0] + g.res[1] + g.res[2] + 3;
+  for (int step = 0; valid && step < cap; ++step) {
+    const uint32_t cx = (uint32_t)clampf(cell.x, 0.f, g.resf.x - 1.f);
+    const uint32_t cy = (uint32_t)clampf(cell.y, 0.f, g.resf.y - 1.f);
+    const uint32_t cz = (uint32_t)clampf(cell.z, 0.f, g.resf.z - 1.f);
+    const uint2 cw = __ldg(G.cells + (cx + cy * (uint32_t)g.res[0] + cz * (uint32_t)g.res[0] * (uint32_t)g.res[1]));
+    if (cw.y & kNotEmpty) {
+      const V3 ent = add(org, divv(mk(tEntry, tEntry, tEntry), rcp));
+      const V3 cres = mk((float)(cw.y & 0xFFu), (float)((cw.y >> 8) & 0xFFu), (float)((cw.y >> 16) & 0xFFu));
+      const V3 subRCP = mul(g.rcpTrav, cres);
+      const V3 minB = add(mul(cell, g.cs), g.gmin);
+      V3 sc;
+      sc.x = floorf((ent.x - minB.x) * subRCP.x);
+      sc.y = floorf((ent.y - minB.y) * subRCP.y);
+      sc.z = floorf((ent.z - minB.z) * subRCP.z);
+      const V3 scs = divv(mk(1.f, 1.f, 1.f), subRCP);
+      sc = vmin(sub(cres, mk(1.f, 1.f, 1.f)), vmax(sc, mk(0.f, 0.f, 0.f)));
+      V3 sMax;
+      sMax.x = ((sc.x + tmp.x) * scs.x + minB.x - org.x) * rcp.x;
+      sMax.y = ((sc.y + tmp.y) * scs.y + minB.y - org.y) * rcp.y;
+      sMax.z = ((sc.z + tmp.z) * scs.z + minB.z - org.z) * rcp.z;
+      bool v2 = true;
+      const int cap2 = (int)cres.x + (int)cres.y + (int)cres.z + 3;
+      for (int s2 = 0; v2 && s2 < cap2; ++s2) {
+        const uint32_t li = cw.x + (uint32_t)(sc.x + cres.x * sc.y + cres.x * cres.y * sc.z);
+        const uint2 range = __ldg(G.leaves + li);
+        if (test_range<ANY>(G, w, range.x, range.y, h)) return;
+        v2 = h.t > sMax.x || h.t > sMax.y || h.t > sMax.z;
+        if (!v2) break;
+        const int d = min_dim(sMax);
+        const float rd = sel(d, rcp);
+        bump(sc, d, rd > 0.f ? 1.f : -1.f);
+        bump(sMax, d, sel(d, scs) * fabsf(rd));
+        const float cd = sel(d, sc);
+        v2 = !(fabsf(cd - sel(d, cres)) < 0.1f || fabsf(cd + 1.f) < 0.1f);
+      }
+    }
+    valid = h.t > tMax.x || h.t > tMax.y || h.t > tMax.z;
+    if (!valid) break;
+    const int d = min_dim(tMax);
+    tEntry = sel(d, tMax);
+    const float rd = sel(d, rcp);
+    bump(cell, d, rd > 0.f ? 1.f : -1.f);
+    bump(tMax, d, sel(d, g.cs) * fabsf(rd));
+    const float cd = sel(d, cell);
+    valid = !(fabsf(cd - sel(d, g.resf)) < 0.1f || fabsf(cd + 1.f) < 0.1f);
+  }
+}
+
+template <int KIND, bool ANY>
+SHN_D void trace_ray(const GridView& G, V3 org, V3 dir, Hit& h) {
+  if (KIND == 0) trace_uniform<ANY>(G, org, dir, h);
+  else trace_two_level<ANY>(G, org, dir, h);
+}
+
+// Camera::init result + RegularPixelSampler<1,1> (src/Primitive/Camera.h:67-70,
+// src/Primitive/PixelSampler.h:40-52).
+struct CamView {
+  V3 eye, tl, sx, sy;
+  float resx;
+  uint32_t res_x, res_y;
+};
+
+SHN_D V3 primary_dir(const CamView& c, uint32_t id, uint32_t image_id) {
+  float tmp = (float)image_id / 1.0f;
+  float py = (truncf(tmp) + 0.5f) / 1.0f;
+  float px = tmp - truncf(tmp) + 0.5f / 1.0f;
+  tmp = (float)id / c.resx;
+  py += truncf(tmp);
+  px += (tmp - truncf(tmp)) * c.resx;
+  return mk(c.tl.x + px * c.sx.x + py * c.sy.x, c.tl.y + px * c.sx.y + py * c.sy.y,
+            c.tl.z + px * c.sx.z + py * c.sy.z);
+}
+
+}  // namespace shn
