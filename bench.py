@@ -1,0 +1,429 @@
+"""Benchmark of the grid ray-tracing hot path on B200.
+
+Workload (one step): the 1,048,576-triangle "dense cluster in a sparse
+field" scene held resident in HBM is rebuilt as a two-level grid (top
+lambda = 1/16, leaf lambda = 4), then 1920x1080 primary closest-hit rays are
+traced from a pinhole camera and 4 cosine-distributed ambient-occlusion
+any-hit rays of length 0.1 are traced per primary hit (Philox seed 1).
+The metric is Mrays/s over the whole step (build included); the build's
+ms per million triangles is reported beside it.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU: replicas (every rank renders its own frame of the same scene, no
+collective on the data path); value = all ranks' rays / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mrays/s"
+N_TRIS = 1 << 20
+AO_SPP, AO_LEN, AO_OFFSET, AO_SEED = 4, 0.1, 1e-4, 1
+LAMBDA_TOP, LAMBDA_LEAF = 1.0 / 16.0, 4.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="shinobi", choices=["shinobi", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-stride", type=int, default=64)
+    ap.add_argument("--case", default="full", choices=["full", "small"],
+                    help="small: 480x270 camera, for profiler captures (not a bench line)")
+    return ap.parse_args()
+
+
+def workload_config(extra=None):
+    c = {"workload": "two-level grid rebuild + 1920x1080 primary + 4 AO rays/hit",
+         "scene": "cluster_in_field: 1,048,576 tris (90% in r=0.05 sphere, offsets 0.002; 10% in [-50,50]^3, offsets 0.5), seed 1",
+         "grid": "two-level, lambda_top=1/16 (divisor 1, min res 2), lambda_leaf=4, leaf threshold 16",
+         "camera": "eye (0,0,-0.25), +z, 45 deg vertical FOV, 1920x1080, 1 spp",
+         "ao": "4 cosine rays per hit, length 0.1, origin offset 1e-4, Philox4x32-10 seed 1",
+         "l2": "flushed between timed steps (256 MiB write, outside the timed region)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def fp32_peak_tflops(torch) -> float:
+    """FP32 SIMT peak measured here: cuBLAS SGEMM (TF32 off), 8192^3, best of 5."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(8192, 8192, device="cuda")
+    b = torch.randn(8192, 8192, device="cuda")
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        a @ b
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e))
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    return 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary (or None)."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(sc, cam, stride: int, use_reference_build: bool):
+    """Oracle port (or reference build + port traversal) on a bounded sample, host cores."""
+    import oracle
+    from shinobi_b200 import scenes  # noqa: F401
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    b = oracle.bounds(sc.vertices, sc.indices)
+    res = oracle.resolution(sc.num_triangles, b, LAMBDA_TOP, 1, 2)
+    t0 = time.perf_counter()
+    if use_reference_build:
+        cells, leaves, refs = oracle.ref_host_build(sc.vertices, sc.indices, b, res)
+        t_build = time.perf_counter() - t0
+        g = oracle.grid_from_arrays(1, b, res, cells, leaves, refs, sc.vertices, sc.indices)
+    else:
+        g = oracle.build_two_level(sc.vertices, sc.indices, b, res, LAMBDA_LEAF, 16)
+        t_build = time.perf_counter() - t0
+    org, d = oracle.primary_rays(cam)
+    sel = np.arange(0, org.shape[0], stride)
+    t1 = time.perf_counter()
+    tri, t, _, _, _ = oracle.trace_closest(g, org[sel], d[sel])
+    ro, rd, _ = oracle.ao_rays(sc.vertices, sc.indices, org[sel], d[sel], tri, t, AO_SPP, AO_SEED, AO_OFFSET)
+    oracle.trace_any(g, ro, rd, np.full(ro.shape[0], AO_LEN, np.float32))
+    t_trace = time.perf_counter() - t1
+    sample_rays = sel.size + ro.shape[0]
+    # full-frame estimate: every pixel traced, AO rays in proportion to the sample's hit rate
+    full_rays = org.shape[0] + ro.shape[0] * (org.shape[0] / sel.size)
+    full_time = t_build + t_trace * (full_rays / sample_rays)
+    return {
+        "value": full_rays / full_time / 1e6, "unit": METRIC, "cores": threads,
+        "kind": "reference" if use_reference_build else "port",
+        "sample": (f"full grid build ({'reference TwoLevelGridBuilderHost::hostBuild, 1 thread' if use_reference_build else 'oracle two-level build, 1 thread'}, "
+                   f"{t_build:.2f} s) + every {stride}th pixel's primary ray and its AO rays "
+                   f"({sample_rays} rays, {t_trace:.2f} s on {threads} threads), scaled to the full frame"),
+        "build_ms_per_mtri": t_build * 1e3 / (sc.num_triangles / 1e6),
+        "sample_seconds": t_build + t_trace,
+    }
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from shinobi_b200 import scenes
+    sc = scenes.cluster_in_field(N_TRIS, seed=1)
+    cam = scenes.CAMERA_CLUSTER
+    # per-step sample sized so the whole run stays within a few minutes
+    stride = max(64, 32 * (args.steps + args.warmup))
+    for _ in range(args.warmup):
+        cpu_baseline(sc, cam, stride * 4, True)
+    vals, secs = [], 0.0
+    last = None
+    for _ in range(args.steps):
+        last = cpu_baseline(sc, cam, stride, True)
+        vals.append(last["value"])
+        secs += last["sample_seconds"]
+    v = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Philox4x32-10 scene)",
+            "config": workload_config({"cpu_sample": last["sample"]}),
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": last["cores"], "kind": "reference",
+                             "sample": last["sample"]},
+            "build_ms_per_mtri": last["build_ms_per_mtri"],
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def run_shinobi(args):
+    import torch
+
+    import shinobi_b200 as shn
+    from shinobi_b200 import scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    ctx = shn.Context(local)
+    sc = scenes.cluster_in_field(N_TRIS, seed=1)
+    cam = scenes.CAMERA_CLUSTER
+    if args.case == "small":
+        cam = scenes.Camera(cam.eye, cam.forward, cam.up, cam.fov_deg, 480, 270)
+        args.no_cpu_baseline = True
+    npix = cam.res_x * cam.res_y
+    stream = torch.cuda.current_stream()
+    soup = shn.FaceSoup(sc.vertices, sc.indices, ctx=ctx)
+    p = shn.grid_params(shn.SHN_GRID_TWO_LEVEL, lambda_=LAMBDA_TOP, top_divisor=1, min_res=2,
+                        lambda_leaf=LAMBDA_LEAF, leaf_threshold=16)
+    g = shn.Grid(ctx)
+    hits = shn.alloc_hits(npix)
+    ao = torch.empty(npix, dtype=torch.float32, device="cuda")
+    nao = torch.zeros(1, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def step(times=None):
+        e0, e1, e2, e3 = ev(), ev(), ev(), ev()
+        e0.record()
+        g.build(soup, p)
+        e1.record()
+        g.trace_primary(cam, out=hits)
+        e2.record()
+        g.trace_ao(cam, hits, AO_SPP, AO_LEN, AO_OFFSET, AO_SEED, out=ao, num_rays=nao)
+        e3.record()
+        if times is not None:
+            times.append((e0, e1, e2, e3))
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    n_ao = int(nao.item())
+    rays_per_step = npix + n_ao
+
+    # ---- device-timed region (inputs resident in HBM) -------------------------
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1)          # L2 flush, outside the step's events
+        step(times)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    per = np.array([[a.elapsed_time(b), b.elapsed_time(c), c.elapsed_time(d)] for a, b, c, d in times])
+    step_ms = per.sum(axis=1)
+    total_ms = float(step_ms.sum())
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    value = world * args.steps * rays_per_step / (total_ms * 1e-3) / 1e6
+    build_ms = float(per[:, 0].mean())
+    prim_ms = float(per[:, 1].mean())
+    ao_ms = float(per[:, 2].mean())
+
+    # ---- end to end through the C ABI with host buffers ------------------------
+    hv = torch.from_numpy(sc.vertices).pin_memory()
+    h_tri = torch.empty(npix, dtype=torch.int32).pin_memory()
+    h_t = torch.empty(npix, dtype=torch.float32).pin_memory()
+    h_ao = torch.empty(npix, dtype=torch.float32).pin_memory()
+    vnp = hv.numpy()
+
+    def e2e_step():
+        soup.update_vertices(vnp)                       # H2D of the step's geometry (pinned)
+        step()
+        h_tri.copy_(hits.tri, non_blocking=True)        # D2H of the step's results
+        h_t.copy_(hits.t, non_blocking=True)
+        h_ao.copy_(ao, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    e_s, e_e = ev(), ev()
+    e2e_total = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e_s.record()
+        e2e_step()
+        e_e.record()
+        torch.cuda.synchronize()
+        e2e_total += e_s.elapsed_time(e_e)
+    t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_total = float(t.item())
+    e2e_value = world * args.steps * rays_per_step / (e2e_total * 1e-3) / 1e6
+    h2d = int(sc.vertices.nbytes)
+    d2h = int(npix * 12)
+
+    # ---- roofline of the dominant kernel (work counters, untimed pass) ---------
+    cnt = torch.zeros(2, dtype=torch.int64, device="cuda")
+    ctx.lib.shn_grid_set_stats(g.handle, shn._ptr(cnt))
+    cnt.zero_()
+    g.trace_primary(cam, out=hits)
+    torch.cuda.synchronize()
+    prim_steps, prim_tests = [int(x) for x in cnt.cpu().tolist()]
+    cnt.zero_()
+    g.trace_ao(cam, hits, AO_SPP, AO_LEN, AO_OFFSET, AO_SEED, out=ao, num_rays=nao)
+    torch.cuda.synchronize()
+    ao_steps, ao_tests = [int(x) for x in cnt.cpu().tolist()]
+    ctx.lib.shn_grid_set_stats(g.handle, None)
+    fp32 = fp32_peak_tflops(torch)
+    # dominant kernel: the longer of the two trace kernels
+    if ao_ms >= prim_ms:
+        kname, kms, ksteps, ktests = "k_trace_ao<two-level>", ao_ms, ao_steps, ao_tests
+    else:
+        kname, kms, ksteps, ktests = "k_trace_camera<two-level>", prim_ms, prim_steps, prim_tests
+    work = 10.0 * ksteps + 40.0 * ktests  # FP32 ops per launch (cell visit 10, triangle test 40)
+    achieved = work / (kms * 1e-3) / 1e12
+    traffic = profile_traffic().get(kname)
+    inf = g.info()
+    peaks, peak_kind = measured_peaks()
+    # build bytes (algorithmic): geometry 2 passes + emit + sort + ranges, both levels
+    P, R, L = int(inf.num_top_refs), int(inf.num_refs), int(inf.num_leaves)
+    C0 = int(inf.num_cells)
+
+    def sort_bytes(k, bits):
+        return 8 * k * (1 + 2 * ((bits + 7) // 8))
+
+    b_build = (96 * N_TRIS + 8 * P + sort_bytes(P, max(1, (C0 - 1).bit_length())) + 12 * P + 8 * C0
+               + 48 * P + 8 * R + sort_bytes(R, max(1, (L - 1).bit_length())) + 12 * R + 8 * L + 4 * C0
+               + 48 * R)
+    build_gbs = b_build / (build_ms * 1e-3) / 1e9
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Philox4x32-10 scene, resident in HBM)",
+        "config": workload_config({"rays_per_step": rays_per_step, "parallelism": f"replicas x{world}"}),
+        "build_ms_per_mtri": build_ms / (N_TRIS / 1e6),
+        "phase_ms": {"build": build_ms, "primary": prim_ms, "ao": ao_ms},
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {
+            "bound": "fp32", "kernel": kname, "achieved": achieved, "peak": fp32, "unit": "TFLOP/s",
+            "frac": achieved / fp32, "traffic": traffic,
+            "work": f"{ksteps} cell visits x 10 + {ktests} triangle tests x 40 FP32 ops per launch",
+            "peak_source": "cuBLAS SGEMM (TF32 off) 8192^3 measured in this run; no FP32 figure in MEASURED_PEAKS.json",
+        },
+        "roofline_build": {
+            "bound": "hbm", "achieved": build_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": build_gbs / peaks["hbm_gbs"], "traffic": None,
+            "note": f"whole two-level build (all kernels) per step; peak {peak_kind}",
+        },
+        "clocks": clk,
+    }
+    # kernels launched per step: build (uniform count+emit+sort+ranges, leaf stage) + primary + AO (compact, trace, finalize)
+    line["gpu_launches"] = args.steps * launches_per_step(P, R, C0, L)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(sc, cam, args.cpu_sample_stride, False)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def launches_per_step(P, R, C0, L):
+    def sort_launches(n, cells):
+        if n <= 1:
+            return 0
+        passes = (max(1, (cells - 1).bit_length()) + 7) // 8
+        return 2 + passes
+    build = (1 + 1 + sort_launches(P, C0) + 1      # count-scan, emit, sort, top ranges
+             + 1 + 1 + 1 + sort_launches(R, L) + 1)  # leaf cells scan, leaf count scan, emit, sort, ranges
+    return build + 1 + 3                               # primary; AO compact + trace + finalize
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_shinobi(args)
+
+
+if __name__ == "__main__":
+    main()

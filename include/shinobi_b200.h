@@ -186,6 +186,12 @@ shn_status shn_trace_ao(const shn_grid* g, const shn_camera* cam, const shn_hits
                         uint32_t spp, float length, float offset, uint32_t seed, float* d_ao,
                         uint32_t* d_num_rays, void* stream);
 
+/* Work counters: when d_counters (2 x uint64, device) is non-NULL, later
+ * trace calls on this grid run counting variants of their kernels and add
+ * {cell visits, triangle tests} to it (for roofline accounting); NULL turns
+ * counting off.  Not part of the reference interface. */
+shn_status shn_grid_set_stats(shn_grid* g, uint64_t* d_counters);
+
 /* ---- path tracer --------------------------------------------------------------- */
 typedef struct shn_pt_params {
   uint32_t spp;              /* samples per pixel */

@@ -58,6 +58,8 @@ def lib():
         L.orc_build_two_level.argtypes = [vp, u32, vp, u32, vp, vp, f32, u32]
         L.orc_build_two_level.restype = vp
         L.orc_grid_free.argtypes = [vp]
+        L.orc_grid_from_arrays.argtypes = [i32, vp, vp, vp, vp, C.c_uint64, vp, C.c_uint64, vp, u32, vp, u32]
+        L.orc_grid_from_arrays.restype = vp
         L.orc_grid_info.argtypes = [vp, vp]
         for nm in ("orc_grid_cells", "orc_grid_leaves", "orc_grid_indices", "orc_grid_top_pairs"):
             getattr(L, nm).argtypes = [vp]
@@ -161,6 +163,34 @@ def build_two_level(vtx, idx, b, res, lambda_leaf: float, leaf_threshold: int = 
     h = lib().orc_build_two_level(_p(vtx), vtx.shape[0], _p(idx), idx.shape[0], _p(b), _p(r),
                                   lambda_leaf, leaf_threshold)
     return _wrap(h, 1, r, b)
+
+
+def grid_from_arrays(kind, b, res, cells, leaves, indices, vtx, idx) -> Grid:
+    """Oracle traversal over grid arrays built elsewhere (e.g. by the reference builder)."""
+    b, vtx, idx = _f32(b), _f32(vtx), _u32(idx)
+    r = np.ascontiguousarray(res, np.int32)
+    cells, indices = _u32(cells), _u32(indices)
+    leaves = _u32(leaves) if leaves is not None else np.zeros((0, 2), np.uint32)
+    h = lib().orc_grid_from_arrays(kind, _p(b), _p(r), _p(cells), _p(leaves), leaves.size // 2,
+                                   _p(indices), indices.size, _p(vtx), vtx.shape[0], _p(idx), idx.shape[0])
+    return Grid(kind, r, b, cells.reshape(-1, 2), leaves.reshape(-1, 2), indices, np.zeros(0, np.uint64), h)
+
+
+def ref_host_build(vtx, idx, b, res):
+    """The reference's TwoLevelGridBuilderHost::hostBuild (compiled in place) -> (cells, leaves, refs)."""
+    R = ref_lib()
+    if R is None:
+        raise RuntimeError("reference checker library not built (oracle/_ref)")
+    vtx, idx, b = _f32(vtx), _u32(idx), _f32(b)
+    sizes = np.zeros(3, np.uint64)
+    h = R.ref_host_build(_p(vtx), vtx.shape[0], _p(idx), idx.shape[0], int(res[0]), int(res[1]),
+                         int(res[2]), _p(b), _p(sizes))
+    cells = np.zeros((int(sizes[0]), 2), np.uint32)
+    leaves = np.zeros((int(sizes[1]), 2), np.uint32)
+    refs = np.zeros(int(sizes[2]), np.uint32)
+    R.ref_host_build_copy(h, _p(cells), _p(leaves), _p(refs))
+    R.ref_host_build_free(h)
+    return cells, leaves, refs
 
 
 def trace_closest(g: Grid, org, dirs, tmax=None):

@@ -387,6 +387,25 @@ orc_grid* orc_build_two_level(const float* vtx, uint32_t nv, const uint32_t* idx
   return G;
 }
 
+// Wrap grid arrays built elsewhere (e.g. by the reference's host builder) so
+// the DDA traversal can run over them.  kind 0: cells are [begin,end) ranges;
+// kind 1: cells are TwoLevelGridCell words and leaves are ranges.
+orc_grid* orc_grid_from_arrays(int kind, const float bounds[6], const int res[3],
+                               const uint32_t* cells, const uint32_t* leaves, uint64_t nleaves,
+                               const uint32_t* indices, uint64_t nrefs, const float* vtx,
+                               uint32_t nv, const uint32_t* idx, uint32_t nt) {
+  orc_grid* G = new orc_grid();
+  G->kind = kind;
+  G->g = make_geom(bounds, res);
+  const size_t C = (size_t)res[0] * res[1] * res[2];
+  G->cells.assign(cells, cells + 2 * C);
+  if (kind == 1) G->leaves.assign(leaves, leaves + 2 * nleaves);
+  G->indices.assign(indices, indices + nrefs);
+  G->vtx.assign(vtx, vtx + 3 * (size_t)nv);
+  G->idx.assign(idx, idx + 3 * (size_t)nt);
+  return G;
+}
+
 void orc_grid_free(orc_grid* G) { delete G; }
 
 void orc_grid_info(const orc_grid* G, uint64_t out[8]) {

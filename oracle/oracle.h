@@ -15,6 +15,10 @@ orc_grid* orc_build_uniform(const float* vtx, uint32_t nv, const uint32_t* idx, 
 orc_grid* orc_build_two_level(const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
                               const float bounds[6], const int res[3], float lambda_leaf,
                               uint32_t leaf_threshold);
+orc_grid* orc_grid_from_arrays(int kind, const float bounds[6], const int res[3],
+                               const uint32_t* cells, const uint32_t* leaves, uint64_t nleaves,
+                               const uint32_t* indices, uint64_t nrefs, const float* vtx,
+                               uint32_t nv, const uint32_t* idx, uint32_t nt);
 void orc_grid_free(orc_grid* g);
 void orc_grid_info(const orc_grid* g, uint64_t out[8]);
 const uint32_t* orc_grid_cells(const orc_grid* g);

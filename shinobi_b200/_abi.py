@@ -77,6 +77,7 @@ SIGNATURES = {
     "shn_trace_any": ([vp, C.POINTER(Rays), u32, vp, vp], i32),
     "shn_trace_primary": ([vp, C.POINTER(Camera), u32, C.POINTER(Hits), vp], i32),
     "shn_trace_ao": ([vp, C.POINTER(Camera), C.POINTER(Hits), u32, f32, f32, u32, vp, vp, vp], i32),
+    "shn_grid_set_stats": ([vp, vp], i32),
     "shn_pt_params_default": ([C.POINTER(PtParams)], None),
     "shn_pt_render": ([vp, vp, C.POINTER(Camera), C.POINTER(PtParams), vp, vp, vp], i32),
     "shn_exclusive_scan_u32": ([vp, vp, vp, u32, vp], i32),

@@ -70,6 +70,8 @@ struct shn_grid {
   // scene the grid was built over (triangles by id, for shading / AO frames)
   const float4* src_tri = nullptr;
   uint32_t src_nt = 0;
+  // optional device counters {cell visits, triangle tests} of the stats kernels
+  unsigned long long* stats = nullptr;
 };
 
 namespace shn {

@@ -17,6 +17,22 @@ struct RaysView {
   const float *ox, *oy, *oz, *dx, *dy, *dz, *tmax;
 };
 
+// Work counters of the stats variants: {cell visits, triangle tests}, warp-aggregated.
+template <bool STATS>
+SHN_D void add_stats(unsigned long long* stats, const Hit& h, bool valid) {
+  if (!STATS) return;
+  unsigned long long s = valid ? h.steps : 0u, t = valid ? h.tests : 0u;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+    t += __shfl_xor_sync(0xFFFFFFFFu, t, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(stats, s);
+    atomicAdd(stats + 1, t);
+  }
+}
+
 SHN_D bool next_batch(uint32_t* counter, uint32_t n, uint32_t& base) {
   const int lane = threadIdx.x & 31;
   uint32_t b = 0;
@@ -25,18 +41,19 @@ SHN_D bool next_batch(uint32_t* counter, uint32_t n, uint32_t& base) {
   return base < n;
 }
 
-template <int KIND, bool ANY>
+template <int KIND, bool ANY, bool STATS>
 __global__ void __launch_bounds__(kTraceBlock) k_trace_rays(GridView G, RaysView R, uint32_t n,
                                                             uint32_t* counter, uint32_t* otri,
                                                             float* ot, float* ou, float* ov,
-                                                            uint8_t* occ) {
+                                                            uint8_t* occ, unsigned long long* stats) {
   uint32_t base;
   while (next_batch(counter, n, base)) {
     const uint32_t i = base + (threadIdx.x & 31);
+    Hit h{FLT_MAX, kMiss, 0.f, 0.f};
     if (i < n) {
       const V3 o = mk(R.ox[i], R.oy[i], R.oz[i]);
       const V3 d = mk(R.dx[i], R.dy[i], R.dz[i]);
-      Hit h{R.tmax ? R.tmax[i] : FLT_MAX, kMiss, 0.f, 0.f};
+      h.t = R.tmax ? R.tmax[i] : FLT_MAX;
       trace_ray<KIND, ANY>(G, o, d, h);
       if (ANY) {
         occ[i] = h.tri != kMiss ? 1 : 0;
@@ -47,26 +64,29 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_rays(GridView G, RaysView
         if (ov) ov[i] = h.v;
       }
     }
+    add_stats<STATS>(stats, h, i < n);
   }
 }
 
-template <int KIND>
+template <int KIND, bool STATS>
 __global__ void __launch_bounds__(kTraceBlock) k_trace_camera(GridView G, CamView cam,
                                                               uint32_t image_id, uint32_t n,
                                                               uint32_t* counter, uint32_t* otri,
-                                                              float* ot, float* ou, float* ov) {
+                                                              float* ot, float* ou, float* ov,
+                                                              unsigned long long* stats) {
   uint32_t base;
   while (next_batch(counter, n, base)) {
     const uint32_t i = base + (threadIdx.x & 31);
+    Hit h{FLT_MAX, kMiss, 0.f, 0.f};
     if (i < n) {
       const V3 d = primary_dir(cam, i, image_id);
-      Hit h{FLT_MAX, kMiss, 0.f, 0.f};
       trace_ray<KIND, false>(G, cam.eye, d, h);
       otri[i] = h.tri;
       ot[i] = h.t;
       if (ou) ou[i] = h.u;
       if (ov) ov[i] = h.v;
     }
+    add_stats<STATS>(stats, h, i < n);
   }
 }
 
@@ -93,17 +113,19 @@ struct AoParams {
   uint32_t snt;
 };
 
-template <int KIND>
+template <int KIND, bool STATS>
 __global__ void __launch_bounds__(kTraceBlock) k_trace_ao(GridView G, AoParams A,
                                                           const uint32_t* __restrict__ ptri,
                                                           const float* __restrict__ pt,
                                                           const uint32_t* __restrict__ hit_idx,
                                                           const uint32_t* d_m, uint32_t* counter,
-                                                          uint8_t* __restrict__ occ) {
+                                                          uint8_t* __restrict__ occ,
+                                                          unsigned long long* stats) {
   const uint32_t n = (*d_m) * A.spp;
   uint32_t base;
   while (next_batch(counter, n, base)) {
     const uint32_t r = base + (threadIdx.x & 31);
+    Hit h{A.len, kMiss, 0.f, 0.f};
     if (r < n) {
       const uint32_t k = r / A.spp, s = r - k * A.spp;
       const uint32_t p = hit_idx[k];
@@ -128,10 +150,10 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_ao(GridView G, AoParams A
       const float lx = sn * rr, ly = cs * rr, lz = sqrtf(u2);
       const V3 dir = mk(tx.x * lx + ty.x * ly + nn.x * lz, tx.y * lx + ty.y * ly + nn.y * lz,
                         tx.z * lx + ty.z * ly + nn.z * lz);
-      Hit h{A.len, kMiss, 0.f, 0.f};
       trace_ray<KIND, true>(G, o, dir, h);
       occ[r] = h.tri != kMiss ? 1 : 0;
     }
+    add_stats<STATS>(stats, h, r < n);
   }
 }
 
@@ -227,6 +249,12 @@ using namespace shn;
 
 extern "C" {
 
+shn_status shn_grid_set_stats(shn_grid* g, uint64_t* d_counters) {
+  if (!g) return SHN_ERR_INVALID;
+  g->stats = (unsigned long long*)d_counters;
+  return SHN_OK;
+}
+
 shn_status shn_trace_closest(const shn_grid* g, const shn_rays* rays, uint32_t n, shn_hits* hits,
                              void* stream) {
   if (!g || !rays || !hits) return SHN_ERR_INVALID;
@@ -241,13 +269,19 @@ shn_status shn_trace_closest(const shn_grid* g, const shn_rays* rays, uint32_t n
   cudaMemsetAsync(counter, 0, 4, st);
   const GridView G = view_of(g);
   const RaysView R{rays->ox, rays->oy, rays->oz, rays->dx, rays->dy, rays->dz, rays->tmax};
-  if (g->kind == SHN_GRID_UNIFORM) {
-    static int blocks = persistent_blocks(k_trace_rays<0, false>, g->ctx->num_sms);
-    k_trace_rays<0, false><<<blocks, kTraceBlock, 0, st>>>(G, R, n, counter, hits->tri, hits->t, hits->u, hits->v, nullptr);
-  } else {
-    static int blocks = persistent_blocks(k_trace_rays<1, false>, g->ctx->num_sms);
-    k_trace_rays<1, false><<<blocks, kTraceBlock, 0, st>>>(G, R, n, counter, hits->tri, hits->t, hits->u, hits->v, nullptr);
+#define SHN_LAUNCH_RAYS(K, S)                                                                   \
+  {                                                                                             \
+    static int blocks = persistent_blocks(k_trace_rays<K, false, S>, g->ctx->num_sms);          \
+    k_trace_rays<K, false, S><<<blocks, kTraceBlock, 0, st>>>(G, R, n, counter, hits->tri,      \
+                                                            hits->t, hits->u, hits->v, nullptr, \
+                                                            g->stats);                          \
   }
+  if (g->kind == SHN_GRID_UNIFORM) {
+    if (g->stats) SHN_LAUNCH_RAYS(0, true) else SHN_LAUNCH_RAYS(0, false)
+  } else {
+    if (g->stats) SHN_LAUNCH_RAYS(1, true) else SHN_LAUNCH_RAYS(1, false)
+  }
+#undef SHN_LAUNCH_RAYS
   return check_launch(g->ctx, "trace_closest");
 }
 
@@ -256,6 +290,8 @@ shn_status shn_trace_any(const shn_grid* g, const shn_rays* rays, uint32_t n, ui
   if (!g || !rays || !d_occluded) return SHN_ERR_INVALID;
   if (!g->built) return set_error(g->ctx, SHN_ERR_NOT_BUILT, "grid not built");
   if (n == 0) return SHN_OK;
+  if (!rays->ox || !rays->oy || !rays->oz || !rays->dx || !rays->dy || !rays->dz)
+    return set_error(g->ctx, SHN_ERR_INVALID, "null ray array");
   cudaStream_t st = (cudaStream_t)stream;
   Scratch S{g->ctx, st};
   uint32_t* counter = S.get<uint32_t>(1);
@@ -263,13 +299,19 @@ shn_status shn_trace_any(const shn_grid* g, const shn_rays* rays, uint32_t n, ui
   cudaMemsetAsync(counter, 0, 4, st);
   const GridView G = view_of(g);
   const RaysView R{rays->ox, rays->oy, rays->oz, rays->dx, rays->dy, rays->dz, rays->tmax};
-  if (g->kind == SHN_GRID_UNIFORM) {
-    static int blocks = persistent_blocks(k_trace_rays<0, true>, g->ctx->num_sms);
-    k_trace_rays<0, true><<<blocks, kTraceBlock, 0, st>>>(G, R, n, counter, nullptr, nullptr, nullptr, nullptr, d_occluded);
-  } else {
-    static int blocks = persistent_blocks(k_trace_rays<1, true>, g->ctx->num_sms);
-    k_trace_rays<1, true><<<blocks, kTraceBlock, 0, st>>>(G, R, n, counter, nullptr, nullptr, nullptr, nullptr, d_occluded);
+#define SHN_LAUNCH_ANY(K, S)                                                                    \
+  {                                                                                             \
+    static int blocks = persistent_blocks(k_trace_rays<K, true, S>, g->ctx->num_sms);           \
+    k_trace_rays<K, true, S><<<blocks, kTraceBlock, 0, st>>>(G, R, n, counter, nullptr, nullptr, \
+                                                           nullptr, nullptr, d_occluded,        \
+                                                           g->stats);                           \
   }
+  if (g->kind == SHN_GRID_UNIFORM) {
+    if (g->stats) SHN_LAUNCH_ANY(0, true) else SHN_LAUNCH_ANY(0, false)
+  } else {
+    if (g->stats) SHN_LAUNCH_ANY(1, true) else SHN_LAUNCH_ANY(1, false)
+  }
+#undef SHN_LAUNCH_ANY
   return check_launch(g->ctx, "trace_any");
 }
 
@@ -288,13 +330,18 @@ shn_status shn_trace_primary(const shn_grid* g, const shn_camera* cam, uint32_t 
   cudaMemsetAsync(counter, 0, 4, st);
   const GridView G = view_of(g);
   const CamView C = make_camera(cam);
-  if (g->kind == SHN_GRID_UNIFORM) {
-    static int blocks = persistent_blocks(k_trace_camera<0>, g->ctx->num_sms);
-    k_trace_camera<0><<<blocks, kTraceBlock, 0, st>>>(G, C, image_id, n, counter, hits->tri, hits->t, hits->u, hits->v);
-  } else {
-    static int blocks = persistent_blocks(k_trace_camera<1>, g->ctx->num_sms);
-    k_trace_camera<1><<<blocks, kTraceBlock, 0, st>>>(G, C, image_id, n, counter, hits->tri, hits->t, hits->u, hits->v);
+#define SHN_LAUNCH_CAM(K, S)                                                                    \
+  {                                                                                             \
+    static int blocks = persistent_blocks(k_trace_camera<K, S>, g->ctx->num_sms);               \
+    k_trace_camera<K, S><<<blocks, kTraceBlock, 0, st>>>(G, C, image_id, n, counter, hits->tri, \
+                                                       hits->t, hits->u, hits->v, g->stats);    \
   }
+  if (g->kind == SHN_GRID_UNIFORM) {
+    if (g->stats) SHN_LAUNCH_CAM(0, true) else SHN_LAUNCH_CAM(0, false)
+  } else {
+    if (g->stats) SHN_LAUNCH_CAM(1, true) else SHN_LAUNCH_CAM(1, false)
+  }
+#undef SHN_LAUNCH_CAM
   return check_launch(g->ctx, "trace_primary");
 }
 
@@ -332,13 +379,18 @@ shn_status shn_trace_ao(const shn_grid* g, const shn_camera* cam, const shn_hits
   A.offset = offset;
   A.stri = g->src_tri;
   A.snt = g->src_nt;
-  if (g->kind == SHN_GRID_UNIFORM) {
-    static int blocks = persistent_blocks(k_trace_ao<0>, g->ctx->num_sms);
-    k_trace_ao<0><<<blocks, kTraceBlock, 0, st>>>(G, A, primary->tri, primary->t, hit_idx, d_m, counter, occ);
-  } else {
-    static int blocks = persistent_blocks(k_trace_ao<1>, g->ctx->num_sms);
-    k_trace_ao<1><<<blocks, kTraceBlock, 0, st>>>(G, A, primary->tri, primary->t, hit_idx, d_m, counter, occ);
+#define SHN_LAUNCH_AO(K, S)                                                                       \
+  {                                                                                               \
+    static int blocks = persistent_blocks(k_trace_ao<K, S>, g->ctx->num_sms);                     \
+    k_trace_ao<K, S><<<blocks, kTraceBlock, 0, st>>>(G, A, primary->tri, primary->t, hit_idx, d_m, \
+                                                   counter, occ, g->stats);                       \
   }
+  if (g->kind == SHN_GRID_UNIFORM) {
+    if (g->stats) SHN_LAUNCH_AO(0, true) else SHN_LAUNCH_AO(0, false)
+  } else {
+    if (g->stats) SHN_LAUNCH_AO(1, true) else SHN_LAUNCH_AO(1, false)
+  }
+#undef SHN_LAUNCH_AO
   k_ao_finalize<<<(n + 255) / 256, 256, 0, st>>>(primary->tri, pos, occ, n, spp, d_m, d_ao, d_num_rays);
   return check_launch(g->ctx, "trace_ao");
 }

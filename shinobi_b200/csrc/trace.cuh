@@ -32,6 +32,7 @@ struct Hit {
   float t;
   uint32_t tri;
   float u, v;
+  uint32_t steps = 0, tests = 0;  // work counters (only read by the stats variants)
 };
 
 // Watertight ray/triangle test (Woop, Benthin, Wald, JCGT 2(1), 2013).
@@ -94,7 +95,9 @@ SHN_D bool wt_test(const RayWT& r, float4 p0, float4 p1, float4 p2, float tmin, 
 
 template <bool ANY>
 SHN_D bool test_range(const GridView& G, const RayWT& r, uint32_t b, uint32_t e, Hit& h) {
+  h.steps += 1;
   for (uint32_t it = b; it < e; ++it) {
+    h.tests += 1;
     const float4 p0 = __ldg(G.rv0 + it);
     const float4 p1 = __ldg(G.rv1 + it);
     const float4 p2 = __ldg(G.rv2 + it);
