@@ -219,6 +219,20 @@ shn_status shn_pt_render(const shn_grid* g, const shn_scene* s, const shn_camera
  * Single-pass decoupled look-back.  n < 2^31. */
 shn_status shn_exclusive_scan_u32(shn_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t n,
                                   void* stream);
+/* Same result as shn_exclusive_scan_u32, for callers that cannot allocate
+ * device memory on this path (an engine that has pre-claimed all device
+ * memory for its own allocator, or a loop whose memory budget is already
+ * committed): the look-back scratch lives in a fixed file-scope device array
+ * of about 64 KiB held by every GPU that loads the library, not in a pool.
+ * n <= 2^24 (SHN_SCAN_NOALLOC_MAX_N), larger n returns SHN_ERR_INVALID.  All
+ * calls on a device share that array: calls whose work overlaps on the GPU
+ * race, so order them on one stream.  The first call on each device looks up
+ * the array's device address (cudaGetSymbolAddress, with that device
+ * current); make it before any stream capture.  No counterpart in the
+ * reference. */
+#define SHN_SCAN_NOALLOC_MAX_N (1u << 24)
+shn_status shn_exclusive_scan_u32_noalloc(const uint32_t* d_in, uint32_t* d_out, uint32_t n,
+                                          void* stream);
 /* Stable compaction: d_out_idx[0..m) = indices i with d_flags[i] != 0, in
  * order; *d_count = m (device). */
 shn_status shn_compact_u32(shn_ctx* ctx, const uint32_t* d_flags, uint32_t n, uint32_t* d_out_idx,

@@ -81,6 +81,7 @@ SIGNATURES = {
     "shn_pt_params_default": ([C.POINTER(PtParams)], None),
     "shn_pt_render": ([vp, vp, C.POINTER(Camera), C.POINTER(PtParams), vp, vp, vp], i32),
     "shn_exclusive_scan_u32": ([vp, vp, vp, u32, vp], i32),
+    "shn_exclusive_scan_u32_noalloc": ([vp, vp, u32, vp], i32),
     "shn_compact_u32": ([vp, vp, u32, vp, vp, vp], i32),
     "shn_sort_keys_u64": ([vp, vp, vp, u32, u32, u32, vp], i32),
 }
