@@ -6,6 +6,7 @@
 // generated from compacted primary hits.
 #include "internal.h"
 #include "trace.cuh"
+#include "trace_coop.cuh"
 
 namespace shn {
 
@@ -41,31 +42,36 @@ SHN_D bool next_batch(uint32_t* counter, uint32_t n, uint32_t& base) {
   return base < n;
 }
 
+template <bool STATS>
+SHN_D void add_counts(unsigned long long* stats, uint32_t steps, uint32_t tests) {
+  if (!STATS) return;
+  atomicAdd(stats, (unsigned long long)steps);
+  atomicAdd(stats + 1, (unsigned long long)tests);
+}
+
 template <int KIND, bool ANY, bool STATS>
 __global__ void __launch_bounds__(kTraceBlock) k_trace_rays(GridView G, RaysView R, uint32_t n,
                                                             uint32_t* counter, uint32_t* otri,
                                                             float* ot, float* ou, float* ov,
                                                             uint8_t* occ, unsigned long long* stats) {
-  uint32_t base;
-  while (next_batch(counter, n, base)) {
-    const uint32_t i = base + (threadIdx.x & 31);
-    Hit h{FLT_MAX, kMiss, 0.f, 0.f};
-    if (i < n) {
-      const V3 o = mk(R.ox[i], R.oy[i], R.oz[i]);
-      const V3 d = mk(R.dx[i], R.dy[i], R.dz[i]);
-      h.t = R.tmax ? R.tmax[i] : FLT_MAX;
-      trace_ray<KIND, ANY>(G, o, d, h);
-      if (ANY) {
-        occ[i] = h.tri != kMiss ? 1 : 0;
-      } else {
-        otri[i] = h.tri;
-        ot[i] = h.t;
-        if (ou) ou[i] = h.u;
-        if (ov) ov[i] = h.v;
-      }
-    }
-    add_stats<STATS>(stats, h, i < n);
-  }
+  warp_trace<KIND, ANY>(
+      G, n, counter,
+      [&](uint32_t i, V3& o, V3& d, float& tmax) {
+        o = mk(R.ox[i], R.oy[i], R.oz[i]);
+        d = mk(R.dx[i], R.dy[i], R.dz[i]);
+        tmax = R.tmax ? R.tmax[i] : FLT_MAX;
+      },
+      [&](uint32_t i, const Hit& h, uint32_t steps, uint32_t tests) {
+        if (ANY) {
+          occ[i] = h.tri != kMiss ? 1 : 0;
+        } else {
+          otri[i] = h.tri;
+          ot[i] = h.t;
+          if (ou) ou[i] = h.u;
+          if (ov) ov[i] = h.v;
+        }
+        add_counts<STATS>(stats, steps, tests);
+      });
 }
 
 template <int KIND, bool STATS>
@@ -74,20 +80,20 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_camera(GridView G, CamVie
                                                               uint32_t* counter, uint32_t* otri,
                                                               float* ot, float* ou, float* ov,
                                                               unsigned long long* stats) {
-  uint32_t base;
-  while (next_batch(counter, n, base)) {
-    const uint32_t i = base + (threadIdx.x & 31);
-    Hit h{FLT_MAX, kMiss, 0.f, 0.f};
-    if (i < n) {
-      const V3 d = primary_dir(cam, i, image_id);
-      trace_ray<KIND, false>(G, cam.eye, d, h);
-      otri[i] = h.tri;
-      ot[i] = h.t;
-      if (ou) ou[i] = h.u;
-      if (ov) ov[i] = h.v;
-    }
-    add_stats<STATS>(stats, h, i < n);
-  }
+  warp_trace<KIND, false>(
+      G, n, counter,
+      [&](uint32_t i, V3& o, V3& d, float& tmax) {
+        o = cam.eye;
+        d = primary_dir(cam, i, image_id);
+        tmax = FLT_MAX;
+      },
+      [&](uint32_t i, const Hit& h, uint32_t steps, uint32_t tests) {
+        otri[i] = h.tri;
+        ot[i] = h.t;
+        if (ou) ou[i] = h.u;
+        if (ov) ov[i] = h.v;
+        add_counts<STATS>(stats, steps, tests);
+      });
 }
 
 // Compaction of hit pixels: hit_idx[k] = k-th pixel with a hit, pos[p] = its rank.
@@ -122,39 +128,38 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_ao(GridView G, AoParams A
                                                           uint8_t* __restrict__ occ,
                                                           unsigned long long* stats) {
   const uint32_t n = (*d_m) * A.spp;
-  uint32_t base;
-  while (next_batch(counter, n, base)) {
-    const uint32_t r = base + (threadIdx.x & 31);
-    Hit h{A.len, kMiss, 0.f, 0.f};
-    if (r < n) {
-      const uint32_t k = r / A.spp, s = r - k * A.spp;
-      const uint32_t p = hit_idx[k];
-      const uint32_t tri = ptri[p];
-      const float t = pt[p];
-      const V3 d = primary_dir(A.cam, p, A.image_id);
-      const V3 v0 = f4v(__ldg(A.stri + tri));
-      const V3 v1 = f4v(__ldg(A.stri + A.snt + tri));
-      const V3 v2 = f4v(__ldg(A.stri + 2 * (size_t)A.snt + tri));
-      const V3 e1 = sub(v1, v0);
-      V3 nn = normalize(cross(e1, sub(v2, v0)));
-      if (dot(nn, d) > 0.f) nn = mk(-nn.x, -nn.y, -nn.z);
-      const V3 tx = normalize(e1);
-      const V3 ty = cross(nn, tx);
-      const V3 hp = add(A.cam.eye, muls(d, t));
-      const V3 o = add(hp, muls(nn, A.offset));
-      const uint4 w = philox4x32(make_uint4(p, s, 0u, 0x414Fu), A.seed, 0u);
-      const float u1 = u01(w.x), u2 = u01(w.y);
-      float sn, cs;
-      sincos_2pi(u1, sn, cs);
-      const float rr = sqrtf(1.f - u2);
-      const float lx = sn * rr, ly = cs * rr, lz = sqrtf(u2);
-      const V3 dir = mk(tx.x * lx + ty.x * ly + nn.x * lz, tx.y * lx + ty.y * ly + nn.y * lz,
-                        tx.z * lx + ty.z * ly + nn.z * lz);
-      trace_ray<KIND, true>(G, o, dir, h);
-      occ[r] = h.tri != kMiss ? 1 : 0;
-    }
-    add_stats<STATS>(stats, h, r < n);
-  }
+  warp_trace<KIND, true>(
+      G, n, counter,
+      [&](uint32_t r, V3& o, V3& dir, float& tmax) {
+        const uint32_t k = r / A.spp, s = r - k * A.spp;
+        const uint32_t p = hit_idx[k];
+        const uint32_t tri = ptri[p];
+        const float t = pt[p];
+        const V3 d = primary_dir(A.cam, p, A.image_id);
+        const V3 v0 = f4v(__ldg(A.stri + tri));
+        const V3 v1 = f4v(__ldg(A.stri + A.snt + tri));
+        const V3 v2 = f4v(__ldg(A.stri + 2 * (size_t)A.snt + tri));
+        const V3 e1 = sub(v1, v0);
+        V3 nn = normalize(cross(e1, sub(v2, v0)));
+        if (dot(nn, d) > 0.f) nn = mk(-nn.x, -nn.y, -nn.z);
+        const V3 tx = normalize(e1);
+        const V3 ty = cross(nn, tx);
+        const V3 hp = add(A.cam.eye, muls(d, t));
+        o = add(hp, muls(nn, A.offset));
+        const uint4 w = philox4x32(make_uint4(p, s, 0u, 0x414Fu), A.seed, 0u);
+        const float u1 = u01(w.x), u2 = u01(w.y);
+        float sn, cs;
+        sincos_2pi(u1, sn, cs);
+        const float rr = sqrtf(1.f - u2);
+        const float lx = sn * rr, ly = cs * rr, lz = sqrtf(u2);
+        dir = mk(tx.x * lx + ty.x * ly + nn.x * lz, tx.y * lx + ty.y * ly + nn.y * lz,
+                 tx.z * lx + ty.z * ly + nn.z * lz);
+        tmax = A.len;
+      },
+      [&](uint32_t r, const Hit& h, uint32_t steps, uint32_t tests) {
+        occ[r] = h.tri != kMiss ? 1 : 0;
+        add_counts<STATS>(stats, steps, tests);
+      });
 }
 
 __global__ void k_ao_finalize(const uint32_t* __restrict__ ptri, const uint32_t* __restrict__ pos,

@@ -1,0 +1,408 @@
+// Warp-cooperative traversal engine.
+//
+// Every lane owns one ray and walks the grid with an explicit DDA state
+// machine, so the lanes of a warp reach "here is my next cell range" at the
+// same point of the loop.  The ranges are then tested in two phases:
+//  * small ranges (<= kCoopThreshold references): each lane tests its own
+//    range, as the reference's SimpleIntersector does;
+//  * large ranges: the whole warp tests one lane's range, 32 triangles per
+//    instruction, with that lane's ray broadcast (warp-uniform, so the
+//    watertight test's axis permutation is a compile-time constant), and the
+//    closest hit is reduced across the warp.  This generalises the
+//    reference's HybridIntersector work donation
+//    (src/Intersector/HybridIntersector.hpp:472-704) and keeps lanes busy
+//    when one ray sits in a cell with tens of thousands of references.
+// Lanes whose ray has finished take a new ray from the global pool at the
+// top of the loop (persistent threads with per-lane replenishment).
+//
+// The per-ray sequence of cell visits, tests and continuation decisions is
+// exactly that of trace_uniform / trace_two_level (trace.cuh); the closest
+// hit is the argmin of (t, reference index) over the tested references, the
+// same winner the sequential strict-< loop keeps, so results are identical.
+#pragma once
+#include "trace.cuh"
+
+namespace shn {
+
+constexpr uint32_t kCoopThreshold = 32;
+
+enum : uint32_t { ST_DONE = 0, ST_TOP = 1, ST_LEAF = 2, ST_LEAF_TESTED = 3, ST_TOP_NEXT = 4, ST_U_TESTED = 5 };
+
+struct Lane {
+  V3 org, rcp;
+  float Sx, Sy, Sz;
+  uint32_t perm;          // kx | ky << 2 | kz << 4
+  float tbest;
+  uint32_t best;          // reference index of the best hit, kMiss if none
+  V3 cell, tMax;
+  float tEntry;
+  int vis, cap;
+  V3 sc, sMax, scs, cres;
+  uint32_t lb;
+  int vis2;
+  uint32_t b, e;
+  uint32_t st;
+};
+
+SHN_D RayWT lane_ray(const Lane& L) {
+  RayWT r;
+  r.org = L.org;
+  r.kx = L.perm & 3;
+  r.ky = (L.perm >> 2) & 3;
+  r.kz = (L.perm >> 4) & 3;
+  r.Sx = L.Sx;
+  r.Sy = L.Sy;
+  r.Sz = L.Sz;
+  return r;
+}
+
+template <int KIND>
+SHN_D void lane_init(const GridView& G, Lane& L, V3 org, V3 dir, float tmax) {
+  const Geom& g = G.g;
+  L.org = org;
+  L.rcp = divv(mk(1.f, 1.f, 1.f), dir);
+  const RayWT w = wt_setup(org, dir);
+  L.Sx = w.Sx;
+  L.Sy = w.Sy;
+  L.Sz = w.Sz;
+  L.perm = (uint32_t)w.kx | ((uint32_t)w.ky << 2) | ((uint32_t)w.kz << 4);
+  L.tbest = tmax;
+  L.best = kMiss;
+  L.st = ST_DONE;
+  L.b = L.e = 0;
+  if (!(L.tbest > 0.f)) return;
+  const V3 rcp = L.rcp;
+  const V3 t1 = mul(sub(g.gmin, org), rcp);
+  V3 t2 = mul(sub(g.gmax, org), rcp);
+  const V3 tmn = vmin(t1, t2);
+  t2 = vmax(t1, t2);
+  float tEntry = fmaxf(fmaxf(tmn.x, tmn.y), tmn.z);
+  const float tExit = fminf(fminf(t2.x, t2.y), t2.z);
+  if (tExit <= tEntry || tExit < 0.f) return;
+  V3 entry;
+  if (KIND == 0) {
+    const float te = tEntry + kEps;
+    entry = (tEntry >= 0.f) ? add(org, divv(mk(te, te, te), rcp)) : org;
+  } else {
+    tEntry = fmaxf(0.f, tEntry);
+    const float te = tEntry + kEps;
+    entry = add(org, divv(mk(te, te, te), rcp));
+  }
+  L.tEntry = tEntry;
+  V3 cell = mul(sub(entry, g.gmin), g.rcpTrav);
+  cell = mk(floorf(cell.x), floorf(cell.y), floorf(cell.z));
+  const V3 tmp = mk(rcp.x > 0.f ? 1.f : 0.f, rcp.y > 0.f ? 1.f : 0.f, rcp.z > 0.f ? 1.f : 0.f);
+  L.cell = cell;
+  L.tMax = mul(sub(add(mul(add(cell, tmp), g.cs), g.gmin), org), rcp);
+  const bool valid = (cell.x != (rcp.x > 0.f ? g.resf.x : -1.f)) &&
+                     (cell.y != (rcp.y > 0.f ? g.resf.y : -1.f)) &&
+                     (cell.z != (rcp.z > 0.f ? g.resf.z : -1.f));
+  L.vis = 0;
+  L.cap = g.res[0] + g.res[1] + g.res[2] + 3;
+  L.st = valid ? ST_TOP : ST_DONE;
+}
+
+// Runs the lane's state machine until it has a non-empty range to test
+// (returns true, range in L.b/L.e) or the ray is finished (returns false).
+template <int KIND, bool ANY>
+SHN_D bool lane_advance(const GridView& G, Lane& L, uint32_t& steps) {
+  const Geom& g = G.g;
+  while (true) {
+    switch (L.st) {
+      case ST_TOP: {
+        L.vis++;
+        const uint32_t cx = (uint32_t)clampf(L.cell.x, 0.f, g.resf.x - 1.f);
+        const uint32_t cy = (uint32_t)clampf(L.cell.y, 0.f, g.resf.y - 1.f);
+        const uint32_t cz = (uint32_t)clampf(L.cell.z, 0.f, g.resf.z - 1.f);
+        const uint2 cw = __ldg(G.cells + (cx + cy * (uint32_t)g.res[0] + cz * (uint32_t)g.res[0] * (uint32_t)g.res[1]));
+        steps++;
+        if (KIND == 0) {
+          L.b = cw.x;
+          L.e = cw.y;
+          L.st = ST_U_TESTED;
+          if (L.e > L.b) return true;
+          break;
+        }
+        if (cw.y & kNotEmpty) {
+          const V3 rcp = L.rcp, org = L.org;
+          const float te = L.tEntry;
+          const V3 ent = add(org, divv(mk(te, te, te), rcp));
+          const V3 cres = mk((float)(cw.y & 0xFFu), (float)((cw.y >> 8) & 0xFFu), (float)((cw.y >> 16) & 0xFFu));
+          const V3 subRCP = mul(g.rcpTrav, cres);
+          const V3 minB = add(mul(L.cell, g.cs), g.gmin);
+          V3 sc;
+          sc.x = floorf((ent.x - minB.x) * subRCP.x);
+          sc.y = floorf((ent.y - minB.y) * subRCP.y);
+          sc.z = floorf((ent.z - minB.z) * subRCP.z);
+          const V3 scs = divv(mk(1.f, 1.f, 1.f), subRCP);
+          sc = vmin(sub(cres, mk(1.f, 1.f, 1.f)), vmax(sc, mk(0.f, 0.f, 0.f)));
+          const V3 tmp = mk(rcp.x > 0.f ? 1.f : 0.f, rcp.y > 0.f ? 1.f : 0.f, rcp.z > 0.f ? 1.f : 0.f);
+          L.sMax.x = ((sc.x + tmp.x) * scs.x + minB.x - org.x) * rcp.x;
+          L.sMax.y = ((sc.y + tmp.y) * scs.y + minB.y - org.y) * rcp.y;
+          L.sMax.z = ((sc.z + tmp.z) * scs.z + minB.z - org.z) * rcp.z;
+          L.sc = sc;
+          L.scs = scs;
+          L.cres = cres;
+          L.lb = cw.x;
+          L.vis2 = 0;
+          L.st = ST_LEAF;
+        } else {
+          L.st = ST_TOP_NEXT;
+        }
+        break;
+      }
+      case ST_LEAF: {
+        L.vis2++;
+        const V3 sc = L.sc, cres = L.cres;
+        const uint32_t li = L.lb + (uint32_t)(sc.x + cres.x * sc.y + cres.x * cres.y * sc.z);
+        const uint2 range = __ldg(G.leaves + li);
+        steps++;
+        L.b = range.x;
+        L.e = range.y;
+        L.st = ST_LEAF_TESTED;
+        if (L.e > L.b) return true;
+        break;
+      }
+      case ST_LEAF_TESTED: {
+        if (ANY && L.best != kMiss) {
+          L.st = ST_DONE;
+          return false;
+        }
+        const float tb = L.tbest;
+        bool v2 = tb > L.sMax.x || tb > L.sMax.y || tb > L.sMax.z;
+        if (!v2) {
+          L.st = ST_TOP_NEXT;
+          break;
+        }
+        const int d = min_dim(L.sMax);
+        const float rd = sel(d, L.rcp);
+        bump(L.sc, d, rd > 0.f ? 1.f : -1.f);
+        bump(L.sMax, d, sel(d, L.scs) * fabsf(rd));
+        const float cd = sel(d, L.sc);
+        v2 = !(fabsf(cd - sel(d, L.cres)) < 0.1f || fabsf(cd + 1.f) < 0.1f);
+        const int cap2 = (int)L.cres.x + (int)L.cres.y + (int)L.cres.z + 3;
+        L.st = (v2 && L.vis2 < cap2) ? ST_LEAF : ST_TOP_NEXT;
+        break;
+      }
+      case ST_U_TESTED:
+      case ST_TOP_NEXT: {
+        if (ANY && L.best != kMiss) {
+          L.st = ST_DONE;
+          return false;
+        }
+        const float tb = L.tbest;
+        bool valid = tb > L.tMax.x || tb > L.tMax.y || tb > L.tMax.z;
+        if (!valid) {
+          L.st = ST_DONE;
+          return false;
+        }
+        const int d = min_dim(L.tMax);
+        if (KIND == 1) L.tEntry = sel(d, L.tMax);
+        const float rd = sel(d, L.rcp);
+        bump(L.cell, d, rd > 0.f ? 1.f : -1.f);
+        bump(L.tMax, d, sel(d, g.cs) * fabsf(rd));
+        const float cd = sel(d, L.cell);
+        valid = !(fabsf(cd - sel(d, g.resf)) < 0.1f || fabsf(cd + 1.f) < 0.1f);
+        L.st = (valid && L.vis < L.cap) ? ST_TOP : ST_DONE;
+        if (L.st == ST_DONE) return false;
+        break;
+      }
+      default:
+        return false;
+    }
+  }
+}
+
+// ---- watertight test with a compile-time axis permutation ---------------------
+template <int K>
+SHN_D float cget(V3 v) {
+  return K == 0 ? v.x : (K == 1 ? v.y : v.z);
+}
+
+template <int KX, int KY, int KZ>
+SHN_D bool wt_test_p(V3 org, float Sx, float Sy, float Sz, float4 p0, float4 p1, float4 p2,
+                     float tmin, float tbest, float& t) {
+  const V3 A = sub(f4v(p0), org), B = sub(f4v(p1), org), C = sub(f4v(p2), org);
+  const float Akz = cget<KZ>(A), Bkz = cget<KZ>(B), Ckz = cget<KZ>(C);
+  const float Ax = cget<KX>(A) - Sx * Akz;
+  const float Ay = cget<KY>(A) - Sy * Akz;
+  const float Bx = cget<KX>(B) - Sx * Bkz;
+  const float By = cget<KY>(B) - Sy * Bkz;
+  const float Cx = cget<KX>(C) - Sx * Ckz;
+  const float Cy = cget<KY>(C) - Sy * Ckz;
+  float U = Cx * By - Cy * Bx;
+  float V = Ax * Cy - Ay * Cx;
+  float W = Bx * Ay - By * Ax;
+  if (U == 0.f || V == 0.f || W == 0.f) {
+    U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+    V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+    W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+  }
+  if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
+  const float det = U + V + W;
+  if (det == 0.f) return false;
+  const float T = U * (Sz * Akz) + V * (Sz * Bkz) + W * (Sz * Ckz);
+  const float tt = T / det;
+  if (!(tt > tmin && tt < tbest)) return false;
+  t = tt;
+  return true;
+}
+
+// Whole warp tests references [b, e) against one (warp-uniform) ray.
+// Closest: returns the packed argmin key (t bits << 32 | ref) in every lane,
+// or ~0 when nothing beats tbest.  Any: returns a hit ref or ~0.
+template <bool ANY, int KX, int KY, int KZ>
+SHN_D uint64_t warp_range_p(const GridView& G, V3 org, float Sx, float Sy, float Sz, float tbest,
+                            uint32_t b, uint32_t e, uint32_t& tests) {
+  const int lane = threadIdx.x & 31;
+  uint64_t key = ~0ull;
+  float tb = tbest;
+  for (uint32_t base = b; base < e; base += 32) {
+    const uint32_t it = base + lane;
+    bool hit = false;
+    if (it < e) {
+      const float4 p0 = __ldg(G.rv0 + it);
+      const float4 p1 = __ldg(G.rv1 + it);
+      const float4 p2 = __ldg(G.rv2 + it);
+      float t;
+      if (wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, p0, p1, p2, kEps, tb, t)) {
+        tb = t;
+        key = ((uint64_t)__float_as_uint(t) << 32) | it;
+        hit = true;
+      }
+    }
+    tests += min(32u, e - base);
+    if (ANY && __any_sync(0xFFFFFFFFu, hit)) break;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint64_t other = __shfl_xor_sync(0xFFFFFFFFu, key, o);
+    key = other < key ? other : key;
+  }
+  return key;
+}
+
+template <bool ANY>
+SHN_D uint64_t warp_range(const GridView& G, uint32_t perm, V3 org, float Sx, float Sy, float Sz,
+                          float tbest, uint32_t b, uint32_t e, uint32_t& tests) {
+  switch (perm) {
+    case (1u | 2u << 2 | 0u << 4): return warp_range_p<ANY, 1, 2, 0>(G, org, Sx, Sy, Sz, tbest, b, e, tests);
+    case (2u | 1u << 2 | 0u << 4): return warp_range_p<ANY, 2, 1, 0>(G, org, Sx, Sy, Sz, tbest, b, e, tests);
+    case (2u | 0u << 2 | 1u << 4): return warp_range_p<ANY, 2, 0, 1>(G, org, Sx, Sy, Sz, tbest, b, e, tests);
+    case (0u | 2u << 2 | 1u << 4): return warp_range_p<ANY, 0, 2, 1>(G, org, Sx, Sy, Sz, tbest, b, e, tests);
+    case (0u | 1u << 2 | 2u << 4): return warp_range_p<ANY, 0, 1, 2>(G, org, Sx, Sy, Sz, tbest, b, e, tests);
+    default:                        return warp_range_p<ANY, 1, 0, 2>(G, org, Sx, Sy, Sz, tbest, b, e, tests);
+  }
+}
+
+// Per-lane test of its own (small) range with the generic watertight test.
+template <bool ANY>
+SHN_D void lane_range(const GridView& G, Lane& L, uint32_t& tests) {
+  const RayWT w = lane_ray(L);
+  for (uint32_t it = L.b; it < L.e; ++it) {
+    tests++;
+    const float4 p0 = __ldg(G.rv0 + it);
+    const float4 p1 = __ldg(G.rv1 + it);
+    const float4 p2 = __ldg(G.rv2 + it);
+    float t, u, v;
+    if (wt_test(w, p0, p1, p2, kEps, L.tbest, t, u, v)) {
+      L.tbest = t;
+      L.best = it;
+      if (ANY) return;
+    }
+  }
+}
+
+// Final hit record of a lane: triangle id and barycentrics of the best
+// reference, recomputed with the same arithmetic.
+SHN_D void lane_result(const GridView& G, const Lane& L, Hit& h) {
+  h.t = L.tbest;
+  h.tri = kMiss;
+  h.u = h.v = 0.f;
+  if (L.best == kMiss) return;
+  const float4 p0 = __ldg(G.rv0 + L.best);
+  const float4 p1 = __ldg(G.rv1 + L.best);
+  const float4 p2 = __ldg(G.rv2 + L.best);
+  float t, u, v;
+  wt_test(lane_ray(L), p0, p1, p2, kEps, INFINITY, t, u, v);
+  h.tri = __float_as_uint(p0.w);
+  h.u = u;
+  h.v = v;
+}
+
+// The warp loop.  src(i, org, dir, tmax) generates ray i; sink(i, hit, steps, tests)
+// consumes its result.  n rays are taken from *counter (pre-zeroed).
+template <int KIND, bool ANY, class Src, class Sink>
+SHN_D void warp_trace(const GridView& G, uint32_t n, uint32_t* counter, Src&& src, Sink&& sink) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  Lane L;
+  L.st = ST_DONE;
+  bool has = false;
+  uint32_t rid = 0, steps = 0, tests = 0;
+  bool pool_empty = false;
+  while (true) {
+    const uint32_t idle = __ballot_sync(0xFFFFFFFFu, !has);
+    if (idle && !pool_empty) {
+      const uint32_t cnt = __popc(idle);
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(counter, cnt);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (base + cnt >= n) pool_empty = true;
+      if (!has) {
+        const uint32_t r = base + __popc(idle & lt);
+        if (r < n) {
+          rid = r;
+          has = true;
+          steps = tests = 0;
+          V3 o, d;
+          float tmax;
+          src(r, o, d, tmax);
+          lane_init<KIND>(G, L, o, d, tmax);
+        }
+      }
+    }
+    bool pending = false;
+    if (has) {
+      pending = lane_advance<KIND, ANY>(G, L, steps);
+      if (!pending) {
+        Hit h;
+        lane_result(G, L, h);
+        sink(rid, h, steps, tests);
+        has = false;
+      }
+    }
+    const uint32_t pmask = __ballot_sync(0xFFFFFFFFu, pending);
+    if (pmask == 0) {
+      if (pool_empty && __ballot_sync(0xFFFFFFFFu, has) == 0) break;
+      continue;
+    }
+    const bool big = pending && (L.e - L.b > kCoopThreshold);
+    if (pending && !big) lane_range<ANY>(G, L, tests);
+    uint32_t bmask = __ballot_sync(0xFFFFFFFFu, big);
+    while (bmask) {
+      const int j = __ffs(bmask) - 1;
+      bmask &= bmask - 1;
+      const V3 org = mk(__shfl_sync(0xFFFFFFFFu, L.org.x, j), __shfl_sync(0xFFFFFFFFu, L.org.y, j),
+                        __shfl_sync(0xFFFFFFFFu, L.org.z, j));
+      const float Sx = __shfl_sync(0xFFFFFFFFu, L.Sx, j);
+      const float Sy = __shfl_sync(0xFFFFFFFFu, L.Sy, j);
+      const float Sz = __shfl_sync(0xFFFFFFFFu, L.Sz, j);
+      const uint32_t perm = __shfl_sync(0xFFFFFFFFu, L.perm, j);
+      const float tb = __shfl_sync(0xFFFFFFFFu, L.tbest, j);
+      const uint32_t b = __shfl_sync(0xFFFFFFFFu, L.b, j);
+      const uint32_t e = __shfl_sync(0xFFFFFFFFu, L.e, j);
+      uint32_t wt = 0;
+      const uint64_t key = warp_range<ANY>(G, perm, org, Sx, Sy, Sz, tb, b, e, wt);
+      if (lane == j) {
+        tests += wt;
+        if (key != ~0ull) {
+          L.tbest = __uint_as_float((uint32_t)(key >> 32));
+          L.best = (uint32_t)key;
+        }
+      }
+    }
+  }
+}
+
+}  // namespace shn
