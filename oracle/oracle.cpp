@@ -458,15 +458,17 @@ inline WT wt_setup(V3 d) {
 inline bool wt_intersect(const WT& w, V3 org, const Tri& tri, float tmin, float tbest, float& t,
                          float& u, float& v) {
   const V3 A = sub(tri.v[0], org), B = sub(tri.v[1], org), C = sub(tri.v[2], org);
-  const float Ax = at(A, w.kx) - w.Sx * at(A, w.kz);
-  const float Ay = at(A, w.ky) - w.Sy * at(A, w.kz);
-  const float Bx = at(B, w.kx) - w.Sx * at(B, w.kz);
-  const float By = at(B, w.ky) - w.Sy * at(B, w.kz);
-  const float Cx = at(C, w.kx) - w.Sx * at(C, w.kz);
-  const float Cy = at(C, w.ky) - w.Sy * at(C, w.kz);
-  float U = Cx * By - Cy * Bx;
-  float V = Ax * Cy - Ay * Cx;
-  float W = Bx * Ay - By * Ax;
+  // shear with one fused multiply-add per coordinate; edge functions as one
+  // rounded product plus a fused multiply-add (fmaf is correctly rounded)
+  const float Ax = fmaf(-w.Sx, at(A, w.kz), at(A, w.kx));
+  const float Ay = fmaf(-w.Sy, at(A, w.kz), at(A, w.ky));
+  const float Bx = fmaf(-w.Sx, at(B, w.kz), at(B, w.kx));
+  const float By = fmaf(-w.Sy, at(B, w.kz), at(B, w.ky));
+  const float Cx = fmaf(-w.Sx, at(C, w.kz), at(C, w.kx));
+  const float Cy = fmaf(-w.Sy, at(C, w.kz), at(C, w.ky));
+  float U = fmaf(Cx, By, -(Cy * Bx));
+  float V = fmaf(Ax, Cy, -(Ay * Cx));
+  float W = fmaf(Bx, Ay, -(By * Ax));
   if (U == 0.f || V == 0.f || W == 0.f) {
     U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
     V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
@@ -478,7 +480,7 @@ inline bool wt_intersect(const WT& w, V3 org, const Tri& tri, float tmin, float 
   const float Az = w.Sz * at(A, w.kz);
   const float Bz = w.Sz * at(B, w.kz);
   const float Cz = w.Sz * at(C, w.kz);
-  const float T = U * Az + V * Bz + W * Cz;
+  const float T = fmaf(W, Cz, fmaf(V, Bz, U * Az));
   const float tt = T / det;
   if (!(tt > tmin && tt < tbest)) return false;
   t = tt;

@@ -90,14 +90,17 @@ _lib = None
 
 
 def load(auto_build: bool = True):
-    """Load libshinobi_b200.so (building it first when missing or stale)."""
+    """Load libshinobi_b200.so (building it first when missing or stale).
+
+    SHINOBI_B200_LIB may name another build of the library to load instead."""
     global _lib
     if _lib is None:
-        if auto_build and _build.stale():
+        path = os.environ.get("SHINOBI_B200_LIB", _build.LIB)
+        if path == _build.LIB and auto_build and _build.stale():
             _build.build()
-        if not os.path.exists(_build.LIB):
-            raise RuntimeError(f"libshinobi_b200.so not built ({_build.LIB})")
-        lib = C.CDLL(_build.LIB)
+        if not os.path.exists(path):
+            raise RuntimeError(f"libshinobi_b200.so not built ({path})")
+        lib = C.CDLL(path)
         for name, (args, res) in SIGNATURES.items():
             fn = getattr(lib, name)
             fn.argtypes = args

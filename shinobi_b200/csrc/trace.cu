@@ -34,14 +34,6 @@ SHN_D void add_stats(unsigned long long* stats, const Hit& h, bool valid) {
   }
 }
 
-SHN_D bool next_batch(uint32_t* counter, uint32_t n, uint32_t& base) {
-  const int lane = threadIdx.x & 31;
-  uint32_t b = 0;
-  if (lane == 0) b = atomicAdd(counter, 32u);
-  base = __shfl_sync(0xFFFFFFFFu, b, 0);
-  return base < n;
-}
-
 template <bool STATS>
 SHN_D void add_counts(unsigned long long* stats, uint32_t steps, uint32_t tests) {
   if (!STATS) return;
@@ -53,7 +45,8 @@ template <int KIND, bool ANY, bool STATS>
 __global__ void __launch_bounds__(kTraceBlock) k_trace_rays(GridView G, RaysView R, uint32_t n,
                                                             uint32_t* counter, uint32_t* otri,
                                                             float* ot, float* ou, float* ov,
-                                                            uint8_t* occ, unsigned long long* stats) {
+                                                            uint8_t* occ, unsigned long long* stats,
+                                                            uint32_t* err) {
   warp_trace<KIND, ANY>(
       G, n, counter,
       [&](uint32_t i, V3& o, V3& d, float& tmax) {
@@ -79,7 +72,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_camera(GridView G, CamVie
                                                               uint32_t image_id, uint32_t n,
                                                               uint32_t* counter, uint32_t* otri,
                                                               float* ot, float* ou, float* ov,
-                                                              unsigned long long* stats) {
+                                                              unsigned long long* stats,
+                                                              uint32_t* err) {
   warp_trace<KIND, false>(
       G, n, counter,
       [&](uint32_t i, V3& o, V3& d, float& tmax) {
@@ -126,7 +120,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_ao(GridView G, AoParams A
                                                           const uint32_t* __restrict__ hit_idx,
                                                           const uint32_t* d_m, uint32_t* counter,
                                                           uint8_t* __restrict__ occ,
-                                                          unsigned long long* stats) {
+                                                          unsigned long long* stats,
+                                                          uint32_t* err) {
   const uint32_t n = (*d_m) * A.spp;
   warp_trace<KIND, true>(
       G, n, counter,
@@ -279,7 +274,7 @@ shn_status shn_trace_closest(const shn_grid* g, const shn_rays* rays, uint32_t n
     static int blocks = persistent_blocks(k_trace_rays<K, false, S>, g->ctx->num_sms);          \
     k_trace_rays<K, false, S><<<blocks, kTraceBlock, 0, st>>>(G, R, n, counter, hits->tri,      \
                                                             hits->t, hits->u, hits->v, nullptr, \
-                                                            g->stats);                          \
+                                                            g->stats, g->d_err);                          \
   }
   if (g->kind == SHN_GRID_UNIFORM) {
     if (g->stats) SHN_LAUNCH_RAYS(0, true) else SHN_LAUNCH_RAYS(0, false)
@@ -309,7 +304,7 @@ shn_status shn_trace_any(const shn_grid* g, const shn_rays* rays, uint32_t n, ui
     static int blocks = persistent_blocks(k_trace_rays<K, true, S>, g->ctx->num_sms);           \
     k_trace_rays<K, true, S><<<blocks, kTraceBlock, 0, st>>>(G, R, n, counter, nullptr, nullptr, \
                                                            nullptr, nullptr, d_occluded,        \
-                                                           g->stats);                           \
+                                                           g->stats, g->d_err);                           \
   }
   if (g->kind == SHN_GRID_UNIFORM) {
     if (g->stats) SHN_LAUNCH_ANY(0, true) else SHN_LAUNCH_ANY(0, false)
@@ -339,7 +334,8 @@ shn_status shn_trace_primary(const shn_grid* g, const shn_camera* cam, uint32_t 
   {                                                                                             \
     static int blocks = persistent_blocks(k_trace_camera<K, S>, g->ctx->num_sms);               \
     k_trace_camera<K, S><<<blocks, kTraceBlock, 0, st>>>(G, C, image_id, n, counter, hits->tri, \
-                                                       hits->t, hits->u, hits->v, g->stats);    \
+                                                       hits->t, hits->u, hits->v, g->stats, \
+                                                       g->d_err);    \
   }
   if (g->kind == SHN_GRID_UNIFORM) {
     if (g->stats) SHN_LAUNCH_CAM(0, true) else SHN_LAUNCH_CAM(0, false)
@@ -388,7 +384,7 @@ shn_status shn_trace_ao(const shn_grid* g, const shn_camera* cam, const shn_hits
   {                                                                                               \
     static int blocks = persistent_blocks(k_trace_ao<K, S>, g->ctx->num_sms);                     \
     k_trace_ao<K, S><<<blocks, kTraceBlock, 0, st>>>(G, A, primary->tri, primary->t, hit_idx, d_m, \
-                                                   counter, occ, g->stats);                       \
+                                                   counter, occ, g->stats, g->d_err);                       \
   }
   if (g->kind == SHN_GRID_UNIFORM) {
     if (g->stats) SHN_LAUNCH_AO(0, true) else SHN_LAUNCH_AO(0, false)

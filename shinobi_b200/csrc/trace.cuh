@@ -67,15 +67,17 @@ SHN_D bool wt_test(const RayWT& r, float4 p0, float4 p1, float4 p2, float tmin, 
                    float& t, float& u, float& v) {
   const V3 A = sub(f4v(p0), r.org), B = sub(f4v(p1), r.org), C = sub(f4v(p2), r.org);
   const float Akz = sel(r.kz, A), Bkz = sel(r.kz, B), Ckz = sel(r.kz, C);
-  const float Ax = sel(r.kx, A) - r.Sx * Akz;
-  const float Ay = sel(r.ky, A) - r.Sy * Akz;
-  const float Bx = sel(r.kx, B) - r.Sx * Bkz;
-  const float By = sel(r.ky, B) - r.Sy * Bkz;
-  const float Cx = sel(r.kx, C) - r.Sx * Ckz;
-  const float Cy = sel(r.ky, C) - r.Sy * Ckz;
-  float U = Cx * By - Cy * Bx;
-  float V = Ax * Cy - Ay * Cx;
-  float W = Bx * Ay - By * Ax;
+  // shear: one fused multiply-add per coordinate; edge functions: one product
+  // rounded, then a fused multiply-add (the oracle uses fmaf identically)
+  const float Ax = __fmaf_rn(-r.Sx, Akz, sel(r.kx, A));
+  const float Ay = __fmaf_rn(-r.Sy, Akz, sel(r.ky, A));
+  const float Bx = __fmaf_rn(-r.Sx, Bkz, sel(r.kx, B));
+  const float By = __fmaf_rn(-r.Sy, Bkz, sel(r.ky, B));
+  const float Cx = __fmaf_rn(-r.Sx, Ckz, sel(r.kx, C));
+  const float Cy = __fmaf_rn(-r.Sy, Ckz, sel(r.ky, C));
+  float U = __fmaf_rn(Cx, By, -(Cy * Bx));
+  float V = __fmaf_rn(Ax, Cy, -(Ay * Cx));
+  float W = __fmaf_rn(Bx, Ay, -(By * Ax));
   if (U == 0.f || V == 0.f || W == 0.f) {
     U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
     V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
@@ -84,7 +86,7 @@ SHN_D bool wt_test(const RayWT& r, float4 p0, float4 p1, float4 p2, float tmin, 
   if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
   const float det = U + V + W;
   if (det == 0.f) return false;
-  const float T = U * (r.Sz * Akz) + V * (r.Sz * Bkz) + W * (r.Sz * Ckz);
+  const float T = __fmaf_rn(W, r.Sz * Ckz, __fmaf_rn(V, r.Sz * Bkz, U * (r.Sz * Akz)));
   const float tt = T / det;
   if (!(tt > tmin && tt < tbest)) return false;
   t = tt;

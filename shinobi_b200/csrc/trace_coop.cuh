@@ -224,15 +224,15 @@ SHN_D bool wt_test_p(V3 org, float Sx, float Sy, float Sz, float4 p0, float4 p1,
                      float tmin, float tbest, float& t) {
   const V3 A = sub(f4v(p0), org), B = sub(f4v(p1), org), C = sub(f4v(p2), org);
   const float Akz = cget<KZ>(A), Bkz = cget<KZ>(B), Ckz = cget<KZ>(C);
-  const float Ax = cget<KX>(A) - Sx * Akz;
-  const float Ay = cget<KY>(A) - Sy * Akz;
-  const float Bx = cget<KX>(B) - Sx * Bkz;
-  const float By = cget<KY>(B) - Sy * Bkz;
-  const float Cx = cget<KX>(C) - Sx * Ckz;
-  const float Cy = cget<KY>(C) - Sy * Ckz;
-  float U = Cx * By - Cy * Bx;
-  float V = Ax * Cy - Ay * Cx;
-  float W = Bx * Ay - By * Ax;
+  const float Ax = __fmaf_rn(-Sx, Akz, cget<KX>(A));
+  const float Ay = __fmaf_rn(-Sy, Akz, cget<KY>(A));
+  const float Bx = __fmaf_rn(-Sx, Bkz, cget<KX>(B));
+  const float By = __fmaf_rn(-Sy, Bkz, cget<KY>(B));
+  const float Cx = __fmaf_rn(-Sx, Ckz, cget<KX>(C));
+  const float Cy = __fmaf_rn(-Sy, Ckz, cget<KY>(C));
+  float U = __fmaf_rn(Cx, By, -(Cy * Bx));
+  float V = __fmaf_rn(Ax, Cy, -(Ay * Cx));
+  float W = __fmaf_rn(Bx, Ay, -(By * Ax));
   if (U == 0.f || V == 0.f || W == 0.f) {
     U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
     V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
@@ -241,7 +241,7 @@ SHN_D bool wt_test_p(V3 org, float Sx, float Sy, float Sz, float4 p0, float4 p1,
   if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
   const float det = U + V + W;
   if (det == 0.f) return false;
-  const float T = U * (Sz * Akz) + V * (Sz * Bkz) + W * (Sz * Ckz);
+  const float T = __fmaf_rn(W, Sz * Ckz, __fmaf_rn(V, Sz * Bkz, U * (Sz * Akz)));
   const float tt = T / det;
   if (!(tt > tmin && tt < tbest)) return false;
   t = tt;
@@ -251,6 +251,8 @@ SHN_D bool wt_test_p(V3 org, float Sx, float Sy, float Sz, float4 p0, float4 p1,
 // Whole warp tests references [b, e) against one (warp-uniform) ray.
 // Closest: returns the packed argmin key (t bits << 32 | ref) in every lane,
 // or ~0 when nothing beats tbest.  Any: returns a hit ref or ~0.
+// Loads of the next 32-reference chunk are issued before the current chunk
+// is tested (register double buffering) to cover the L2 latency.
 template <bool ANY, int KX, int KY, int KZ>
 SHN_D uint64_t warp_range_p(const GridView& G, V3 org, float Sx, float Sy, float Sz, float tbest,
                             uint32_t b, uint32_t e, uint32_t& tests) {
