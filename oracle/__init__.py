@@ -76,6 +76,7 @@ def lib():
         L.orc_primary_rays.argtypes = [vp, u32, u32, u32, vp, vp, vp]
         L.orc_ao_rays.argtypes = [vp, vp] + [vp] * 8 + [u32, u32, u32, f32] + [vp] * 7
         L.orc_ao_rays.restype = u32
+        L.orc_pt_render.argtypes = [vp, vp, vp, u32, u32, u32, u32, u32, f32, vp, vp, vp, vp, vp, f32, u32, vp]
         L.orc_compact.argtypes = [vp, u32, vp]
         L.orc_compact.restype = u32
         _lib = L
@@ -287,6 +288,17 @@ def ao_rays(vtx, idx, org, dirs, tri, t, spp: int, seed: int, offset: float):
     ro = np.stack(outs[0:3], axis=1)
     rd = np.stack(outs[3:6], axis=1)
     return ro, rd, outs[6]
+
+
+def pt_render(g: Grid, cam, spp, max_depth, rr_depth, albedo, light_pos, light_e1, light_e2,
+              light_radiance, background, offset, seed) -> np.ndarray:
+    """Path-traced image (resy, resx, 3) with the same semantics as shn_pt_render."""
+    c = camera(cam)
+    img = np.zeros(cam.res_x * cam.res_y * 3, np.float32)
+    lib().orc_pt_render(g.handle, _p(c), _p(_f32(cam.eye)), cam.res_x, cam.res_y, spp, max_depth,
+                        rr_depth, albedo, _p(_f32(light_pos)), _p(_f32(light_e1)), _p(_f32(light_e2)),
+                        _p(_f32(light_radiance)), _p(_f32(background)), offset, seed, _p(img))
+    return img.reshape(cam.res_y, cam.res_x, 3)
 
 
 def compact(flags) -> np.ndarray:

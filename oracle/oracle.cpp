@@ -895,6 +895,105 @@ uint32_t orc_ao_rays(const float* vtx, const uint32_t* idx, const float* ox, con
   return m;
 }
 
+// Path tracer, path by path (the CUDA side runs it as a wavefront with
+// compaction; results are per path and independent of the schedule).
+// Semantics: SimplePathTracer (src/Integrator/SimplePathTracer.hpp:65-241)
+// restated with next-event estimation at every vertex to a parallelogram
+// light, Russian roulette with continuation probability = albedo from depth
+// rr_depth on, cosine-weighted bounces (CosineHemisphereSampler,
+// src/Utils/HemisphereSamplers.hpp:54-72), camera jitter as in
+// RandomPixelSampler (src/Primitive/PixelSampler.h:56-70), Philox4x32-10
+// counters (pixel, sample, depth, tag) with key (seed, 0).  The image is the
+// per-pixel mean of the per-path radiance summed in sample order.
+void orc_pt_render(const orc_grid* G, const float cam9[9], const float eye[3], uint32_t resx,
+                   uint32_t resy, uint32_t spp, uint32_t max_depth, uint32_t rr_depth, float albedo,
+                   const float lpos[3], const float le1[3], const float le2[3], const float lrad[3],
+                   const float bg[3], float offset, uint32_t seed, float* image) {
+  const uint32_t npix = resx * resy;
+  const V3 LP = mk(lpos[0], lpos[1], lpos[2]), E1 = mk(le1[0], le1[1], le1[2]),
+           E2 = mk(le2[0], le2[1], le2[2]), LR = mk(lrad[0], lrad[1], lrad[2]), BG = mk(bg[0], bg[1], bg[2]);
+  const V3 ln = cross(E1, E2);
+  const float larea = sqrtf(dot(ln, ln));
+  const V3 lnrm = normalize(ln);
+  const V3 tl = mk(cam9[0], cam9[1], cam9[2]), sx = mk(cam9[3], cam9[4], cam9[5]), sy = mk(cam9[6], cam9[7], cam9[8]);
+  const V3 E = mk(eye[0], eye[1], eye[2]);
+  const float rxf = (float)resx;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t pi = 0; pi < (int64_t)npix; ++pi) {
+    const uint32_t p = (uint32_t)pi;
+    float ir = 0.f, ig = 0.f, ib = 0.f;
+    for (uint32_t s = 0; s < spp; ++s) {
+      uint32_t c[4] = {p, s, 0u, 0x4A49u};
+      philox(c, seed, 0u);
+      float ox = u01(c[0]), oy = u01(c[1]);
+      const float tmp = (float)p / rxf;
+      oy = truncf(tmp) + oy;
+      ox = (tmp - truncf(tmp)) * rxf + ox;
+      V3 d = mk(tl.x + ox * sx.x + oy * sy.x, tl.y + ox * sx.y + oy * sy.y, tl.z + ox * sx.z + oy * sy.z);
+      V3 org = E;
+      V3 beta = mk(1.f, 1.f, 1.f), L = mk(0.f, 0.f, 0.f);
+      for (uint32_t depth = 0; depth < max_depth; ++depth) {
+        Hit h{FLT_MAX, kMiss, 0.f, 0.f};
+        Stats st;
+        trace_one(G, Ray{org, d}, h, false, st);
+        if (h.ref == kMiss) {
+          L = add(L, mul(beta, BG));
+          break;
+        }
+        const Tri tr = load_tri(G->vtx.data(), G->idx.data(), G->indices[h.ref]);
+        const V3 e1 = sub(tr.v[1], tr.v[0]);
+        V3 nn = normalize(cross(e1, sub(tr.v[2], tr.v[0])));
+        if (dot(nn, d) > 0.f) nn = mk(-nn.x, -nn.y, -nn.z);
+        const V3 hp = add(org, muls(d, h.t));
+        const V3 o = add(hp, muls(nn, offset));
+        uint32_t cl4[4] = {p, s, depth, 0x4C54u};
+        philox(cl4, seed, 0u);
+        const float lu = u01(cl4[0]), lv = u01(cl4[1]), urr = u01(cl4[2]);
+        const V3 lp = add(add(LP, muls(E1, lu)), muls(E2, lv));
+        const V3 wv = sub(lp, o);
+        const float d2 = dot(wv, wv);
+        const V3 l = muls(wv, 1.0f / sqrtf(d2));
+        const float cs = dot(nn, l);
+        const float clg = -dot(lnrm, l);
+        if (cs > 0.f && clg > 0.f) {
+          Hit sh{0.9999f, kMiss, 0.f, 0.f};
+          Stats st2;
+          trace_one(G, Ray{o, wv}, sh, true, st2);
+          if (sh.ref == kMiss) {
+            const float f = ((((albedo * 0.31830988618379067f) * cs) * clg) * larea) / d2;
+            L = add(L, muls(mul(beta, LR), f));
+          }
+        }
+        bool live = depth + 1 < max_depth;
+        if (live && depth >= rr_depth) {
+          if (urr < albedo) beta = muls(beta, 1.0f / albedo);
+          else live = false;
+        }
+        if (!live) break;
+        uint32_t cd[4] = {p, s, depth, 0x4449u};
+        philox(cd, seed, 0u);
+        const float u1 = u01(cd[0]), u2 = u01(cd[1]);
+        float sn, cn;
+        sincos_2pi(u1, sn, cn);
+        const float rr = sqrtf(1.f - u2);
+        const float lx = sn * rr, ly = cn * rr, lz = sqrtf(u2);
+        const V3 tx = normalize(e1);
+        const V3 ty = cross(nn, tx);
+        d = mk(tx.x * lx + ty.x * ly + nn.x * lz, tx.y * lx + ty.y * ly + nn.y * lz,
+               tx.z * lx + ty.z * ly + nn.z * lz);
+        beta = muls(beta, albedo);
+        org = o;
+      }
+      ir += L.x;
+      ig += L.y;
+      ib += L.z;
+    }
+    image[3 * (size_t)p] = ir / (float)spp;
+    image[3 * (size_t)p + 1] = ig / (float)spp;
+    image[3 * (size_t)p + 2] = ib / (float)spp;
+  }
+}
+
 // Stable stream compaction: indices of non-zero flags in order.
 uint32_t orc_compact(const uint32_t* flags, uint32_t n, uint32_t* out) {
   uint32_t m = 0;

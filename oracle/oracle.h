@@ -52,6 +52,10 @@ uint32_t orc_ao_rays(const float* vtx, const uint32_t* idx, const float* ox, con
                      const uint32_t* tri, const float* t, uint32_t n, uint32_t spp, uint32_t seed,
                      float offset, float* rox, float* roy, float* roz, float* rdx, float* rdy,
                      float* rdz, uint32_t* rpix);
+void orc_pt_render(const orc_grid* g, const float cam9[9], const float eye[3], uint32_t resx,
+                   uint32_t resy, uint32_t spp, uint32_t max_depth, uint32_t rr_depth, float albedo,
+                   const float lpos[3], const float le1[3], const float le2[3], const float lrad[3],
+                   const float bg[3], float offset, uint32_t seed, float* image);
 uint32_t orc_compact(const uint32_t* flags, uint32_t n, uint32_t* out);
 
 #endif

@@ -166,6 +166,20 @@ def grid_params(kind: int = SHN_GRID_UNIFORM, lambda_: float | None = None, top_
     return p
 
 
+def pt_params(**kw) -> _abi.PtParams:
+    """Path tracer parameters (defaults: 16 spp, depth 4, roulette from depth 2, albedo 0.7)."""
+    p = _abi.PtParams()
+    _abi.load().shn_pt_params_default(C.byref(p))
+    for k, v in kw.items():
+        if isinstance(v, (tuple, list)):
+            arr = getattr(p, k)
+            for i, x in enumerate(v):
+                arr[i] = x
+        else:
+            setattr(p, k, v)
+    return p
+
+
 def camera_struct(cam) -> _abi.Camera:
     c = _abi.Camera()
     for k in range(3):
@@ -275,6 +289,18 @@ class Grid:
         self.ctx.check(self.ctx.lib.shn_trace_ao(self.handle, C.byref(c), C.byref(h), spp, length,
                                                  offset, seed, _ptr(out), _ptr(num_rays),
                                                  _stream(stream)), "shn_trace_ao")
+        return out
+
+    def pt_render(self, scene: FaceSoup, cam, params=None, out=None, stats=None, stream=None):
+        """Wavefront path tracer; returns the (res_y, res_x, 3) mean-radiance image (device)."""
+        torch = _torch()
+        p = params or pt_params()
+        out = out if out is not None else torch.empty(cam.res_y, cam.res_x, 3, dtype=torch.float32,
+                                                      device="cuda")
+        c = camera_struct(cam)
+        self.ctx.check(self.ctx.lib.shn_pt_render(self.handle, scene.handle, C.byref(c), C.byref(p),
+                                                  _ptr(out), _ptr(stats), _stream(stream)),
+                       "shn_pt_render")
         return out
 
     def close(self):

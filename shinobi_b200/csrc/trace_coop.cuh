@@ -57,8 +57,7 @@ SHN_D RayWT lane_ray(const Lane& L) {
 }
 
 template <int KIND>
-SHN_D void lane_init(const GridView& G, Lane& L, V3 org, V3 dir, float tmax) {
-  const Geom& g = G.g;
+SHN_D void lane_init(const Geom& g, Lane& L, V3 org, V3 dir, float tmax) {
   L.org = org;
   L.rcp = divv(mk(1.f, 1.f, 1.f), dir);
   const RayWT w = wt_setup(org, dir);
@@ -105,8 +104,8 @@ SHN_D void lane_init(const GridView& G, Lane& L, V3 org, V3 dir, float tmax) {
 // Runs the lane's state machine until it has a non-empty range to test
 // (returns true, range in L.b/L.e) or the ray is finished (returns false).
 template <int KIND, bool ANY>
-SHN_D bool lane_advance(const GridView& G, Lane& L, uint32_t& steps) {
-  const Geom& g = G.g;
+SHN_D bool lane_advance(const Geom& g, const uint2* __restrict__ cells, const uint2* __restrict__ leaves,
+                        Lane& L, uint32_t& steps) {
   while (true) {
     switch (L.st) {
       case ST_TOP: {
@@ -114,7 +113,7 @@ SHN_D bool lane_advance(const GridView& G, Lane& L, uint32_t& steps) {
         const uint32_t cx = (uint32_t)clampf(L.cell.x, 0.f, g.resf.x - 1.f);
         const uint32_t cy = (uint32_t)clampf(L.cell.y, 0.f, g.resf.y - 1.f);
         const uint32_t cz = (uint32_t)clampf(L.cell.z, 0.f, g.resf.z - 1.f);
-        const uint2 cw = __ldg(G.cells + (cx + cy * (uint32_t)g.res[0] + cz * (uint32_t)g.res[0] * (uint32_t)g.res[1]));
+        const uint2 cw = __ldg(cells + (cx + cy * (uint32_t)g.res[0] + cz * (uint32_t)g.res[0] * (uint32_t)g.res[1]));
         steps++;
         if (KIND == 0) {
           L.b = cw.x;
@@ -155,7 +154,7 @@ SHN_D bool lane_advance(const GridView& G, Lane& L, uint32_t& steps) {
         L.vis2++;
         const V3 sc = L.sc, cres = L.cres;
         const uint32_t li = L.lb + (uint32_t)(sc.x + cres.x * sc.y + cres.x * cres.y * sc.z);
-        const uint2 range = __ldg(G.leaves + li);
+        const uint2 range = __ldg(leaves + li);
         steps++;
         L.b = range.x;
         L.e = range.y;
@@ -332,16 +331,19 @@ SHN_D void lane_result(const GridView& G, const Lane& L, Hit& h) {
   h.v = v;
 }
 
-// The warp loop.  src(i, org, dir, tmax) generates ray i; sink(i, hit, steps, tests)
-// consumes its result.  n rays are taken from *counter (pre-zeroed).
-template <int KIND, bool ANY, class Src, class Sink>
-SHN_D void warp_trace(const GridView& G, uint32_t n, uint32_t* counter, Src&& src, Sink&& sink) {
+// The warp loop.  acc gives the lane's grid (geometry, cells, leaves) by its
+// scene id; G holds the reference-ordered triangle arrays shared by all
+// scenes.  src(i, org, dir, tmax, scene) generates ray i; sink(i, hit, steps,
+// tests) consumes its result.  n rays are taken from *counter (pre-zeroed).
+template <int KIND, bool ANY, class Acc, class Src, class Sink>
+SHN_D void warp_trace_acc(const GridView& G, const Acc& acc, uint32_t n, uint32_t* counter,
+                          Src&& src, Sink&& sink) {
   const int lane = threadIdx.x & 31;
   const uint32_t lt = (1u << lane) - 1u;
   Lane L;
   L.st = ST_DONE;
   bool has = false;
-  uint32_t rid = 0, steps = 0, tests = 0;
+  uint32_t rid = 0, steps = 0, tests = 0, scene = 0;
   bool pool_empty = false;
   while (true) {
     const uint32_t idle = __ballot_sync(0xFFFFFFFFu, !has);
@@ -359,18 +361,18 @@ SHN_D void warp_trace(const GridView& G, uint32_t n, uint32_t* counter, Src&& sr
           steps = tests = 0;
           V3 o, d;
           float tmax;
-          src(r, o, d, tmax);
-          lane_init<KIND>(G, L, o, d, tmax);
+          src(r, o, d, tmax, scene);
+          lane_init<KIND>(acc.geom(scene), L, o, d, tmax);
         }
       }
     }
     bool pending = false;
     if (has) {
-      pending = lane_advance<KIND, ANY>(G, L, steps);
+      pending = lane_advance<KIND, ANY>(acc.geom(scene), acc.cells(scene), acc.leaves(scene), L, steps);
       if (!pending) {
         Hit h;
         lane_result(G, L, h);
-        sink(rid, h, steps, tests);
+        sink(rid, h, steps, tests, scene);
         has = false;
       }
     }
@@ -405,6 +407,25 @@ SHN_D void warp_trace(const GridView& G, uint32_t n, uint32_t* counter, Src&& sr
       }
     }
   }
+}
+
+// Grid access of a lane: the single-grid kernels use one GridView for every lane.
+struct OneGrid {
+  const GridView* G;
+  SHN_D const Geom& geom(uint32_t) const { return G->g; }
+  SHN_D const uint2* cells(uint32_t) const { return G->cells; }
+  SHN_D const uint2* leaves(uint32_t) const { return G->leaves; }
+};
+
+template <int KIND, bool ANY, class Src, class Sink>
+SHN_D void warp_trace(const GridView& G, uint32_t n, uint32_t* counter, Src&& src, Sink&& sink) {
+  warp_trace_acc<KIND, ANY>(
+      G, OneGrid{&G}, n, counter,
+      [&](uint32_t i, V3& o, V3& d, float& tmax, uint32_t& scene) {
+        scene = 0;
+        src(i, o, d, tmax);
+      },
+      [&](uint32_t i, const Hit& h, uint32_t steps, uint32_t tests, uint32_t) { sink(i, h, steps, tests); });
 }
 
 }  // namespace shn
