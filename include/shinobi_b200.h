@@ -192,6 +192,50 @@ shn_status shn_trace_ao(const shn_grid* g, const shn_camera* cam, const shn_hits
  * counting off.  Not part of the reference interface. */
 shn_status shn_grid_set_stats(shn_grid* g, uint64_t* d_counters);
 
+/* ---- batched multi-scene build and trace ----------------------------------------
+ * Many independent scenes, each with its own uniform grid, built by one
+ * fused pipeline (one count/scan, emit, sort and range pass over all
+ * triangles) and traced by one persistent launch over all scenes' rays.
+ * Not a reference interface: the reference builds one scene per engine. */
+typedef struct shn_batch shn_batch;
+/* Scenes are concatenated: scene s has vertices [vtx_offsets[s], vtx_offsets[s+1])
+ * and triangles [tri_offsets[s], tri_offsets[s+1]) whose indices are local to
+ * the scene's vertices.  Offsets are host arrays of num_scenes+1 entries
+ * starting at 0; vertices/indices are host or device memory (mem).  Synchronises. */
+shn_status shn_batch_create(shn_ctx* ctx, uint32_t num_scenes, const float* vtx_xyz,
+                            const uint32_t* vtx_offsets, const uint32_t* idx,
+                            const uint32_t* tri_offsets, uint32_t mem, void* stream, shn_batch** out);
+/* Per-scene cell density (num_scenes floats, default 5). */
+shn_status shn_batch_set_lambdas(shn_batch* b, const float* lambdas);
+/* Measured autotuner: for every scene and candidate lambda, builds the scene's
+ * grid and traces min(sample_rays, expected_rays[s]) uniformly random rays
+ * (origins in [-1,2]^3, unit directions, Philox seed), and keeps the lambda
+ * with the smallest build + scaled trace time.  chosen (optional) receives
+ * the lambdas; they are also applied to the batch.  Synchronises. */
+shn_status shn_batch_autotune(shn_batch* b, const float* candidates, uint32_t num_candidates,
+                              const uint32_t* expected_rays, uint32_t sample_rays, uint32_t seed,
+                              float* chosen, void* stream);
+/* Builds every scene's grid (plans buffers with one read-back on the first
+ * call or after a lambda change).  Synchronises. */
+shn_status shn_batch_build(shn_batch* b, void* stream);
+/* Traces rays of all scenes in one launch: device SoA rays concatenated in
+ * scene order, ray_offsets = host array of num_scenes+1.  Closest hits into
+ * hits (triangle ids local to their scene) or, if d_occluded != NULL, any-hit
+ * flags. */
+shn_status shn_batch_trace(shn_batch* b, const shn_rays* rays, const uint32_t* ray_offsets,
+                           shn_hits* hits, uint8_t* d_occluded, void* stream);
+/* Captures build + closest-hit trace into a CUDA graph (ray and hit buffers
+ * are baked in and must stay valid); shn_batch_replay launches it. */
+shn_status shn_batch_capture(shn_batch* b, const shn_rays* rays, const uint32_t* ray_offsets,
+                             shn_hits* hits, void* stream);
+shn_status shn_batch_replay(shn_batch* b, void* stream);
+shn_status shn_batch_info(const shn_batch* b, uint64_t* num_pairs, uint64_t* total_cells, float* build_ms);
+/* One scene's grid rebased to local indices: cells 2*res product uint32,
+ * indices num_refs uint32 (triangle ids local to the scene).  Synchronises. */
+shn_status shn_batch_export_scene(const shn_batch* b, uint32_t scene, int32_t res[3], float bounds[6],
+                                  uint32_t* cells, uint32_t* indices, uint64_t* num_refs);
+void shn_batch_destroy(shn_batch* b);
+
 /* ---- path tracer --------------------------------------------------------------- */
 typedef struct shn_pt_params {
   uint32_t spp;              /* samples per pixel */

@@ -315,6 +315,106 @@ class Grid:
             pass
 
 
+class Batch:
+    """Many scenes built by one fused pipeline and traced by one launch (uniform grids)."""
+
+    def __init__(self, scenes_list, ctx: Context | None = None, stream=None):
+        self.ctx = ctx or default_context()
+        vo = np.zeros(len(scenes_list) + 1, np.uint32)
+        to = np.zeros(len(scenes_list) + 1, np.uint32)
+        for i, sc in enumerate(scenes_list):
+            vo[i + 1] = vo[i] + sc.vertices.shape[0]
+            to[i + 1] = to[i] + sc.indices.shape[0]
+        v = np.ascontiguousarray(np.concatenate([sc.vertices for sc in scenes_list]), np.float32)
+        ix = np.ascontiguousarray(np.concatenate([sc.indices for sc in scenes_list]), np.uint32)
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.shn_batch_create(
+            self.ctx.handle, len(scenes_list), v.ctypes.data_as(C.c_void_p), vo.ctypes.data_as(C.c_void_p),
+            ix.ctypes.data_as(C.c_void_p), to.ctypes.data_as(C.c_void_p), SHN_MEM_HOST, _stream(stream),
+            C.byref(h)), "shn_batch_create")
+        self.handle = h
+        self.num_scenes = len(scenes_list)
+        self.tri_offsets = to
+
+    def set_lambdas(self, lambdas):
+        a = np.ascontiguousarray(lambdas, np.float32)
+        self.ctx.check(self.ctx.lib.shn_batch_set_lambdas(self.handle, a.ctypes.data_as(C.c_void_p)),
+                       "shn_batch_set_lambdas")
+
+    def autotune(self, candidates, expected_rays, sample_rays=16384, seed=7, stream=None):
+        c = np.ascontiguousarray(candidates, np.float32)
+        e = np.ascontiguousarray(expected_rays, np.uint32)
+        out = np.zeros(self.num_scenes, np.float32)
+        self.ctx.check(self.ctx.lib.shn_batch_autotune(
+            self.handle, c.ctypes.data_as(C.c_void_p), c.size, e.ctypes.data_as(C.c_void_p), sample_rays,
+            seed, out.ctypes.data_as(C.c_void_p), _stream(stream)), "shn_batch_autotune")
+        return out
+
+    def build(self, stream=None):
+        self.ctx.check(self.ctx.lib.shn_batch_build(self.handle, _stream(stream)), "shn_batch_build")
+        return self
+
+    def info(self):
+        p, c, ms = C.c_uint64(), C.c_uint64(), C.c_float()
+        self.ctx.check(self.ctx.lib.shn_batch_info(self.handle, C.byref(p), C.byref(c), C.byref(ms)),
+                       "shn_batch_info")
+        return {"num_pairs": p.value, "total_cells": c.value, "build_ms": ms.value}
+
+    def trace(self, org, dirs, ray_offsets, tmax=None, out: HitBuffers | None = None, any_hit=False,
+              stream=None):
+        torch = _torch()
+        n = org.shape[0]
+        r, keep = Grid._rays(org, dirs, tmax)
+        ro = np.ascontiguousarray(ray_offsets, np.uint32)
+        if any_hit:
+            occ = torch.empty(n, dtype=torch.uint8, device=org.device)
+            self.ctx.check(self.ctx.lib.shn_batch_trace(self.handle, C.byref(r), ro.ctypes.data_as(C.c_void_p),
+                                                        None, _ptr(occ), _stream(stream)), "shn_batch_trace")
+            return occ
+        out = out or alloc_hits(n, org.device)
+        h = out.struct()
+        self.ctx.check(self.ctx.lib.shn_batch_trace(self.handle, C.byref(r), ro.ctypes.data_as(C.c_void_p),
+                                                    C.byref(h), None, _stream(stream)), "shn_batch_trace")
+        return out
+
+    def capture(self, org, dirs, ray_offsets, out: HitBuffers, stream=None):
+        """Capture build + trace into a CUDA graph; keeps the ray columns alive."""
+        r, self._graph_cols = Grid._rays(org, dirs, None)
+        self._graph_ro = np.ascontiguousarray(ray_offsets, np.uint32)
+        h = out.struct()
+        self.ctx.check(self.ctx.lib.shn_batch_capture(self.handle, C.byref(r),
+                                                      self._graph_ro.ctypes.data_as(C.c_void_p),
+                                                      C.byref(h), _stream(stream)), "shn_batch_capture")
+
+    def replay(self, stream=None):
+        self.ctx.check(self.ctx.lib.shn_batch_replay(self.handle, _stream(stream)), "shn_batch_replay")
+
+    def export_scene(self, s: int, max_cells: int, max_refs: int):
+        res = (C.c_int32 * 3)()
+        b = (C.c_float * 6)()
+        cells = np.zeros(2 * max_cells, np.uint32)
+        idx = np.zeros(max(1, max_refs), np.uint32)
+        nref = C.c_uint64()
+        self.ctx.check(self.ctx.lib.shn_batch_export_scene(self.handle, s, res, b, cells.ctypes.data_as(C.c_void_p),
+                                                           idx.ctypes.data_as(C.c_void_p), C.byref(nref)),
+                       "shn_batch_export_scene")
+        r = np.array(res[:], np.int32)
+        nc = int(np.prod(r))
+        return {"res": r, "bounds": np.array(b[:], np.float32), "cells": cells[:2 * nc].reshape(-1, 2),
+                "indices": idx[:nref.value]}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx.lib.shn_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def exclusive_scan(x, ctx: Context | None = None, stream=None):
     """uint32 exclusive scan; returns n+1 values (last = total)."""
     torch = _torch()

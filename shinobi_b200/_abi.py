@@ -78,6 +78,16 @@ SIGNATURES = {
     "shn_trace_primary": ([vp, C.POINTER(Camera), u32, C.POINTER(Hits), vp], i32),
     "shn_trace_ao": ([vp, C.POINTER(Camera), C.POINTER(Hits), u32, f32, f32, u32, vp, vp, vp], i32),
     "shn_grid_set_stats": ([vp, vp], i32),
+    "shn_batch_create": ([vp, u32, vp, vp, vp, vp, u32, vp, C.POINTER(vp)], i32),
+    "shn_batch_set_lambdas": ([vp, vp], i32),
+    "shn_batch_autotune": ([vp, vp, u32, vp, u32, u32, vp, vp], i32),
+    "shn_batch_build": ([vp, vp], i32),
+    "shn_batch_trace": ([vp, C.POINTER(Rays), vp, C.POINTER(Hits), vp, vp], i32),
+    "shn_batch_capture": ([vp, C.POINTER(Rays), vp, C.POINTER(Hits), vp], i32),
+    "shn_batch_replay": ([vp, vp], i32),
+    "shn_batch_info": ([vp, vp, vp, vp], i32),
+    "shn_batch_export_scene": ([vp, u32, vp, vp, vp, vp, vp], i32),
+    "shn_batch_destroy": ([vp], None),
     "shn_pt_params_default": ([C.POINTER(PtParams)], None),
     "shn_pt_render": ([vp, vp, C.POINTER(Camera), C.POINTER(PtParams), vp, vp, vp], i32),
     "shn_exclusive_scan_u32": ([vp, vp, vp, u32, vp], i32),

@@ -347,6 +347,112 @@ __global__ void k_leaf_emit(TriSoA tri, const uint64_t* __restrict__ top, uint32
   }
 }
 
+// ---- batched multi-scene build ---------------------------------------------------
+// All scenes' triangles are one array (global triangle ids); scene s owns
+// triangles [tri_off[s], tri_off[s+1]) and global cells
+// [scenes[s].cell_offset, + res product).  One count/scan, one emit, one sort
+// and one range pass serve every scene.
+SHN_D uint32_t find_segment(const uint32_t* __restrict__ off, uint32_t nseg, uint32_t i) {
+  uint32_t lo = 0, hi = nseg;  // off[lo] <= i < off[hi]
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(off + mid) <= i) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_batch_pack(const float* __restrict__ vtx, const uint32_t* __restrict__ vtx_off,
+                             const uint32_t* __restrict__ idx, const uint32_t* __restrict__ tri_off,
+                             uint32_t ns, uint32_t T, float4* __restrict__ tri) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+    const uint32_t s = find_segment(tri_off, ns, t);
+    const uint32_t vb = __ldg(vtx_off + s);
+    const uint32_t i0 = vb + idx[3 * (size_t)t], i1 = vb + idx[3 * (size_t)t + 1], i2 = vb + idx[3 * (size_t)t + 2];
+    const float* a = vtx + 3 * (size_t)i0;
+    const float* b = vtx + 3 * (size_t)i1;
+    const float* c = vtx + 3 * (size_t)i2;
+    tri[t] = make_float4(a[0], a[1], a[2], __uint_as_float(t));
+    tri[T + (size_t)t] = make_float4(b[0], b[1], b[2], 0.f);
+    tri[2 * (size_t)T + t] = make_float4(c[0], c[1], c[2], 0.f);
+  }
+}
+
+__global__ void k_batch_bounds(const float4* __restrict__ tri, const uint32_t* __restrict__ tri_off,
+                               uint32_t ns, uint32_t T, uint32_t* __restrict__ out) {
+  for (uint32_t t0 = blockIdx.x * blockDim.x; t0 < T; t0 += gridDim.x * blockDim.x) {
+    const uint32_t t = t0 + threadIdx.x;
+    const bool valid = t < T;
+    const uint32_t s = valid ? find_segment(tri_off, ns, t) : 0xFFFFFFFFu;
+    V3 mn = mk(FLT_MAX, FLT_MAX, FLT_MAX), mx = mk(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+    if (valid) {
+      for (int k = 0; k < 3; ++k) {
+        const V3 p = f4v(tri[(size_t)k * T + t]);
+        mn = vmin(mn, p);
+        mx = vmax(mx, p);
+      }
+    }
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, s);
+    const int lane = threadIdx.x & 31;
+    if (peers == 0xFFFFFFFFu) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        mn.x = fminf(mn.x, __shfl_xor_sync(0xFFFFFFFFu, mn.x, o));
+        mn.y = fminf(mn.y, __shfl_xor_sync(0xFFFFFFFFu, mn.y, o));
+        mn.z = fminf(mn.z, __shfl_xor_sync(0xFFFFFFFFu, mn.z, o));
+        mx.x = fmaxf(mx.x, __shfl_xor_sync(0xFFFFFFFFu, mx.x, o));
+        mx.y = fmaxf(mx.y, __shfl_xor_sync(0xFFFFFFFFu, mx.y, o));
+        mx.z = fmaxf(mx.z, __shfl_xor_sync(0xFFFFFFFFu, mx.z, o));
+      }
+      if (lane != 0) continue;
+    }
+    if (!valid) continue;
+    uint32_t* o6 = out + 6 * (size_t)s;
+    atomicMin(o6 + 0, fkey(mn.x)); atomicMin(o6 + 1, fkey(mn.y)); atomicMin(o6 + 2, fkey(mn.z));
+    atomicMax(o6 + 3, fkey(mx.x)); atomicMax(o6 + 4, fkey(mx.y)); atomicMax(o6 + 5, fkey(mx.z));
+  }
+}
+
+__global__ void k_batch_bounds_decode(uint32_t* io, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) io[i] = __float_as_uint(fval(io[i]));
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_batch_count_scan(TriSoA tri, const uint32_t* __restrict__ tri_off,
+                                                                const BatchScene* __restrict__ scenes,
+                                                                uint32_t ns, uint32_t T, LookbackState st,
+                                                                uint32_t* offs) {
+  __shared__ TileScanSmem<kScanBlock, kScanItems> sm;
+  tile_scan<kScanBlock, kScanItems>(
+      st, T, sm,
+      [&](uint32_t i) {
+        const uint32_t s = find_segment(tri_off, ns, i);
+        V3 a, b, c;
+        load_tri(tri, i, a, b, c);
+        uint32_t cnt = 0;
+        for_each_cell(a, b, c, scenes[s].g, [&](uint32_t) { ++cnt; });
+        return cnt;
+      },
+      [&](uint32_t i, uint32_t ex) { offs[i] = ex; }, offs + T);
+}
+
+__global__ void k_batch_emit(TriSoA tri, const uint32_t* __restrict__ tri_off,
+                             const BatchScene* __restrict__ scenes, uint32_t ns, uint32_t T,
+                             const uint32_t* __restrict__ offs, uint64_t* __restrict__ keys,
+                             uint32_t capacity, uint32_t* err) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+    const uint32_t s = find_segment(tri_off, ns, t);
+    V3 a, b, c;
+    load_tri(tri, t, a, b, c);
+    uint32_t o = offs[t];
+    const uint64_t cb = scenes[s].cell_offset;
+    for_each_cell(a, b, c, scenes[s].g, [&](uint32_t cell) {
+      if (o < capacity) keys[o] = ((cb + cell) << 32) | t;
+      else atomicOr(err, kErrCapacity);
+      ++o;
+    });
+  }
+}
+
 int grid_for(uint64_t n, int block, int max_blocks) {
   const uint64_t b = (n + block - 1) / block;
   return (int)std::max<uint64_t>(1, std::min<uint64_t>(b, (uint64_t)max_blocks));
@@ -577,6 +683,53 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   g->num_refs = R;
   g->top_pairs = sortedTop;
   return finish(g, st);
+}
+
+
+// ---- batch launch wrappers (host) ------------------------------------------------------
+void launch_batch_pack(const float* vtx, const uint32_t* vtx_off, const uint32_t* idx,
+                       const uint32_t* tri_off, uint32_t ns, uint32_t T, float4* tri, cudaStream_t st) {
+  if (T) k_batch_pack<<<grid_for(T, 256, 148 * 16), 256, 0, st>>>(vtx, vtx_off, idx, tri_off, ns, T, tri);
+}
+
+void launch_batch_bounds(const float4* tri, const uint32_t* tri_off, uint32_t ns, uint32_t T,
+                         float* d_out6ns, cudaStream_t st) {
+  std::vector<uint32_t> init(6 * (size_t)ns);
+  for (uint32_t s = 0; s < ns; ++s)
+    for (int i = 0; i < 6; ++i) init[6 * s + i] = i < 3 ? 0xFFFFFFFFu : 0u;
+  cudaMemcpyAsync(d_out6ns, init.data(), init.size() * 4, cudaMemcpyHostToDevice, st);
+  cudaStreamSynchronize(st);  // init lives on the host stack
+  if (T) k_batch_bounds<<<grid_for(T, 256, 148 * 16), 256, 0, st>>>(tri, tri_off, ns, T, (uint32_t*)d_out6ns);
+  k_batch_bounds_decode<<<(6 * ns + 255) / 256, 256, 0, st>>>((uint32_t*)d_out6ns, 6 * ns);
+}
+
+size_t batch_scan_bytes(uint32_t T) { return (((size_t)T + kScanTile - 1) / kScanTile + 2) * 8; }
+
+void launch_batch_count(const float4* tri, uint32_t T, const uint32_t* tri_off, const BatchScene* scenes,
+                        uint32_t ns, void* scan_ws, uint32_t* err, uint32_t* offs, cudaStream_t st) {
+  if (!T) {
+    cudaMemsetAsync(offs, 0, 4, st);
+    return;
+  }
+  const size_t tiles = ((size_t)T + kScanTile - 1) / kScanTile;
+  uint64_t* status = (uint64_t*)scan_ws;
+  cudaMemsetAsync(status, 0, (tiles + 2) * 8, st);
+  LookbackState ls{status, (uint32_t*)(status + tiles + 1), err};
+  const TriSoA ts{tri, tri + T, tri + 2 * (size_t)T};
+  k_batch_count_scan<<<(unsigned)tiles, kScanBlock, 0, st>>>(ts, tri_off, scenes, ns, T, ls, offs);
+}
+
+void launch_batch_emit(const float4* tri, uint32_t T, const uint32_t* tri_off, const BatchScene* scenes,
+                       uint32_t ns, const uint32_t* offs, uint64_t* keys, uint32_t capacity,
+                       uint32_t* err, cudaStream_t st) {
+  const TriSoA ts{tri, tri + T, tri + 2 * (size_t)T};
+  if (T) k_batch_emit<<<grid_for(T, 256, 148 * 16), 256, 0, st>>>(ts, tri_off, scenes, ns, T, offs, keys, capacity, err);
+}
+
+void launch_ranges(const uint64_t* keys, uint32_t n, uint2* ranges, uint32_t* indices,
+                   const float4* tri, uint32_t T, float4* rtri, cudaStream_t st) {
+  const TriSoA ts{tri, tri + T, tri + 2 * (size_t)T};
+  if (n) k_ranges<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(keys, n, ranges, indices, ts, rtri);
 }
 
 }  // namespace shn

@@ -98,6 +98,26 @@ void launch_pack_triangles(const float* vtx, const uint32_t* idx, uint32_t nt, f
                            cudaStream_t st);
 void launch_bounds_reduce(const float4* tri, uint32_t nt, float* d_out6, cudaStream_t st);
 
+// batched multi-scene build (build.cu)
+struct BatchScene {
+  Geom g;
+  uint32_t tri_offset, nt;
+  uint64_t cell_offset;
+  uint32_t ncells, pad;
+};
+void launch_batch_pack(const float* vtx, const uint32_t* vtx_off, const uint32_t* idx,
+                       const uint32_t* tri_off, uint32_t ns, uint32_t T, float4* tri, cudaStream_t st);
+void launch_batch_bounds(const float4* tri, const uint32_t* tri_off, uint32_t ns, uint32_t T,
+                         float* d_out6ns, cudaStream_t st);
+size_t batch_scan_bytes(uint32_t T);
+void launch_batch_count(const float4* tri, uint32_t T, const uint32_t* tri_off, const BatchScene* scenes,
+                        uint32_t ns, void* scan_ws, uint32_t* err, uint32_t* offs, cudaStream_t st);
+void launch_batch_emit(const float4* tri, uint32_t T, const uint32_t* tri_off, const BatchScene* scenes,
+                       uint32_t ns, const uint32_t* offs, uint64_t* keys, uint32_t capacity,
+                       uint32_t* err, cudaStream_t st);
+void launch_ranges(const uint64_t* keys, uint32_t n, uint2* ranges, uint32_t* indices,
+                   const float4* tri, uint32_t T, float4* rtri, cudaStream_t st);
+
 // trace.cu
 struct CamView;
 CamView make_camera(const shn_camera* c);
