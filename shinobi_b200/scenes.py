@@ -275,3 +275,80 @@ CAMERA_CLUSTER = Camera((0.0, 0.0, -0.25), (0.0, 0.0, 1.0), (0.0, 1.0, 0.0), 45.
 # Camera of the heightfield path-tracing case: above the field looking down at 45 deg.
 CAMERA_HEIGHTFIELD = Camera((0.5, -0.35, 0.65), (0.0, 0.70710678, -0.70710678),
                             (0.0, 0.0, 1.0), 45.0, 1920, 1080)
+
+
+# ---------------------------------------------------------------------------
+# Device-side generation (torch on CUDA) for the large batched workloads: the
+# same Philox counters and float32 arithmetic as the numpy functions above,
+# so the outputs are identical, only produced on the GPU.
+def _philox_torch(c0, c1, c2, c3, k0: int, k1: int):
+    import torch
+    m = 0xFFFFFFFF
+    M0t, M1t = 0xD2511F53, 0xCD9E8D57
+    k0 &= m
+    k1 &= m
+    for _ in range(10):
+        p0 = c0 * M0t
+        p1 = c2 * M1t
+        h0 = (p0 >> 32) & m
+        l0 = p0 & m
+        h1 = (p1 >> 32) & m
+        l1 = p1 & m
+        n0 = h1 ^ c1 ^ k0
+        n2 = h0 ^ c3 ^ k1
+        c0, c1, c2, c3 = n0, l1, n2, l0
+        k0 = (k0 + W0) & m
+        k1 = (k1 + W1) & m
+    return c0, c1, c2, c3
+
+
+def _u01_torch(w):
+    import torch
+    return (w >> 8).to(torch.float32) * torch.tensor(1.0 / 16777216.0, dtype=torch.float32, device=w.device)
+
+
+def uniform_soup_device(n: int, seed: int = 0, offset_scale: float = 0.01, device="cuda", chunk=1 << 22):
+    """uniform_soup generated on the GPU: returns (vertices (3n,3) float32, indices (n,3) int32)."""
+    import torch
+    verts = torch.empty(3 * n, 3, dtype=torch.float32, device=device)
+    s = torch.tensor(offset_scale, dtype=torch.float32, device=device)
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        ids = torch.arange(a, b, dtype=torch.int64, device=device)
+        zero = torch.zeros_like(ids)
+        u = []
+        for blk in range(3):
+            w = _philox_torch(ids, zero + blk, zero, zero, seed, TAG_SOUP)
+            u.extend(_u01_torch(x) for x in w)
+        c = torch.stack(u[0:3], dim=1)
+        off = (torch.stack(u[3:12], dim=1).reshape(-1, 3, 3) * 2.0 - 1.0) * s
+        verts[3 * a:3 * b] = (c[:, None, :] + off).reshape(-1, 3)
+    idx = torch.arange(3 * n, dtype=torch.int32, device=device).reshape(n, 3)
+    return verts, idx
+
+
+def random_rays_device(n: int, seed: int, lo: float = -1.0, hi: float = 2.0, stream: int = 0,
+                       device="cuda"):
+    """random_rays generated on the GPU (float64 trigonometry, then float32)."""
+    import torch
+    ids = torch.arange(n, dtype=torch.int64, device=device)
+    zero = torch.zeros_like(ids)
+    w = _philox_torch(ids, zero, zero + stream, zero, seed, TAG_RAYS)
+    w2 = _philox_torch(ids, zero + 1, zero + stream, zero, seed, TAG_RAYS)
+    u = [_u01_torch(x) for x in w] + [_u01_torch(w2[0])]
+    span = torch.tensor(hi - lo, dtype=torch.float32, device=device)
+    org = torch.stack(u[0:3], dim=1) * span + torch.tensor(lo, dtype=torch.float32, device=device)
+    z = 2.0 * u[3].double() - 1.0
+    phi = 2.0 * math.pi * u[4].double()
+    rho = torch.sqrt(torch.clamp(1.0 - z * z, min=0.0))
+    d = torch.stack([rho * torch.cos(phi), rho * torch.sin(phi), z], dim=1).float()
+    return org.contiguous(), d.contiguous()
+
+
+def batch_workload_sizes(num_scenes: int = 256, seed: int = 3):
+    """Per-scene triangle counts log-U[1K, 2M], offset scales log-U[0.001, 0.05], ray counts log-U[64K, 1M]."""
+    tris = log_uniform_ints(num_scenes, 1e3, 2e6, seed, TAG_BATCH, 0)
+    u = uniform_draws(num_scenes, 1, seed, TAG_BATCH, stream=1)[:, 0].astype(np.float64)
+    scales = np.exp(math.log(0.001) + u * (math.log(0.05) - math.log(0.001))).astype(np.float32)
+    rays = log_uniform_ints(num_scenes, 65536, 1 << 20, seed, TAG_BATCH, 2)
+    return tris, scales, rays
