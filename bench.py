@@ -47,9 +47,12 @@ def parse():
     ap.add_argument("--cpu-sample-stride", type=int, default=64)
     ap.add_argument("--case", default="full", choices=["full", "small"],
                     help="small: 480x270 camera, for profiler captures (not a bench line)")
-    ap.add_argument("--workload", default="cluster", choices=["cluster", "batch"],
-                    help="cluster: the headline line; batch: 256-scene batched vs one launch per scene")
+    ap.add_argument("--workload", default="cluster", choices=["cluster", "batch", "serve"],
+                    help="cluster: the headline line; batch: 256-scene batched vs one launch per scene; "
+                         "serve: request stream with continuous batching vs one launch per request")
     ap.add_argument("--scenes", type=int, default=256, help="batch workload: number of scenes")
+    ap.add_argument("--requests", type=int, default=20000, help="serve workload: requests per rate")
+    ap.add_argument("--rates", default="1000,5000,20000,50000", help="serve workload: arrival rates (req/s)")
     return ap.parse_args()
 
 
@@ -549,12 +552,105 @@ def run_batch(args):
     bt.close()
 
 
+def run_serve(args):
+    """Served ray-query stream: 64 resident scenes, Poisson arrivals, closest/any mix, 2% updates."""
+    import torch
+
+    import shinobi_b200 as shn
+    from shinobi_b200 import scenes
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    ns = 64
+    tris, scales, _ = scenes.batch_workload_sizes(ns, seed=11)
+    scs = []
+    for i in range(ns):
+        v, t = scenes.uniform_soup_device(int(tris[i]), seed=2000 + i, offset_scale=float(scales[i]))
+        scs.append(scenes.Scene(v.cpu().numpy(), t.cpu().numpy().astype(np.uint32)))
+    repl = []
+    for k in range(8):   # replacement scenes (new seeds) for the update requests
+        i = k % ns
+        v, t = scenes.uniform_soup_device(int(tris[i]), seed=9000 + k, offset_scale=float(scales[i]))
+        repl.append((i, scenes.Scene(v.cpu().numpy(), t.cpu().numpy().astype(np.uint32))))
+    pool_n = 8 << 20
+    o, d = scenes.random_rays_device(pool_n, seed=55)
+    pool = torch.zeros(pool_n, 8, dtype=torch.float32)
+    pool[:, 0:3] = o.cpu()
+    pool[:, 3:6] = d.cpu()
+    pool[:, 6] = 1e30
+    pool = pool.pin_memory()
+    any_pool = pool.clone().pin_memory()
+    any_pool[:, 6] = 0.1
+    out_tri = torch.empty(pool_n, dtype=torch.int32).pin_memory()
+    out_t = torch.empty(pool_n, dtype=torch.float32).pin_memory()
+    rng = np.random.default_rng(99)
+    n_req = args.requests
+    counts = np.floor(np.exp(rng.uniform(np.log(1e3), np.log(1e6), n_req))).astype(np.int64)
+    kinds = (rng.random(n_req) < 0.5).astype(np.int64)
+    slots = rng.integers(0, ns, n_req)
+    is_upd = rng.random(n_req) < 0.02
+    starts = np.array([rng.integers(0, pool_n - c) for c in counts], np.int64)
+    budget = 120 << 30
+    results = {}
+    for coalesce in (True, False):
+        ctx = shn.Context(0, hbm_budget_bytes=budget)
+        srv = shn.Server(ctx=ctx, num_slots=ns, coalesce=coalesce)
+        for i, sc in enumerate(scs):
+            srv.load_scene(i, sc)
+        reqs = []
+        upd_k = 0
+        for k in range(n_req):
+            if is_upd[k]:
+                slot, sc = repl[upd_k % len(repl)]
+                upd_k += 1
+                reqs.append(srv.update_request(slot, sc))
+                continue
+            src = pool if kinds[k] == 0 else any_pool
+            a, c = int(starts[k]), int(counts[k])
+            r = shn._abi.Request()
+            r.kind, r.scene, r.num_rays = int(kinds[k]), int(slots[k]), c
+            r.rays = C_void_p(src.data_ptr() + 32 * a)
+            r.out_tri = C_void_p(out_tri.data_ptr() + 4 * a)
+            r.out_t = C_void_p(out_t.data_ptr() + 4 * a)
+            reqs.append(r)
+        per_rate = {}
+        for rate in [float(x) for x in args.rates.split(",")]:
+            gaps = rng.exponential(1.0 / rate, n_req)
+            arr = np.cumsum(gaps) - gaps[0]
+            srv.stats(reset=True)
+            res = srv.run_schedule(reqs, arr)
+            st = srv.stats(reset=True)
+            per_rate[str(int(rate))] = {"p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3,
+                                        "mrays_per_s": st["mrays_per_s"], "launches": st["launches"],
+                                        "requests": st["requests"], "failed": int((res != 0).sum()),
+                                        "wall_s": st["wall_s"], "offered_mrays_per_s": float(counts[~is_upd].sum()) / arr[-1] / 1e6}
+        results["coalesced" if coalesce else "plain"] = per_rate
+        srv.close()
+        ctx.close()
+    rates = list(results["coalesced"].keys())
+    top = rates[-1]
+    line = {
+        "metric": METRIC, "value": results["coalesced"][top]["mrays_per_s"], "unit": METRIC, "n_gpus": 1,
+        "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded scenes and ray pool)",
+        "config": {"workload": f"served: {ns} resident scenes ({int(tris.sum())} tris), {n_req} requests per rate, "
+                               "rays log-U[1K,1M] from a pinned pool, closest/any p=0.5 (any: length 0.1), "
+                               "2% scene replacements (device rebuild), HBM budget 120 GB",
+                   "rates_req_per_s": rates},
+        "served": results,
+        "speedup_at_rate": {r: results["coalesced"][r]["mrays_per_s"] / max(1e-9, results["plain"][r]["mrays_per_s"]) for r in rates},
+        "p99_ratio_at_rate": {r: results["coalesced"][r]["p99_ms"] / max(1e-9, results["plain"][r]["p99_ms"]) for r in rates},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_shinobi(args)
 

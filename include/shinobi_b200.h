@@ -236,6 +236,65 @@ shn_status shn_batch_export_scene(const shn_batch* b, uint32_t scene, int32_t re
                                   uint32_t* cells, uint32_t* indices, uint64_t* num_refs);
 void shn_batch_destroy(shn_batch* b);
 
+/* ---- ray-query server ------------------------------------------------------------
+ * Resident uniform grids in scene slots, requests admitted by the context's
+ * HBM budget, continuous batching: consecutive ray requests (any scenes,
+ * closest or any hit) are packed into one launch while the previous launch
+ * runs; scene updates rebuild a slot's grid after the requests queued before
+ * them.  coalesce = 0 gives the plain path: one launch per request, no overlap. */
+#define SHN_REQ_CLOSEST 0u
+#define SHN_REQ_ANY 1u
+#define SHN_REQ_UPDATE 2u
+
+typedef struct shn_server shn_server;
+typedef struct shn_server_config {
+  uint32_t num_slots;                /* scene slots (default 64) */
+  uint32_t max_batch_rays;           /* rays per launch and per request (default 4M) */
+  uint32_t max_requests_per_launch;  /* default 4096 */
+  uint32_t max_queue;                /* 0 = unbounded; else submit returns SHN_ERR_BUSY when full */
+  uint32_t coalesce;                 /* 1 = continuous batching (default), 0 = one launch per request */
+} shn_server_config;
+
+typedef struct shn_request {
+  uint32_t kind;       /* SHN_REQ_CLOSEST / SHN_REQ_ANY / SHN_REQ_UPDATE */
+  uint32_t scene;      /* slot */
+  uint32_t num_rays;
+  const float* rays;   /* host, 8 floats per ray: ox oy oz dx dy dz tmax (unused); pinned for overlap */
+  uint32_t* out_tri;   /* host, may be NULL: hit triangle (closest) / any hit (SHN_MISS = not occluded) */
+  float* out_t;        /* host, may be NULL */
+  /* SHN_REQ_UPDATE: new scene for the slot (host arrays, read during processing) */
+  const float* vtx;
+  uint32_t nv;
+  const uint32_t* idx;
+  uint32_t nt;
+  float lambda;
+} shn_request;
+
+typedef struct shn_server_stats {
+  uint64_t requests, updates, rays, launches, max_requests_per_launch;
+  double p50_us, p99_us, max_us, mean_us;  /* submit -> completion latency */
+  double wall_s;                           /* first submit -> last completion */
+  double mrays_per_s;
+} shn_server_stats;
+
+void shn_server_config_default(shn_server_config* c);
+shn_status shn_server_create(shn_ctx* ctx, const shn_server_config* cfg, shn_server** out);
+/* Synchronous initial load of a slot (only while no request is pending). */
+shn_status shn_server_load_scene(shn_server* s, uint32_t slot, const float* vtx_xyz, uint32_t nv,
+                                 const uint32_t* idx, uint32_t nt, float lambda);
+shn_status shn_server_submit(shn_server* s, const shn_request* r, uint64_t* ticket);
+/* Waits up to timeout_ms; SHN_OK with *result set when done (the ticket is
+ * released), SHN_ERR_BUSY if still pending. */
+shn_status shn_server_wait(shn_server* s, uint64_t ticket, uint32_t timeout_ms, shn_status* result);
+shn_status shn_server_poll(shn_server* s, uint64_t ticket, shn_status* result);
+shn_status shn_server_drain(shn_server* s, uint32_t timeout_ms);
+shn_status shn_server_get_stats(shn_server* s, shn_server_stats* out, int reset);
+/* Load generator: submits reqs[i] at arrival_s[i] seconds after the call
+ * (from the calling thread), then waits for all; results (optional) per request. */
+shn_status shn_server_run_schedule(shn_server* s, uint32_t n, const shn_request* reqs,
+                                   const double* arrival_s, shn_status* results);
+void shn_server_destroy(shn_server* s);
+
 /* ---- path tracer --------------------------------------------------------------- */
 typedef struct shn_pt_params {
   uint32_t spp;              /* samples per pixel */

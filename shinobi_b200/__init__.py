@@ -415,6 +415,90 @@ class Batch:
             pass
 
 
+class Server:
+    """Ray-query server (continuous batching over resident grids)."""
+
+    def __init__(self, ctx: Context | None = None, num_slots=64, max_batch_rays=4 << 20,
+                 max_requests_per_launch=4096, max_queue=0, coalesce=True):
+        self.ctx = ctx or default_context()
+        cfg = _abi.ServerConfig()
+        self.ctx.lib.shn_server_config_default(C.byref(cfg))
+        cfg.num_slots, cfg.max_batch_rays = num_slots, max_batch_rays
+        cfg.max_requests_per_launch, cfg.max_queue, cfg.coalesce = max_requests_per_launch, max_queue, int(coalesce)
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.shn_server_create(self.ctx.handle, C.byref(cfg), C.byref(h)), "shn_server_create")
+        self.handle = h
+        self._keep = {}
+
+    def load_scene(self, slot, scene, lambda_=5.0):
+        v = np.ascontiguousarray(scene.vertices, np.float32)
+        i = np.ascontiguousarray(scene.indices, np.uint32)
+        self.ctx.check(self.ctx.lib.shn_server_load_scene(self.handle, slot, v.ctypes.data_as(C.c_void_p), v.shape[0],
+                                                          i.ctypes.data_as(C.c_void_p), i.shape[0], lambda_),
+                       "shn_server_load_scene")
+
+    @staticmethod
+    def ray_request(kind, slot, rays8, out_tri=None, out_t=None) -> _abi.Request:
+        """rays8: (n, 8) float32 host array (pinned for overlap): ox oy oz dx dy dz tmax pad."""
+        r = _abi.Request()
+        r.kind, r.scene, r.num_rays = kind, slot, rays8.shape[0]
+        r.rays = rays8.ctypes.data_as(C.c_void_p) if isinstance(rays8, np.ndarray) else C.c_void_p(rays8.data_ptr())
+        if out_tri is not None:
+            r.out_tri = out_tri.ctypes.data_as(C.c_void_p) if isinstance(out_tri, np.ndarray) else C.c_void_p(out_tri.data_ptr())
+        if out_t is not None:
+            r.out_t = out_t.ctypes.data_as(C.c_void_p) if isinstance(out_t, np.ndarray) else C.c_void_p(out_t.data_ptr())
+        return r
+
+    def update_request(self, slot, scene, lambda_=5.0) -> _abi.Request:
+        v = np.ascontiguousarray(scene.vertices, np.float32)
+        i = np.ascontiguousarray(scene.indices, np.uint32)
+        self._keep[id(v)] = (v, i)
+        r = _abi.Request()
+        r.kind, r.scene = _abi.SHN_REQ_UPDATE, slot
+        r.vtx, r.nv = v.ctypes.data_as(C.c_void_p), v.shape[0]
+        r.idx, r.nt = i.ctypes.data_as(C.c_void_p), i.shape[0]
+        r.lambda_ = lambda_
+        return r
+
+    def submit(self, req) -> int:
+        t = C.c_uint64()
+        self.ctx.check(self.ctx.lib.shn_server_submit(self.handle, C.byref(req), C.byref(t)), "shn_server_submit")
+        return t.value
+
+    def wait(self, ticket, timeout_ms=60000) -> int:
+        res = C.c_int32()
+        st = self.ctx.lib.shn_server_wait(self.handle, ticket, timeout_ms, C.byref(res))
+        self.ctx.check(st, "shn_server_wait")
+        return res.value
+
+    def run_schedule(self, reqs, arrival_s):
+        arr = (_abi.Request * len(reqs))(*reqs)
+        t = np.ascontiguousarray(arrival_s, np.float64)
+        res = np.zeros(len(reqs), np.int32)
+        self.ctx.lib.shn_server_run_schedule(self.handle, len(reqs), arr, t.ctypes.data_as(C.c_void_p),
+                                            res.ctypes.data_as(C.c_void_p))
+        return res
+
+    def stats(self, reset=False) -> dict:
+        st = _abi.ServerStats()
+        self.ctx.check(self.ctx.lib.shn_server_get_stats(self.handle, C.byref(st), int(reset)), "shn_server_get_stats")
+        return {k: getattr(st, k) for k, _ in _abi.ServerStats._fields_}
+
+    def drain(self, timeout_ms=600000):
+        self.ctx.check(self.ctx.lib.shn_server_drain(self.handle, timeout_ms), "shn_server_drain")
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx.lib.shn_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def exclusive_scan(x, ctx: Context | None = None, stream=None):
     """uint32 exclusive scan; returns n+1 values (last = total)."""
     torch = _torch()

@@ -54,6 +54,27 @@ class PtParams(C.Structure):
                 ("light_radiance", f32 * 3), ("background", f32 * 3), ("offset", f32), ("seed", u32)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("num_slots", u32), ("max_batch_rays", u32), ("max_requests_per_launch", u32),
+                ("max_queue", u32), ("coalesce", u32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("kind", u32), ("scene", u32), ("num_rays", u32), ("rays", vp), ("out_tri", vp),
+                ("out_t", vp), ("vtx", vp), ("nv", u32), ("idx", vp), ("nt", u32), ("lambda_", f32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("requests", u64), ("updates", u64), ("rays", u64), ("launches", u64),
+                ("max_requests_per_launch", u64), ("p50_us", C.c_double), ("p99_us", C.c_double),
+                ("max_us", C.c_double), ("mean_us", C.c_double), ("wall_s", C.c_double),
+                ("mrays_per_s", C.c_double)]
+
+
+SHN_REQ_CLOSEST = 0
+SHN_REQ_ANY = 1
+SHN_REQ_UPDATE = 2
+
 # name -> (argtypes, restype)
 SIGNATURES = {
     "shn_abi_version": ([], u32),
@@ -88,6 +109,16 @@ SIGNATURES = {
     "shn_batch_info": ([vp, vp, vp, vp], i32),
     "shn_batch_export_scene": ([vp, u32, vp, vp, vp, vp, vp], i32),
     "shn_batch_destroy": ([vp], None),
+    "shn_server_config_default": ([C.POINTER(ServerConfig)], None),
+    "shn_server_create": ([vp, C.POINTER(ServerConfig), C.POINTER(vp)], i32),
+    "shn_server_load_scene": ([vp, u32, vp, u32, vp, u32, f32], i32),
+    "shn_server_submit": ([vp, C.POINTER(Request), C.POINTER(u64)], i32),
+    "shn_server_wait": ([vp, u64, u32, C.POINTER(i32)], i32),
+    "shn_server_poll": ([vp, u64, C.POINTER(i32)], i32),
+    "shn_server_drain": ([vp, u32], i32),
+    "shn_server_get_stats": ([vp, C.POINTER(ServerStats), i32], i32),
+    "shn_server_run_schedule": ([vp, u32, vp, vp, vp], i32),
+    "shn_server_destroy": ([vp], None),
     "shn_pt_params_default": ([C.POINTER(PtParams)], None),
     "shn_pt_render": ([vp, vp, C.POINTER(Camera), C.POINTER(PtParams), vp, vp, vp], i32),
     "shn_exclusive_scan_u32": ([vp, vp, vp, u32, vp], i32),

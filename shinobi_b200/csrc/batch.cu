@@ -72,9 +72,11 @@ struct BatchAcc {
 
 struct BatchAccW {
   BatchAcc a;
+  Refs r;
   SHN_D const Geom& geom(uint32_t s) const { return a.geom(s); }
   SHN_D const uint2* cells(uint32_t s) const { return a.cells_of(s); }
   SHN_D const uint2* leaves(uint32_t) const { return nullptr; }
+  SHN_D Refs refs(uint32_t) const { return r; }
 };
 
 struct RaysV {
@@ -88,8 +90,8 @@ __global__ void __launch_bounds__(kBatchTraceBlock) k_batch_trace(GridView G, Ba
                                                                  uint32_t* otri, float* ot, float* ou,
                                                                  float* ov, uint8_t* occ) {
   warp_trace_acc<0, ANY>(
-      G, BatchAccW{A}, n, counter,
-      [&](uint32_t i, V3& o, V3& d, float& tmax, uint32_t& scene) {
+      BatchAccW{A, refs_of(G)}, n, counter,
+      [&](uint32_t i, V3& o, V3& d, float& tmax, uint32_t& scene, uint32_t&) {
         uint32_t lo = 0, hi = ns;
         while (hi - lo > 1) {
           const uint32_t mid = (lo + hi) >> 1;

@@ -1,0 +1,495 @@
+// Ray-query server: resident grids, admission by memory budget, continuous
+// batching.
+//
+// A worker thread takes requests from a FIFO queue and packs consecutive ray
+// requests -- for any resident scenes, closest-hit or any-hit -- into ONE
+// launch of a mixed-scene persistent trace kernel (each lane looks up its
+// request's grid in a segment table), up to the staging capacity.  Two
+// launch slots alternate, so requests that arrive while one launch is on the
+// GPU are packed and copied in for the next one (continuous batching); a
+// completer thread finishes launches in order, copies results out and
+// records per-request latency.  Scene-update requests rebuild a slot's grid
+// on the device after the launches queued before them have finished, so
+// every request sees the scene as of its submission order.  With coalescing
+// off, every request gets its own launch and nothing overlaps: the plain
+// one-launch-per-request path, same kernel.
+//
+// The reference's closest analogue is DynamicRTEngine's two-stream
+// rebuild/render overlap (src/Engine/DynamicRTEngine.h:91-147).
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+#include <unordered_map>
+
+#include "internal.h"
+#include "trace_coop.cuh"
+
+namespace shn {
+namespace {
+
+constexpr int kServeBlock = 128;
+
+struct ServeSeg {
+  uint32_t ray_begin;
+  uint32_t anyhit;
+  GridView g;
+};
+
+struct ServeAcc {
+  const ServeSeg* __restrict__ segs;
+  SHN_D const Geom& geom(uint32_t s) const { return segs[s].g.g; }
+  SHN_D const uint2* cells(uint32_t s) const { return segs[s].g.cells; }
+  SHN_D const uint2* leaves(uint32_t s) const { return segs[s].g.leaves; }
+  SHN_D Refs refs(uint32_t s) const { return Refs{segs[s].g.rv0, segs[s].g.rv1, segs[s].g.rv2}; }
+};
+
+// Rays are AoS records of 8 floats: ox, oy, oz, dx, dy, dz, tmax, unused.
+__global__ void __launch_bounds__(kServeBlock) k_serve_trace(const ServeSeg* __restrict__ segs, uint32_t nseg,
+                                                            const float4* __restrict__ rays, uint32_t n,
+                                                            uint32_t* counter, uint32_t* __restrict__ otri,
+                                                            float* __restrict__ ot) {
+  warp_trace_acc<0, false>(
+      ServeAcc{segs}, n, counter,
+      [&](uint32_t i, V3& o, V3& d, float& tmax, uint32_t& seg, uint32_t& anyhit) {
+        uint32_t lo = 0, hi = nseg;
+        while (hi - lo > 1) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (segs[mid].ray_begin <= i) lo = mid; else hi = mid;
+        }
+        seg = lo;
+        anyhit = segs[lo].anyhit;
+        const float4 a = rays[2 * (size_t)i], b = rays[2 * (size_t)i + 1];
+        o = mk(a.x, a.y, a.z);
+        d = mk(a.w, b.x, b.y);
+        tmax = b.z;
+      },
+      [&](uint32_t i, const Hit& h, uint32_t, uint32_t, uint32_t) {
+        otri[i] = h.tri;
+        ot[i] = h.t;
+      });
+}
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+}  // namespace shn
+
+using namespace shn;
+
+struct ServeReq {
+  shn_request r;
+  uint64_t ticket = 0;
+  double t_submit = 0.0, t_done = 0.0;
+  shn_status result = SHN_OK;
+  bool done = false;
+};
+
+struct ServeLaunch {
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev_done = nullptr;
+  float4* d_rays = nullptr;
+  uint32_t* d_tri = nullptr;
+  float* d_t = nullptr;
+  ServeSeg* d_segs = nullptr;
+  ServeSeg* h_segs = nullptr;   // pinned
+  uint32_t* d_counter = nullptr;
+  std::vector<ServeReq*> reqs;
+  std::vector<uint32_t> begin;
+  uint32_t nrays = 0;
+  bool busy = false;
+};
+
+struct ServeSlot {
+  shn_scene* scene = nullptr;
+  shn_grid* grid = nullptr;
+};
+
+struct shn_server {
+  shn_ctx* ctx = nullptr;
+  shn_server_config cfg{};
+  std::vector<ServeSlot> slots;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done, cv_launch;
+  std::deque<ServeReq*> queue;
+  std::unordered_map<uint64_t, ServeReq*> reqs;
+  uint64_t next_ticket = 1;
+  bool stop = false;
+  std::thread worker, completer;
+  ServeLaunch L[2];
+  std::deque<int> inflight;
+  int blocks = 0;
+  cudaStream_t update_st = nullptr;
+  // stats
+  std::vector<double> lat_us;
+  uint64_t rays_done = 0, launches = 0, requests_done = 0, updates_done = 0;
+  double t_first = 0.0, t_last = 0.0;
+  uint64_t max_requests_per_launch = 0;
+};
+
+namespace {
+
+void complete(shn_server* s, ServeReq* r, shn_status st) {
+  // caller holds s->mu
+  r->result = st;
+  r->done = true;
+  r->t_done = now_s();
+  s->lat_us.push_back((r->t_done - r->t_submit) * 1e6);
+  s->requests_done++;
+  if (r->r.kind != SHN_REQ_UPDATE) s->rays_done += r->r.num_rays;
+  s->t_last = r->t_done;
+  s->cv_done.notify_all();
+}
+
+shn_status load_slot(shn_server* s, uint32_t slot, const float* vtx, uint32_t nv, const uint32_t* idx,
+                     uint32_t nt, float lambda, cudaStream_t st) {
+  shn_scene* sc = nullptr;
+  shn_status rc = shn_scene_create(s->ctx, vtx, nv, idx, nt, SHN_MEM_HOST, st, &sc);
+  if (rc) return rc;
+  shn_grid* g = nullptr;
+  shn_grid_create(s->ctx, &g);
+  shn_grid_params p;
+  shn_grid_params_default(SHN_GRID_UNIFORM, &p);
+  p.lambda = lambda > 0.f ? lambda : 5.f;
+  rc = shn_grid_build(g, sc, &p, st);
+  if (rc) {
+    shn_grid_destroy(g);
+    shn_scene_destroy(sc);
+    return rc;
+  }
+  cudaStreamSynchronize(st);
+  ServeSlot old = s->slots[slot];
+  s->slots[slot].scene = sc;
+  s->slots[slot].grid = g;
+  if (old.grid) shn_grid_destroy(old.grid);
+  if (old.scene) shn_scene_destroy(old.scene);
+  return SHN_OK;
+}
+
+void worker_main(shn_server* s) {
+  cudaSetDevice(s->ctx->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  int next_slot = 0;
+  while (true) {
+    s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
+    if (s->queue.empty() && s->stop) break;
+    ServeReq* head = s->queue.front();
+    if (head->r.kind == SHN_REQ_UPDATE) {
+      // every launch queued before the update must finish first
+      s->cv_launch.wait(lk, [&] { return s->inflight.empty(); });
+      s->queue.pop_front();
+      const shn_request& q = head->r;
+      lk.unlock();
+      shn_status rc = (q.scene < s->slots.size())
+                          ? load_slot(s, q.scene, q.vtx, q.nv, q.idx, q.nt, q.lambda, s->update_st)
+                          : SHN_ERR_INVALID;
+      lk.lock();
+      s->updates_done++;
+      complete(s, head, rc);
+      continue;
+    }
+    // a free launch slot
+    s->cv_launch.wait(lk, [&] { return !s->L[next_slot].busy; });
+    ServeLaunch& la = s->L[next_slot];
+    la.reqs.clear();
+    la.begin.clear();
+    uint32_t total = 0;
+    while (!s->queue.empty()) {
+      ServeReq* r = s->queue.front();
+      if (r->r.kind == SHN_REQ_UPDATE) break;
+      if (!la.reqs.empty() && (!s->cfg.coalesce || total + r->r.num_rays > s->cfg.max_batch_rays ||
+                               la.reqs.size() >= s->cfg.max_requests_per_launch))
+        break;
+      s->queue.pop_front();
+      if (r->r.scene >= s->slots.size() || !s->slots[r->r.scene].grid) {
+        complete(s, r, SHN_ERR_INVALID);
+        continue;
+      }
+      la.begin.push_back(total);
+      la.reqs.push_back(r);
+      total += r->r.num_rays;
+    }
+    if (la.reqs.empty()) continue;
+    la.busy = true;
+    la.nrays = total;
+    // segment table (grid views of the scenes as of now)
+    for (size_t k = 0; k < la.reqs.size(); ++k) {
+      const ServeReq* r = la.reqs[k];
+      const shn_grid* g = s->slots[r->r.scene].grid;
+      ServeSeg& sg = la.h_segs[k];
+      sg.ray_begin = la.begin[k];
+      sg.anyhit = r->r.kind == SHN_REQ_ANY ? 1u : 0u;
+      sg.g.g = g->geom;
+      sg.g.kind = g->kind;
+      sg.g.cells = g->cells;
+      sg.g.leaves = g->leaves;
+      sg.g.rv0 = g->rtri;
+      sg.g.rv1 = g->rtri + g->num_refs;
+      sg.g.rv2 = g->rtri + 2 * g->num_refs;
+    }
+    s->max_requests_per_launch = std::max<uint64_t>(s->max_requests_per_launch, la.reqs.size());
+    const uint32_t nseg = (uint32_t)la.reqs.size();
+    lk.unlock();
+    cudaMemcpyAsync(la.d_segs, la.h_segs, sizeof(ServeSeg) * nseg, cudaMemcpyHostToDevice, la.st);
+    for (size_t k = 0; k < la.reqs.size(); ++k) {
+      const shn_request& q = la.reqs[k]->r;
+      cudaMemcpyAsync(la.d_rays + 2 * (size_t)la.begin[k], q.rays, 32 * (size_t)q.num_rays,
+                      cudaMemcpyHostToDevice, la.st);
+    }
+    cudaMemsetAsync(la.d_counter, 0, 4, la.st);
+    k_serve_trace<<<s->blocks, kServeBlock, 0, la.st>>>(la.d_segs, nseg, la.d_rays, total, la.d_counter,
+                                                        la.d_tri, la.d_t);
+    for (size_t k = 0; k < la.reqs.size(); ++k) {
+      const shn_request& q = la.reqs[k]->r;
+      if (q.out_tri)
+        cudaMemcpyAsync(q.out_tri, la.d_tri + la.begin[k], 4 * (size_t)q.num_rays, cudaMemcpyDeviceToHost, la.st);
+      if (q.out_t)
+        cudaMemcpyAsync(q.out_t, la.d_t + la.begin[k], 4 * (size_t)q.num_rays, cudaMemcpyDeviceToHost, la.st);
+    }
+    cudaEventRecord(la.ev_done, la.st);
+    lk.lock();
+    s->launches++;
+    s->inflight.push_back(next_slot);
+    s->cv_done.notify_all();
+    if (!s->cfg.coalesce) {
+      // plain path: one request, one launch, nothing overlaps
+      s->cv_launch.wait(lk, [&] { return s->inflight.empty(); });
+    }
+    next_slot ^= 1;
+  }
+}
+
+void completer_main(shn_server* s) {
+  cudaSetDevice(s->ctx->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (true) {
+    s->cv_done.wait(lk, [&] { return !s->inflight.empty() || (s->stop && s->queue.empty() && s->inflight.empty()); });
+    if (s->inflight.empty()) {
+      if (s->stop && s->queue.empty()) break;
+      continue;
+    }
+    const int li = s->inflight.front();
+    ServeLaunch& la = s->L[li];
+    lk.unlock();
+    const cudaError_t e = cudaEventSynchronize(la.ev_done);
+    lk.lock();
+    const shn_status st = e == cudaSuccess ? SHN_OK : SHN_ERR_CUDA;
+    for (ServeReq* r : la.reqs) complete(s, r, st);
+    la.reqs.clear();
+    la.busy = false;
+    s->inflight.pop_front();
+    s->cv_launch.notify_all();
+    s->cv_work.notify_all();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void shn_server_config_default(shn_server_config* c) {
+  if (!c) return;
+  memset(c, 0, sizeof(*c));
+  c->num_slots = 64;
+  c->max_batch_rays = 4u << 20;
+  c->max_requests_per_launch = 4096;
+  c->coalesce = 1;
+}
+
+shn_status shn_server_create(shn_ctx* ctx, const shn_server_config* cfg, shn_server** out) {
+  if (!ctx || !cfg || !out || cfg->num_slots == 0 || cfg->max_batch_rays == 0 || cfg->max_requests_per_launch == 0)
+    return SHN_ERR_INVALID;
+  *out = nullptr;
+  shn_server* s = new shn_server();
+  s->ctx = ctx;
+  s->cfg = *cfg;
+  s->slots.resize(cfg->num_slots);
+  cudaStreamCreateWithFlags(&s->update_st, cudaStreamNonBlocking);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_serve_trace, kServeBlock, 0);
+  s->blocks = std::max(1, per_sm) * ctx->num_sms;
+  const size_t cap = cfg->max_batch_rays;
+  for (int i = 0; i < 2; ++i) {
+    ServeLaunch& la = s->L[i];
+    cudaStreamCreateWithFlags(&la.st, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&la.ev_done, cudaEventDisableTiming);
+    cudaError_t e = dev_alloc(ctx, (void**)&la.d_rays, 32 * cap, la.st);
+    if (e == cudaSuccess) e = dev_alloc(ctx, (void**)&la.d_tri, 4 * cap, la.st);
+    if (e == cudaSuccess) e = dev_alloc(ctx, (void**)&la.d_t, 4 * cap, la.st);
+    if (e == cudaSuccess) e = dev_alloc(ctx, (void**)&la.d_segs, sizeof(ServeSeg) * cfg->max_requests_per_launch, la.st);
+    if (e == cudaSuccess) e = dev_alloc(ctx, (void**)&la.d_counter, 64, la.st);
+    if (e == cudaSuccess) e = cudaMallocHost(&la.h_segs, sizeof(ServeSeg) * cfg->max_requests_per_launch);
+    if (e != cudaSuccess) {
+      shn_server_destroy(s);
+      return set_error(ctx, e == cudaErrorNotPermitted ? SHN_ERR_BUDGET : SHN_ERR_OOM, "server staging");
+    }
+  }
+  s->worker = std::thread(worker_main, s);
+  s->completer = std::thread(completer_main, s);
+  *out = s;
+  return SHN_OK;
+}
+
+shn_status shn_server_load_scene(shn_server* s, uint32_t slot, const float* vtx_xyz, uint32_t nv,
+                                 const uint32_t* idx, uint32_t nt, float lambda) {
+  if (!s || slot >= s->slots.size()) return SHN_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (!s->inflight.empty() || !s->queue.empty())
+    return set_error(s->ctx, SHN_ERR_BUSY, "load_scene while requests are pending; submit an update request");
+  return load_slot(s, slot, vtx_xyz, nv, idx, nt, lambda, s->update_st);
+}
+
+shn_status shn_server_submit(shn_server* s, const shn_request* r, uint64_t* ticket) {
+  if (!s || !r || !ticket) return SHN_ERR_INVALID;
+  if (r->kind > SHN_REQ_UPDATE) return SHN_ERR_INVALID;
+  if (r->kind != SHN_REQ_UPDATE) {
+    if (r->num_rays == 0 || !r->rays || r->num_rays > s->cfg.max_batch_rays)
+      return set_error(s->ctx, SHN_ERR_INVALID, "request rays empty or above max_batch_rays");
+  }
+  ServeReq* q = new ServeReq();
+  q->r = *r;
+  q->t_submit = now_s();
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stop) {
+    delete q;
+    return SHN_ERR_CANCELLED;
+  }
+  if (s->cfg.max_queue && s->queue.size() >= s->cfg.max_queue) {
+    delete q;
+    return SHN_ERR_BUSY;
+  }
+  q->ticket = s->next_ticket++;
+  if (s->t_first == 0.0) s->t_first = q->t_submit;
+  s->reqs[q->ticket] = q;
+  s->queue.push_back(q);
+  *ticket = q->ticket;
+  s->cv_work.notify_one();
+  return SHN_OK;
+}
+
+shn_status shn_server_wait(shn_server* s, uint64_t ticket, uint32_t timeout_ms, shn_status* result) {
+  if (!s) return SHN_ERR_INVALID;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return SHN_ERR_INVALID;
+  ServeReq* q = it->second;
+  const bool ok = s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return q->done; });
+  if (!ok) return SHN_ERR_BUSY;
+  if (result) *result = q->result;
+  s->reqs.erase(it);
+  delete q;
+  return SHN_OK;
+}
+
+shn_status shn_server_poll(shn_server* s, uint64_t ticket, shn_status* result) {
+  return shn_server_wait(s, ticket, 0, result);
+}
+
+shn_status shn_server_drain(shn_server* s, uint32_t timeout_ms) {
+  if (!s) return SHN_ERR_INVALID;
+  std::unique_lock<std::mutex> lk(s->mu);
+  const bool ok = s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms),
+                                      [&] { return s->queue.empty() && s->inflight.empty(); });
+  return ok ? SHN_OK : SHN_ERR_BUSY;
+}
+
+shn_status shn_server_get_stats(shn_server* s, shn_server_stats* out, int reset) {
+  if (!s || !out) return SHN_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  memset(out, 0, sizeof(*out));
+  out->requests = s->requests_done;
+  out->updates = s->updates_done;
+  out->rays = s->rays_done;
+  out->launches = s->launches;
+  out->max_requests_per_launch = s->max_requests_per_launch;
+  std::vector<double> v = s->lat_us;
+  std::sort(v.begin(), v.end());
+  if (!v.empty()) {
+    out->p50_us = v[(size_t)(0.50 * (v.size() - 1))];
+    out->p99_us = v[(size_t)(0.99 * (v.size() - 1))];
+    out->max_us = v.back();
+    double sum = 0;
+    for (double x : v) sum += x;
+    out->mean_us = sum / v.size();
+  }
+  out->wall_s = s->t_last > s->t_first ? s->t_last - s->t_first : 0.0;
+  out->mrays_per_s = out->wall_s > 0 ? s->rays_done / out->wall_s / 1e6 : 0.0;
+  if (reset) {
+    s->lat_us.clear();
+    s->rays_done = s->launches = s->requests_done = s->updates_done = 0;
+    s->t_first = s->t_last = 0.0;
+    s->max_requests_per_launch = 0;
+  }
+  return SHN_OK;
+}
+
+shn_status shn_server_run_schedule(shn_server* s, uint32_t n, const shn_request* reqs,
+                                   const double* arrival_s, shn_status* results) {
+  if (!s || (n && (!reqs || !arrival_s))) return SHN_ERR_INVALID;
+  std::vector<uint64_t> tickets(n, 0);
+  std::vector<shn_status> sub(n, SHN_OK);
+  const double t0 = now_s();
+  for (uint32_t i = 0; i < n; ++i) {
+    const double due = t0 + arrival_s[i];
+    while (true) {
+      const double t = now_s();
+      if (t >= due) break;
+      if (due - t > 2e-4) std::this_thread::sleep_for(std::chrono::microseconds((long)((due - t - 1e-4) * 1e6)));
+    }
+    sub[i] = shn_server_submit(s, &reqs[i], &tickets[i]);
+  }
+  shn_status rc = SHN_OK;
+  for (uint32_t i = 0; i < n; ++i) {
+    shn_status r = sub[i];
+    if (r == SHN_OK) {
+      shn_status w = shn_server_wait(s, tickets[i], 600000, &r);
+      if (w != SHN_OK) r = w;
+    }
+    if (results) results[i] = r;
+    if (r != SHN_OK && rc == SHN_OK) rc = r;
+  }
+  return rc;
+}
+
+void shn_server_destroy(shn_server* s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  s->cv_done.notify_all();
+  s->cv_launch.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->cv_done.notify_all();
+  }
+  if (s->completer.joinable()) s->completer.join();
+  cudaDeviceSynchronize();
+  for (auto& kv : s->reqs) delete kv.second;
+  for (auto& sl : s->slots) {
+    if (sl.grid) shn_grid_destroy(sl.grid);
+    if (sl.scene) shn_scene_destroy(sl.scene);
+  }
+  for (int i = 0; i < 2; ++i) {
+    ServeLaunch& la = s->L[i];
+    dev_free(s->ctx, la.d_rays, 32 * (size_t)s->cfg.max_batch_rays, la.st);
+    dev_free(s->ctx, la.d_tri, 4 * (size_t)s->cfg.max_batch_rays, la.st);
+    dev_free(s->ctx, la.d_t, 4 * (size_t)s->cfg.max_batch_rays, la.st);
+    dev_free(s->ctx, la.d_segs, sizeof(ServeSeg) * s->cfg.max_requests_per_launch, la.st);
+    dev_free(s->ctx, la.d_counter, 64, la.st);
+    if (la.h_segs) cudaFreeHost(la.h_segs);
+    if (la.ev_done) cudaEventDestroy(la.ev_done);
+    if (la.st) {
+      cudaStreamSynchronize(la.st);
+      cudaStreamDestroy(la.st);
+    }
+  }
+  if (s->update_st) cudaStreamDestroy(s->update_st);
+  delete s;
+}
+
+}  // extern "C"

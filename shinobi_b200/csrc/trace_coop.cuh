@@ -26,6 +26,14 @@ namespace shn {
 
 constexpr uint32_t kCoopThreshold = 32;
 
+// Reference-ordered triangle arrays of one grid.
+struct Refs {
+  const float4* __restrict__ rv0;
+  const float4* __restrict__ rv1;
+  const float4* __restrict__ rv2;
+};
+SHN_D Refs refs_of(const GridView& G) { return Refs{G.rv0, G.rv1, G.rv2}; }
+
 enum : uint32_t { ST_DONE = 0, ST_TOP = 1, ST_LEAF = 2, ST_LEAF_TESTED = 3, ST_TOP_NEXT = 4, ST_U_TESTED = 5 };
 
 struct Lane {
@@ -42,6 +50,7 @@ struct Lane {
   int vis2;
   uint32_t b, e;
   uint32_t st;
+  uint32_t anyhit;        // runtime any-hit flag (mixed launches)
 };
 
 SHN_D RayWT lane_ray(const Lane& L) {
@@ -67,6 +76,7 @@ SHN_D void lane_init(const Geom& g, Lane& L, V3 org, V3 dir, float tmax) {
   L.perm = (uint32_t)w.kx | ((uint32_t)w.ky << 2) | ((uint32_t)w.kz << 4);
   L.tbest = tmax;
   L.best = kMiss;
+  L.anyhit = 0;
   L.st = ST_DONE;
   L.b = L.e = 0;
   if (!(L.tbest > 0.f)) return;
@@ -163,7 +173,7 @@ SHN_D bool lane_advance(const Geom& g, const uint2* __restrict__ cells, const ui
         break;
       }
       case ST_LEAF_TESTED: {
-        if (ANY && L.best != kMiss) {
+        if ((ANY || L.anyhit) && L.best != kMiss) {
           L.st = ST_DONE;
           return false;
         }
@@ -185,7 +195,7 @@ SHN_D bool lane_advance(const Geom& g, const uint2* __restrict__ cells, const ui
       }
       case ST_U_TESTED:
       case ST_TOP_NEXT: {
-        if (ANY && L.best != kMiss) {
+        if ((ANY || L.anyhit) && L.best != kMiss) {
           L.st = ST_DONE;
           return false;
         }
@@ -253,7 +263,7 @@ SHN_D bool wt_test_p(V3 org, float Sx, float Sy, float Sz, float4 p0, float4 p1,
 // Loads of the next 32-reference chunk are issued before the current chunk
 // is tested (register double buffering) to cover the L2 latency.
 template <bool ANY, int KX, int KY, int KZ>
-SHN_D uint64_t warp_range_p(const GridView& G, V3 org, float Sx, float Sy, float Sz, float tbest,
+SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz, float tbest,
                             uint32_t b, uint32_t e, uint32_t& tests) {
   const int lane = threadIdx.x & 31;
   uint64_t key = ~0ull;
@@ -284,7 +294,7 @@ SHN_D uint64_t warp_range_p(const GridView& G, V3 org, float Sx, float Sy, float
 }
 
 template <bool ANY>
-SHN_D uint64_t warp_range(const GridView& G, uint32_t perm, V3 org, float Sx, float Sy, float Sz,
+SHN_D uint64_t warp_range(const Refs& G, uint32_t perm, V3 org, float Sx, float Sy, float Sz,
                           float tbest, uint32_t b, uint32_t e, uint32_t& tests) {
   switch (perm) {
     case (1u | 2u << 2 | 0u << 4): return warp_range_p<ANY, 1, 2, 0>(G, org, Sx, Sy, Sz, tbest, b, e, tests);
@@ -298,7 +308,7 @@ SHN_D uint64_t warp_range(const GridView& G, uint32_t perm, V3 org, float Sx, fl
 
 // Per-lane test of its own (small) range with the generic watertight test.
 template <bool ANY>
-SHN_D void lane_range(const GridView& G, Lane& L, uint32_t& tests) {
+SHN_D void lane_range(const Refs& G, Lane& L, uint32_t& tests) {
   const RayWT w = lane_ray(L);
   for (uint32_t it = L.b; it < L.e; ++it) {
     tests++;
@@ -309,14 +319,14 @@ SHN_D void lane_range(const GridView& G, Lane& L, uint32_t& tests) {
     if (wt_test(w, p0, p1, p2, kEps, L.tbest, t, u, v)) {
       L.tbest = t;
       L.best = it;
-      if (ANY) return;
+      if (ANY || L.anyhit) return;
     }
   }
 }
 
 // Final hit record of a lane: triangle id and barycentrics of the best
 // reference, recomputed with the same arithmetic.
-SHN_D void lane_result(const GridView& G, const Lane& L, Hit& h) {
+SHN_D void lane_result(const Refs& G, const Lane& L, Hit& h) {
   h.t = L.tbest;
   h.tri = kMiss;
   h.u = h.v = 0.f;
@@ -336,8 +346,7 @@ SHN_D void lane_result(const GridView& G, const Lane& L, Hit& h) {
 // scenes.  src(i, org, dir, tmax, scene) generates ray i; sink(i, hit, steps,
 // tests) consumes its result.  n rays are taken from *counter (pre-zeroed).
 template <int KIND, bool ANY, class Acc, class Src, class Sink>
-SHN_D void warp_trace_acc(const GridView& G, const Acc& acc, uint32_t n, uint32_t* counter,
-                          Src&& src, Sink&& sink) {
+SHN_D void warp_trace_acc(const Acc& acc, uint32_t n, uint32_t* counter, Src&& src, Sink&& sink) {
   const int lane = threadIdx.x & 31;
   const uint32_t lt = (1u << lane) - 1u;
   Lane L;
@@ -361,8 +370,10 @@ SHN_D void warp_trace_acc(const GridView& G, const Acc& acc, uint32_t n, uint32_
           steps = tests = 0;
           V3 o, d;
           float tmax;
-          src(r, o, d, tmax, scene);
+          uint32_t anyhit = 0;
+          src(r, o, d, tmax, scene, anyhit);
           lane_init<KIND>(acc.geom(scene), L, o, d, tmax);
+          L.anyhit = anyhit;
         }
       }
     }
@@ -371,7 +382,7 @@ SHN_D void warp_trace_acc(const GridView& G, const Acc& acc, uint32_t n, uint32_
       pending = lane_advance<KIND, ANY>(acc.geom(scene), acc.cells(scene), acc.leaves(scene), L, steps);
       if (!pending) {
         Hit h;
-        lane_result(G, L, h);
+        lane_result(acc.refs(scene), L, h);
         sink(rid, h, steps, tests, scene);
         has = false;
       }
@@ -382,7 +393,7 @@ SHN_D void warp_trace_acc(const GridView& G, const Acc& acc, uint32_t n, uint32_
       continue;
     }
     const bool big = pending && (L.e - L.b > kCoopThreshold);
-    if (pending && !big) lane_range<ANY>(G, L, tests);
+    if (pending && !big) lane_range<ANY>(acc.refs(scene), L, tests);
     uint32_t bmask = __ballot_sync(0xFFFFFFFFu, big);
     while (bmask) {
       const int j = __ffs(bmask) - 1;
@@ -396,8 +407,12 @@ SHN_D void warp_trace_acc(const GridView& G, const Acc& acc, uint32_t n, uint32_
       const float tb = __shfl_sync(0xFFFFFFFFu, L.tbest, j);
       const uint32_t b = __shfl_sync(0xFFFFFFFFu, L.b, j);
       const uint32_t e = __shfl_sync(0xFFFFFFFFu, L.e, j);
+      const uint32_t sj = __shfl_sync(0xFFFFFFFFu, scene, j);
+      const uint32_t aj = __shfl_sync(0xFFFFFFFFu, L.anyhit, j);
+      const Refs R = acc.refs(sj);
       uint32_t wt = 0;
-      const uint64_t key = warp_range<ANY>(G, perm, org, Sx, Sy, Sz, tb, b, e, wt);
+      const uint64_t key = (ANY || aj) ? warp_range<true>(R, perm, org, Sx, Sy, Sz, tb, b, e, wt)
+                                       : warp_range<false>(R, perm, org, Sx, Sy, Sz, tb, b, e, wt);
       if (lane == j) {
         tests += wt;
         if (key != ~0ull) {
@@ -415,13 +430,14 @@ struct OneGrid {
   SHN_D const Geom& geom(uint32_t) const { return G->g; }
   SHN_D const uint2* cells(uint32_t) const { return G->cells; }
   SHN_D const uint2* leaves(uint32_t) const { return G->leaves; }
+  SHN_D Refs refs(uint32_t) const { return refs_of(*G); }
 };
 
 template <int KIND, bool ANY, class Src, class Sink>
 SHN_D void warp_trace(const GridView& G, uint32_t n, uint32_t* counter, Src&& src, Sink&& sink) {
   warp_trace_acc<KIND, ANY>(
-      G, OneGrid{&G}, n, counter,
-      [&](uint32_t i, V3& o, V3& d, float& tmax, uint32_t& scene) {
+      OneGrid{&G}, n, counter,
+      [&](uint32_t i, V3& o, V3& d, float& tmax, uint32_t& scene, uint32_t&) {
         scene = 0;
         src(i, o, d, tmax);
       },
