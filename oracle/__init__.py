@@ -71,6 +71,7 @@ def lib():
         L.orc_trace_brute.argtypes = [vp, vp, u32] + [vp] * 6 + [u32, vp, vp]
         L.orc_t_fp64.argtypes = [vp, vp, vp] + [vp] * 6 + [u32, vp]
         L.orc_sincos_2pi.argtypes = [vp, u32, vp, vp]
+        L.orc_cosine_local.argtypes = [vp, vp, u32, vp]
         L.orc_philox.argtypes = [vp, u32, u32, u32, vp]
         L.orc_camera.argtypes = [vp, vp, vp, f32, u32, u32, vp]
         L.orc_primary_rays.argtypes = [vp, u32, u32, u32, vp, vp, vp]
@@ -249,6 +250,14 @@ def sincos_2pi(u):
     c = np.zeros_like(u)
     lib().orc_sincos_2pi(_p(u), u.size, _p(s), _p(c))
     return s, c
+
+
+def cosine_local(u1, u2) -> np.ndarray:
+    """Cosine-weighted hemisphere directions in the local frame (z = normal)."""
+    u1, u2 = _f32(u1), _f32(u2)
+    out = np.zeros((u1.shape[0], 3), np.float32)
+    lib().orc_cosine_local(_p(u1), _p(u2), u1.shape[0], _p(out))
+    return out
 
 
 def philox(ctr, k0: int, k1: int) -> np.ndarray:

@@ -804,6 +804,20 @@ void orc_sincos_2pi(const float* u, uint32_t n, float* s, float* c) {
   for (uint32_t i = 0; i < n; ++i) sincos_2pi(u[i], s[i], c[i]);
 }
 
+// CosineHemisphereSampler (src/Utils/HemisphereSamplers.hpp:54-72) in the
+// local frame: (sin 2pi u1 * sqrt(1-u2), cos 2pi u1 * sqrt(1-u2), sqrt(u2)),
+// with the deterministic sincos_2pi above.
+void orc_cosine_local(const float* u1, const float* u2, uint32_t n, float* out) {
+  for (uint32_t i = 0; i < n; ++i) {
+    float sn, cs;
+    sincos_2pi(u1[i], sn, cs);
+    const float r = sqrtf(1.f - u2[i]);
+    out[3 * i] = sn * r;
+    out[3 * i + 1] = cs * r;
+    out[3 * i + 2] = sqrtf(u2[i]);
+  }
+}
+
 void orc_philox(const uint32_t* ctr, uint32_t n, uint32_t k0, uint32_t k1, uint32_t* out) {
   for (uint32_t i = 0; i < n; ++i) {
     uint32_t c[4] = {ctr[4 * i], ctr[4 * i + 1], ctr[4 * i + 2], ctr[4 * i + 3]};

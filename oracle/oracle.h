@@ -42,6 +42,7 @@ void orc_t_fp64(const float* vtx, const uint32_t* idx, const uint32_t* tri, cons
                 uint32_t n, double* t64);
 
 void orc_sincos_2pi(const float* u, uint32_t n, float* s, float* c);
+void orc_cosine_local(const float* u1, const float* u2, uint32_t n, float* out);
 void orc_philox(const uint32_t* ctr, uint32_t n, uint32_t k0, uint32_t k1, uint32_t* out);
 void orc_camera(const float eye[3], const float fwd[3], const float up[3], float fov_deg,
                 uint32_t resx, uint32_t resy, float out[9]);
