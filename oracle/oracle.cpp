@@ -17,6 +17,8 @@
 //  * candidate cells rejected by the plane test are not emitted at all, so
 //    no sentinel pairs reach the sorted arrays or indices[]
 //    (reference: src/Control/Algorithm/FastBuildKernels.h:185-192);
+//  * cell centres for the plane test are (i*s + o) + s/2 per cell instead
+//    of an accumulated "+= cellSize" (see lattice_centre);
 //  * normals use 1/sqrtf instead of rsqrtf, divisions are IEEE instead of
 //    __fdividef;
 //  * leaf resolution is floor(cbrt(cs_a^3 * lambda * refs / V)) evaluated
@@ -116,6 +118,17 @@ Geom make_geom(const float b[6], const int res[3]) {
 }
 
 // ---------------------------------------------------------------------------
+// Centre of cell i along one axis of a lattice with cell size s and origin o:
+// (i*s + o) + s/2, evaluated directly for every cell.  The reference starts
+// from the same expression at the first candidate cell and then accumulates
+// "+= cellSize" (src/Control/Algorithm/FastBuildKernels.h:144-164,
+// src/Control/Algorithm/TwoLevelBuildKernels.h:396-420); the direct form
+// differs from the accumulated one only by rounding and makes every cell's
+// plane test independent of the others, which the CUDA build relies on to
+// find the passing cells of a row as one interval.
+inline float lattice_centre(uint32_t i, float s, float o) { return ((float)i * s + o) + s * 0.5f; }
+
+// ---------------------------------------------------------------------------
 // Candidate cell range of a triangle in a uniform grid.
 // Restates countRefs / buildUnsortedGrid, src/Control/Algorithm/FastBuildKernels.h:47-69, 110-133.
 inline void cell_range(const Tri& tri, const Geom& g, uint32_t lo[3], uint32_t hi[3]) {
@@ -139,18 +152,12 @@ inline void for_each_cell(const Tri& tri, const Geom& g, F&& emit) {
   if (hi[0] - lo[0] > 0 && hi[1] - lo[1] > 0 && hi[2] - lo[2] > 0) {
     const V3 n = normalize(cross(sub(tri.v[1], tri.v[0]), sub(tri.v[2], tri.v[0])));
     const V3 half = muls(g.cs, 0.5f);
-    V3 c0 = mk((float)lo[0], (float)lo[1], (float)lo[2]);
-    c0 = mul(c0, g.cs);
-    c0 = add(add(c0, g.gmin), half);
-    float cz = c0.z - g.cs.z;
     for (uint32_t z = lo[2]; z <= hi[2]; ++z) {
-      cz += g.cs.z;
-      float cy = c0.y - g.cs.y;
+      const float cz = lattice_centre(z, g.cs.z, g.gmin.z);
       for (uint32_t y = lo[1]; y <= hi[1]; ++y) {
-        cy += g.cs.y;
-        float cx = c0.x - g.cs.x;
+        const float cy = lattice_centre(y, g.cs.y, g.gmin.y);
         for (uint32_t x = lo[0]; x <= hi[0]; ++x) {
-          cx += g.cs.x;
+          const float cx = lattice_centre(x, g.cs.x, g.gmin.x);
           const float d = dot(sub(mk(cx, cy, cz), tri.v[0]), n);
           const V3 dist = muls(n, d);
           if (fabsf(dist.x) <= half.x + kEps && fabsf(dist.y) <= half.y + kEps &&
@@ -232,18 +239,12 @@ inline void for_each_leaf(const Tri& tri, const Geom& g, uint32_t topCell, uint3
   if (hp[0] - lo[0] > 1 && hp[1] - lo[1] > 1 && hp[2] - lo[2] > 1) {
     const V3 n = normalize(cross(sub(tri.v[1], tri.v[0]), sub(tri.v[2], tri.v[0])));
     const V3 scs = divv(g.cs, cres);
-    V3 c0 = mk((float)lo[0], (float)lo[1], (float)lo[2]);
-    c0 = mul(c0, scs);
-    c0 = add(add(c0, origin), muls(scs, 0.5f));
-    float cz = c0.z - scs.z;
     for (int z = lo[2]; z < hp[2]; ++z) {
-      cz += scs.z;
-      float cy = c0.y - scs.y;
+      const float cz = lattice_centre((uint32_t)z, scs.z, origin.z);
       for (int y = lo[1]; y < hp[1]; ++y) {
-        cy += scs.y;
-        float cx = c0.x - scs.x;
+        const float cy = lattice_centre((uint32_t)y, scs.y, origin.y);
         for (int x = lo[0]; x < hp[0]; ++x) {
-          cx += scs.x;
+          const float cx = lattice_centre((uint32_t)x, scs.x, origin.x);
           const float d = dot(sub(mk(cx, cy, cz), tri.v[0]), n);
           const V3 dist = muls(n, d);
           if (fabsf(dist.x) <= scs.x * 0.5f + kEps && fabsf(dist.y) <= scs.y * 0.5f + kEps &&

@@ -1,18 +1,19 @@
 // Sort-based uniform and two-level grid construction for sm_100a.
 //
 // Pipeline (uniform grid, and the top level of the two-level grid):
-//   k_count_scan_tris   exact per-triangle cell counts (bbox range + plane
-//                       test) fused with a decoupled look-back exclusive scan
-//                       -> per-triangle output offsets and the pair total
-//   k_emit_tris         packed (cell << 32 | tri) keys, triangle order
+//   k_count_units       exact per-triangle cell counts (bbox range + plane
+//                       test, by row intervals: rows.cuh) fused with a
+//                       decoupled look-back exclusive scan -> per-triangle
+//                       output offsets and the pair total
+//   k_emit_units        packed (cell << 32 | tri) keys, triangle order
 //   onesweep_sort       stable 8-bit-digit LSD sort on the cell bits
 //   k_ranges            [begin,end) per cell, indices[] and the
 //                       reference-ordered SoA float4 triangle copy
 // Two-level leaf stage:
 //   k_leaf_cells_scan   leaf resolution per top cell fused with the scan of
 //                       leaf-cell counts -> TwoLevelGridCell words
-//   k_leaf_count_scan   exact leaf-cell counts per sorted top pair + scan
-//   k_leaf_emit         (leafId << 32 | tri) keys
+//   k_count_units       exact leaf-cell counts per sorted top pair + scan
+//   k_emit_units        (leafId << 32 | tri) keys
 //   onesweep_sort + k_ranges on the leaf keys.
 //
 // The cell arithmetic restates src/Control/Algorithm/FastBuildKernels.h:31-313
@@ -22,6 +23,7 @@
 #include <cmath>
 
 #include "internal.h"
+#include "rows.cuh"
 
 namespace shn {
 
@@ -61,42 +63,29 @@ SHN_D void cell_range(V3 a, V3 b, V3 c, const Geom& g, uint32_t lo[3], uint32_t 
   hi[0] = (uint32_t)maxf.x; hi[1] = (uint32_t)maxf.y; hi[2] = (uint32_t)maxf.z;
 }
 
-// Cells of one triangle in emission order (z, y, x); plane-distance test when
-// the bbox spans >= 2 cells on every axis (FastBuildKernels.h:137-212).
-template <class F>
-SHN_D void for_each_cell(V3 a, V3 b, V3 c, const Geom& g, F&& emit) {
+// Pair-generation unit of a triangle against the top grid: candidate box
+// from countRefs (FastBuildKernels.h:47-69), plane test when the box spans
+// two or more cells on every axis (FastBuildKernels.h:137-212).
+SHN_D void top_unit(V3 a, V3 b, V3 c, const Geom& g, uint32_t id, uint32_t base, Unit& U) {
   uint32_t lo[3], hi[3];
   cell_range(a, b, c, g, lo, hi);
-  const uint32_t rx = (uint32_t)g.resf.x;
-  const uint32_t rxy = (uint32_t)(g.resf.x * g.resf.y);
-  if (hi[0] - lo[0] > 0 && hi[1] - lo[1] > 0 && hi[2] - lo[2] > 0) {
-    const V3 n = normalize(cross(sub(b, a), sub(c, a)));
-    const V3 half = muls(g.cs, 0.5f);
-    V3 c0 = mk((float)lo[0], (float)lo[1], (float)lo[2]);
-    c0 = mul(c0, g.cs);
-    c0 = add(add(c0, g.gmin), half);
-    float cz = c0.z - g.cs.z;
-    for (uint32_t z = lo[2]; z <= hi[2]; ++z) {
-      cz += g.cs.z;
-      float cy = c0.y - g.cs.y;
-      for (uint32_t y = lo[1]; y <= hi[1]; ++y) {
-        cy += g.cs.y;
-        float cx = c0.x - g.cs.x;
-        for (uint32_t x = lo[0]; x <= hi[0]; ++x) {
-          cx += g.cs.x;
-          const float d = dot(sub(mk(cx, cy, cz), a), n);
-          const V3 dist = muls(n, d);
-          if (fabsf(dist.x) <= half.x + kEps && fabsf(dist.y) <= half.y + kEps &&
-              fabsf(dist.z) <= half.z + kEps)
-            emit(x + y * rx + z * rxy);
-        }
-      }
-    }
-  } else {
-    for (uint32_t z = lo[2]; z <= hi[2]; ++z)
-      for (uint32_t y = lo[1]; y <= hi[1]; ++y)
-        for (uint32_t x = lo[0]; x <= hi[0]; ++x) emit(x + y * rx + z * rxy);
+  const bool plane = hi[0] - lo[0] > 0 && hi[1] - lo[1] > 0 && hi[2] - lo[2] > 0;
+  V3 n = mk(0.f, 0.f, 0.f);
+  if (plane) n = normalize(cross(sub(b, a), sub(c, a)));
+  U.a[0] = a.x; U.a[1] = a.y; U.a[2] = a.z;
+  U.n[0] = n.x; U.n[1] = n.y; U.n[2] = n.z;
+  U.s[0] = g.cs.x; U.s[1] = g.cs.y; U.s[2] = g.cs.z;
+  U.o[0] = g.gmin.x; U.o[1] = g.gmin.y; U.o[2] = g.gmin.z;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    U.lo[k] = lo[k];
+    U.span[k] = hi[k] - lo[k] + 1u;
   }
+  U.id = id;
+  U.base = base;
+  U.stride[0] = (uint32_t)g.resf.x;
+  U.stride[1] = (uint32_t)(g.resf.x * g.resf.y);
+  unit_finish(U, plane);
 }
 
 // Leaf resolution: largest r with r^3 <= cs_a^3 * lambda * refs / V, clamped
@@ -132,11 +121,12 @@ SHN_D uint32_t leaf_word(const Geom& g, float lambda, uint32_t refs, uint32_t th
   return y;
 }
 
-// Leaf cells of one (top cell, tri) pair in emission order
-// (TwoLevelBuildKernels.h:175-222, 327-451).
-template <class F>
-SHN_D void for_each_leaf(V3 a, V3 b, V3 c, const Geom& g, uint32_t topCell, uint32_t cellY,
-                         uint32_t leafBegin, F&& emit) {
+// Pair-generation unit of a (top cell, triangle) pair against the cell's leaf
+// grid (countLeafLevelRefs / writeLeafLevelRefs, TwoLevelBuildKernels.h:175-222,
+// 327-451): candidate box [lo, hp) clamped to the leaf resolution, plane test
+// when it spans two or more leaf cells on every axis.
+SHN_D void leaf_unit(V3 a, V3 b, V3 c, const Geom& g, uint32_t topCell, uint32_t cellY,
+                     uint32_t leafBegin, uint32_t id, Unit& U) {
   const uint32_t rX = (uint32_t)g.res[0], rY = (uint32_t)g.res[1];
   const uint32_t tx = topCell % rX;
   const uint32_t ty = (topCell % (rX * rY)) / rX;
@@ -156,36 +146,95 @@ SHN_D void for_each_leaf(V3 a, V3 b, V3 c, const Geom& g, uint32_t topCell, uint
   hp[0] = min((int)cres.x, (int)maxf.x);
   hp[1] = min((int)cres.y, (int)maxf.y);
   hp[2] = min((int)cres.z, (int)maxf.z);
-  const uint32_t crx = (uint32_t)cres.x;
-  const uint32_t crxy = (uint32_t)(cres.x * cres.y);
-  if (hp[0] - lo[0] > 1 && hp[1] - lo[1] > 1 && hp[2] - lo[2] > 1) {
-    const V3 n = normalize(cross(sub(b, a), sub(c, a)));
-    const V3 scs = divv(g.cs, cres);
-    V3 c0 = mk((float)lo[0], (float)lo[1], (float)lo[2]);
-    c0 = mul(c0, scs);
-    c0 = add(add(c0, origin), muls(scs, 0.5f));
-    float cz = c0.z - scs.z;
-    for (int z = lo[2]; z < hp[2]; ++z) {
-      cz += scs.z;
-      float cy = c0.y - scs.y;
-      for (int y = lo[1]; y < hp[1]; ++y) {
-        cy += scs.y;
-        float cx = c0.x - scs.x;
-        for (int x = lo[0]; x < hp[0]; ++x) {
-          cx += scs.x;
-          const float d = dot(sub(mk(cx, cy, cz), a), n);
-          const V3 dist = muls(n, d);
-          if (fabsf(dist.x) <= scs.x * 0.5f + kEps && fabsf(dist.y) <= scs.y * 0.5f + kEps &&
-              fabsf(dist.z) <= scs.z * 0.5f + kEps)
-            emit((uint32_t)x + (uint32_t)y * crx + (uint32_t)z * crxy + leafBegin);
-        }
-      }
-    }
-  } else {
-    for (int z = lo[2]; z < hp[2]; ++z)
-      for (int y = lo[1]; y < hp[1]; ++y)
-        for (int x = lo[0]; x < hp[0]; ++x)
-          emit((uint32_t)x + (uint32_t)y * crx + (uint32_t)z * crxy + leafBegin);
+  const bool plane = hp[0] - lo[0] > 1 && hp[1] - lo[1] > 1 && hp[2] - lo[2] > 1;
+  V3 n = mk(0.f, 0.f, 0.f);
+  if (plane) n = normalize(cross(sub(b, a), sub(c, a)));
+  const V3 scs = divv(g.cs, cres);
+  U.a[0] = a.x; U.a[1] = a.y; U.a[2] = a.z;
+  U.n[0] = n.x; U.n[1] = n.y; U.n[2] = n.z;
+  U.s[0] = scs.x; U.s[1] = scs.y; U.s[2] = scs.z;
+  U.o[0] = origin.x; U.o[1] = origin.y; U.o[2] = origin.z;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    U.lo[k] = (uint32_t)lo[k];
+    U.span[k] = hp[k] > lo[k] ? (uint32_t)(hp[k] - lo[k]) : 0u;
+  }
+  U.id = id;
+  U.base = leafBegin;
+  U.stride[0] = (uint32_t)cres.x;
+  U.stride[1] = (uint32_t)(cres.x * cres.y);
+  unit_finish(U, plane);
+}
+
+// ---- unit makers: item index -> unit ------------------------------------------------
+struct TopMaker {
+  TriSoA tri;
+  Geom g;
+  SHN_D bool operator()(uint32_t t, Unit& U) const {
+    V3 a, b, c;
+    load_tri(tri, t, a, b, c);
+    top_unit(a, b, c, g, t, 0u, U);
+    return true;
+  }
+};
+
+struct LeafMaker {
+  TriSoA tri;
+  const uint64_t* top;  // sorted (top cell << 32 | tri)
+  const uint2* cells;   // top cell words
+  Geom g;
+  SHN_D bool operator()(uint32_t i, Unit& U) const {
+    const uint64_t k = top[i];
+    const uint32_t c = (uint32_t)(k >> 32), t = (uint32_t)k;
+    V3 a, b, cc;
+    load_tri(tri, t, a, b, cc);
+    const uint2 w = cells[c];
+    leaf_unit(a, b, cc, g, c, w.y, w.x, t, U);
+    return true;
+  }
+};
+
+// ---- generic count (fused with the offsets scan) and emit kernels --------------------
+constexpr int kUnitWarps = kScanBlock / 32;
+
+// Exact pair count of every item, exclusive-scanned into offs[0..n], with
+// offs[n] = total.  Each warp produces 32 consecutive items at a time.
+template <class Maker>
+__global__ void __launch_bounds__(kScanBlock) k_count_units(Maker mk, uint32_t n, LookbackState st,
+                                                           uint32_t* offs) {
+  __shared__ TileScanSmem<kScanBlock, kScanItems> sm;
+  __shared__ Unit su[kUnitWarps][32];
+  __shared__ uint32_t acc[kUnitWarps][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t tile = tile_begin(st, sm);
+  const uint64_t base = (uint64_t)tile * kScanTile;
+  for (int k = 0; k < kScanItems; ++k) {
+    const int li = (warp * kScanItems + k) * 32 + lane;
+    const uint64_t i = base + li;
+    const bool valid = i < n && mk((uint32_t)i, su[warp][lane]);
+    __syncwarp();
+    sm.items[pad_idx(li)] = warp_count_units(su[warp], acc[warp], valid);
+    __syncwarp();
+  }
+  tile_finish(st, n, tile, sm, [&](uint32_t i, uint32_t ex) { offs[i] = ex; }, offs + n);
+}
+
+// Keys of every item at offs[item]: 32 items per warp step, coalesced stores.
+template <class Maker>
+__global__ void __launch_bounds__(kScanBlock) k_emit_units(Maker mk, uint32_t n,
+                                                          const uint32_t* __restrict__ offs,
+                                                          uint64_t* __restrict__ keys, uint32_t cap,
+                                                          uint32_t* err) {
+  __shared__ Unit su[kUnitWarps][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t groups = (n + 31u) / 32u;
+  for (uint32_t gi = blockIdx.x * kUnitWarps + warp; gi < groups; gi += gridDim.x * kUnitWarps) {
+    const uint32_t i = gi * 32u + lane;
+    const bool valid = i < n && mk(i, su[warp][lane]);
+    const uint32_t out = offs[gi * 32u];
+    __syncwarp();
+    warp_emit_units(su[warp], valid, out, keys, cap, err);
+    __syncwarp();
   }
 }
 
@@ -245,31 +294,6 @@ __global__ void k_bounds_decode(uint32_t* io6) {
   }
 }
 
-__global__ void __launch_bounds__(kScanBlock) k_count_scan_tris(TriSoA tri, uint32_t nt, Geom g,
-                                                               LookbackState st, uint32_t* offs) {
-  __shared__ TileScanSmem<kScanBlock, kScanItems> sm;
-  tile_scan<kScanBlock, kScanItems>(
-      st, nt, sm,
-      [&](uint32_t i) {
-        V3 a, b, c;
-        load_tri(tri, i, a, b, c);
-        uint32_t cnt = 0;
-        for_each_cell(a, b, c, g, [&](uint32_t) { ++cnt; });
-        return cnt;
-      },
-      [&](uint32_t i, uint32_t ex) { offs[i] = ex; }, offs + nt);
-}
-
-__global__ void k_emit_tris(TriSoA tri, uint32_t nt, Geom g, const uint32_t* __restrict__ offs,
-                            uint64_t* __restrict__ keys) {
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
-    V3 a, b, c;
-    load_tri(tri, t, a, b, c);
-    uint32_t o = offs[t];
-    for_each_cell(a, b, c, g, [&](uint32_t cell) { keys[o++] = ((uint64_t)cell << 32) | t; });
-  }
-}
-
 // Cell ranges from sorted keys (prepareCellRanges, FastBuildKernels.h:243-311)
 // plus indices[] and the reference-ordered triangle copy.
 __global__ void k_ranges(const uint64_t* __restrict__ keys, uint32_t n, uint2* __restrict__ ranges,
@@ -310,41 +334,6 @@ __global__ void __launch_bounds__(kScanBlock) k_leaf_cells_scan(const uint2* __r
         cells[c] = make_uint2(ex, y);
       },
       d_total);
-}
-
-__global__ void __launch_bounds__(kScanBlock) k_leaf_count_scan(TriSoA tri, const uint64_t* __restrict__ top,
-                                                               uint32_t P, Geom g,
-                                                               const uint2* __restrict__ cells,
-                                                               LookbackState st, uint32_t* offs) {
-  __shared__ TileScanSmem<kScanBlock, kScanItems> sm;
-  tile_scan<kScanBlock, kScanItems>(
-      st, P, sm,
-      [&](uint32_t i) {
-        const uint64_t k = top[i];
-        const uint32_t c = (uint32_t)(k >> 32), t = (uint32_t)k;
-        V3 a, b, cc;
-        load_tri(tri, t, a, b, cc);
-        const uint2 w = cells[c];
-        uint32_t cnt = 0;
-        for_each_leaf(a, b, cc, g, c, w.y, w.x, [&](uint32_t) { ++cnt; });
-        return cnt;
-      },
-      [&](uint32_t i, uint32_t ex) { offs[i] = ex; }, offs + P);
-}
-
-__global__ void k_leaf_emit(TriSoA tri, const uint64_t* __restrict__ top, uint32_t P, Geom g,
-                            const uint2* __restrict__ cells, const uint32_t* __restrict__ offs,
-                            uint64_t* __restrict__ keys) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
-    const uint64_t k = top[i];
-    const uint32_t c = (uint32_t)(k >> 32), t = (uint32_t)k;
-    V3 a, b, cc;
-    load_tri(tri, t, a, b, cc);
-    const uint2 w = cells[c];
-    uint32_t o = offs[i];
-    for_each_leaf(a, b, cc, g, c, w.y, w.x,
-                  [&](uint32_t leaf) { keys[o++] = ((uint64_t)leaf << 32) | t; });
-  }
 }
 
 // ---- batched multi-scene build ---------------------------------------------------
@@ -417,41 +406,19 @@ __global__ void k_batch_bounds_decode(uint32_t* io, uint32_t n) {
   if (i < n) io[i] = __float_as_uint(fval(io[i]));
 }
 
-__global__ void __launch_bounds__(kScanBlock) k_batch_count_scan(TriSoA tri, const uint32_t* __restrict__ tri_off,
-                                                                const BatchScene* __restrict__ scenes,
-                                                                uint32_t ns, uint32_t T, LookbackState st,
-                                                                uint32_t* offs) {
-  __shared__ TileScanSmem<kScanBlock, kScanItems> sm;
-  tile_scan<kScanBlock, kScanItems>(
-      st, T, sm,
-      [&](uint32_t i) {
-        const uint32_t s = find_segment(tri_off, ns, i);
-        V3 a, b, c;
-        load_tri(tri, i, a, b, c);
-        uint32_t cnt = 0;
-        for_each_cell(a, b, c, scenes[s].g, [&](uint32_t) { ++cnt; });
-        return cnt;
-      },
-      [&](uint32_t i, uint32_t ex) { offs[i] = ex; }, offs + T);
-}
-
-__global__ void k_batch_emit(TriSoA tri, const uint32_t* __restrict__ tri_off,
-                             const BatchScene* __restrict__ scenes, uint32_t ns, uint32_t T,
-                             const uint32_t* __restrict__ offs, uint64_t* __restrict__ keys,
-                             uint32_t capacity, uint32_t* err) {
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+struct BatchMaker {
+  TriSoA tri;
+  const uint32_t* tri_off;
+  const BatchScene* scenes;
+  uint32_t ns;
+  SHN_D bool operator()(uint32_t t, Unit& U) const {
     const uint32_t s = find_segment(tri_off, ns, t);
     V3 a, b, c;
     load_tri(tri, t, a, b, c);
-    uint32_t o = offs[t];
-    const uint64_t cb = scenes[s].cell_offset;
-    for_each_cell(a, b, c, scenes[s].g, [&](uint32_t cell) {
-      if (o < capacity) keys[o] = ((cb + cell) << 32) | t;
-      else atomicOr(err, kErrCapacity);
-      ++o;
-    });
+    top_unit(a, b, c, scenes[s].g, t, (uint32_t)scenes[s].cell_offset, U);
+    return true;
   }
-}
+};
 
 int grid_for(uint64_t n, int block, int max_blocks) {
   const uint64_t b = (n + block - 1) / block;
@@ -540,6 +507,9 @@ LookbackState scan_state(shn_grid* g, uint64_t n, cudaStream_t st, shn_status* r
   return LookbackState{status, ticket, g->d_err};
 }
 
+// Emit grid: groups of 32 items, kUnitWarps groups per block step.
+int emit_blocks(uint64_t n) { return grid_for((n + 31) / 32, kUnitWarps, 148 * 8); }
+
 uint32_t scan_tiles(uint64_t n) { return (uint32_t)std::max<uint64_t>(1, (n + kScanTile - 1) / kScanTile); }
 
 shn_status read_words(shn_grid* g, const uint32_t* d_src[], int k, uint32_t* out,
@@ -602,7 +572,7 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   if (nt) {
     LookbackState ls = scan_state(g, nt, st, &rc);
     if (rc) return rc;
-    k_count_scan_tris<<<scan_tiles(nt), kScanBlock, 0, st>>>(tri, nt, g->geom, ls, offs);
+    k_count_units<<<scan_tiles(nt), kScanBlock, 0, st>>>(TopMaker{tri, g->geom}, nt, ls, offs);
     const uint32_t* src[1] = {offs + nt};
     if ((rc = read_words(g, src, 1, &P, st))) return rc;
   }
@@ -614,7 +584,8 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   if ((rc = ensure_buf(g, g->sortws, sort_workspace_bytes(P), st))) return rc;
   uint64_t* k0 = (uint64_t*)g->keys[0].ptr;
   uint64_t* k1 = (uint64_t*)g->keys[1].ptr;
-  if (nt) k_emit_tris<<<grid_for(nt, 256, 148 * 16), 256, 0, st>>>(tri, nt, g->geom, offs, k0);
+  if (nt)
+    k_emit_units<<<emit_blocks(nt), kScanBlock, 0, st>>>(TopMaker{tri, g->geom}, nt, offs, k0, P, g->d_err);
   uint64_t* sortedTop =
       onesweep_sort(k0, k1, P, 32, sort_passes_for(C ? C - 1 : 0), g->sortws.ptr, g->d_err, st);
   const int topBuf = sortedTop == k0 ? 0 : 1;
@@ -652,8 +623,8 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   if (P) {
     LookbackState ls = scan_state(g, P, st, &rc);
     if (rc) return rc;
-    k_leaf_count_scan<<<scan_tiles(P), kScanBlock, 0, st>>>(tri, sortedTop, P, g->geom, g->cells, ls,
-                                                           pairOffs);
+    k_count_units<<<scan_tiles(P), kScanBlock, 0, st>>>(LeafMaker{tri, sortedTop, g->cells, g->geom}, P, ls,
+                                                       pairOffs);
   } else {
     cudaMemsetAsync(pairOffs, 0, 4, st);
   }
@@ -670,8 +641,9 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   if ((rc = ensure_buf(g, g->sortws, sort_workspace_bytes(R), st))) return rc;
   uint64_t* lk0 = (uint64_t*)g->keys[bA].ptr;
   uint64_t* lk1 = (uint64_t*)g->keys[bB].ptr;
-  if (P) k_leaf_emit<<<grid_for(P, 256, 148 * 16), 256, 0, st>>>(tri, sortedTop, P, g->geom, g->cells,
-                                                                 pairOffs, lk0);
+  if (P)
+    k_emit_units<<<emit_blocks(P), kScanBlock, 0, st>>>(LeafMaker{tri, sortedTop, g->cells, g->geom}, P,
+                                                       pairOffs, lk0, R, g->d_err);
   uint64_t* sortedLeaf = onesweep_sort(lk0, lk1, R, 32, sort_passes_for(Lc ? Lc - 1 : 0),
                                        g->sortws.ptr, g->d_err, st);
   if ((rc = ensure(g, (void**)&g->leaves, &g->cap_leaves, (size_t)std::max<uint32_t>(Lc, 1) * 8, st))) return rc;
@@ -716,14 +688,16 @@ void launch_batch_count(const float4* tri, uint32_t T, const uint32_t* tri_off, 
   cudaMemsetAsync(status, 0, (tiles + 2) * 8, st);
   LookbackState ls{status, (uint32_t*)(status + tiles + 1), err};
   const TriSoA ts{tri, tri + T, tri + 2 * (size_t)T};
-  k_batch_count_scan<<<(unsigned)tiles, kScanBlock, 0, st>>>(ts, tri_off, scenes, ns, T, ls, offs);
+  k_count_units<<<(unsigned)tiles, kScanBlock, 0, st>>>(BatchMaker{ts, tri_off, scenes, ns}, T, ls, offs);
 }
 
 void launch_batch_emit(const float4* tri, uint32_t T, const uint32_t* tri_off, const BatchScene* scenes,
                        uint32_t ns, const uint32_t* offs, uint64_t* keys, uint32_t capacity,
                        uint32_t* err, cudaStream_t st) {
   const TriSoA ts{tri, tri + T, tri + 2 * (size_t)T};
-  if (T) k_batch_emit<<<grid_for(T, 256, 148 * 16), 256, 0, st>>>(ts, tri_off, scenes, ns, T, offs, keys, capacity, err);
+  if (T)
+    k_emit_units<<<emit_blocks(T), kScanBlock, 0, st>>>(BatchMaker{ts, tri_off, scenes, ns}, T, offs, keys,
+                                                       capacity, err);
 }
 
 void launch_ranges(const uint64_t* keys, uint32_t n, uint2* ranges, uint32_t* indices,

@@ -130,18 +130,20 @@ struct TileScanSmem {
 
 SHN_D int pad_idx(int i) { return i + (i >> 5); }
 
-template <int BLOCK, int ITEMS, class Load, class Store>
-SHN_D void tile_scan(LookbackState st, uint32_t n, TileScanSmem<BLOCK, ITEMS>& sm, Load&& load,
-                     Store&& store, uint32_t* d_total) {
+// Split form for producers that fill the tile cooperatively: take the tile
+// with tile_begin, write item li (0 <= li < BLOCK*ITEMS) of the tile to
+// sm.items[pad_idx(li)] in any order, then call tile_finish, which scans,
+// looks back and hands every item's global exclusive prefix to store().
+template <int BLOCK, int ITEMS>
+SHN_D uint32_t tile_begin(LookbackState st, TileScanSmem<BLOCK, ITEMS>& sm) {
+  return take_tile(st, &sm.scan.tile_id);
+}
+
+template <int BLOCK, int ITEMS, class Store>
+SHN_D void tile_finish(LookbackState st, uint32_t n, uint32_t tile, TileScanSmem<BLOCK, ITEMS>& sm,
+                       Store&& store, uint32_t* d_total) {
   constexpr int TILE = BLOCK * ITEMS;
-  const uint32_t tile = take_tile(st, &sm.scan.tile_id);
   const uint64_t base = (uint64_t)tile * TILE;
-#pragma unroll
-  for (int k = 0; k < ITEMS; ++k) {
-    const int li = k * BLOCK + threadIdx.x;
-    const uint64_t i = base + li;
-    sm.items[pad_idx(li)] = (i < n) ? load((uint32_t)i) : 0u;
-  }
   __syncthreads();
   uint32_t v[ITEMS];
   uint32_t tsum = 0;
@@ -172,6 +174,21 @@ SHN_D void tile_scan(LookbackState st, uint32_t n, TileScanSmem<BLOCK, ITEMS>& s
     if (i < n) store((uint32_t)i, sm.items[pad_idx(li)]);
   }
   if (d_total && base + TILE >= n && threadIdx.x == 0) *d_total = tp + agg;
+}
+
+template <int BLOCK, int ITEMS, class Load, class Store>
+SHN_D void tile_scan(LookbackState st, uint32_t n, TileScanSmem<BLOCK, ITEMS>& sm, Load&& load,
+                     Store&& store, uint32_t* d_total) {
+  constexpr int TILE = BLOCK * ITEMS;
+  const uint32_t tile = tile_begin(st, sm);
+  const uint64_t base = (uint64_t)tile * TILE;
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    const int li = k * BLOCK + threadIdx.x;
+    const uint64_t i = base + li;
+    sm.items[pad_idx(li)] = (i < n) ? load((uint32_t)i) : 0u;
+  }
+  tile_finish(st, n, tile, sm, store, d_total);
 }
 
 }  // namespace shn
