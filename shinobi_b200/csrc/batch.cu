@@ -84,7 +84,7 @@ struct RaysV {
 };
 
 template <bool ANY>
-__global__ void __launch_bounds__(kBatchTraceBlock) k_batch_trace(GridView G, BatchAcc A, RaysV R,
+__global__ void __launch_bounds__(kBatchTraceBlock, 8) k_batch_trace(GridView G, BatchAcc A, RaysV R,
                                                                  const uint32_t* __restrict__ ray_off,
                                                                  uint32_t ns, uint32_t n, uint32_t* counter,
                                                                  uint32_t* otri, float* ot, float* ou,

@@ -295,20 +295,61 @@ __global__ void k_bounds_decode(uint32_t* io6) {
 }
 
 // Cell ranges from sorted keys (prepareCellRanges, FastBuildKernels.h:243-311)
-// plus indices[] and the reference-ordered triangle copy.
-__global__ void k_ranges(const uint64_t* __restrict__ keys, uint32_t n, uint2* __restrict__ ranges,
-                         uint32_t* __restrict__ indices, TriSoA tri, float4* __restrict__ rtri) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint64_t k = keys[i];
-    const uint32_t c = (uint32_t)(k >> 32);
-    const uint32_t t = (uint32_t)k;
-    if (i == 0 || (uint32_t)(keys[i - 1] >> 32) != c) ranges[c].x = i;
-    if (i + 1 == n || (uint32_t)(keys[i + 1] >> 32) != c) ranges[c].y = i + 1;
-    if (indices) indices[i] = t;
+// plus indices[] and the reference-ordered triangle copy.  Every thread
+// handles kRangeItems keys per step (block-strided, so each load and store
+// instruction is coalesced) to keep several gathers in flight; cell
+// boundaries are found with warp shuffles of the neighbouring keys.
+constexpr int kRangeItems = 1;
+constexpr int kRangeBlock = 256;
+
+__global__ void __launch_bounds__(kRangeBlock) k_ranges(const uint64_t* __restrict__ keys, uint32_t n,
+                                                        uint2* __restrict__ ranges,
+                                                        uint32_t* __restrict__ indices, TriSoA tri,
+                                                        float4* __restrict__ rtri) {
+  const int lane = threadIdx.x & 31;
+  constexpr uint32_t kStep = kRangeBlock * kRangeItems;
+  for (uint64_t b0 = (uint64_t)blockIdx.x * kStep; b0 < n; b0 += (uint64_t)gridDim.x * kStep) {
+    uint32_t c[kRangeItems], t[kRangeItems];
+#pragma unroll
+    for (int q = 0; q < kRangeItems; ++q) {
+      const uint64_t i = b0 + q * kRangeBlock + threadIdx.x;
+      const uint64_t k = i < n ? __ldcs(keys + i) : ~0ull;
+      c[q] = (uint32_t)(k >> 32);
+      t[q] = (uint32_t)k;
+    }
+    float4 a[kRangeItems], b[kRangeItems], d[kRangeItems];
     if (rtri) {
-      rtri[i] = __ldg(tri.v0 + t);
-      rtri[(size_t)n + i] = __ldg(tri.v1 + t);
-      rtri[2 * (size_t)n + i] = __ldg(tri.v2 + t);
+#pragma unroll
+      for (int q = 0; q < kRangeItems; ++q) {
+        const uint64_t i = b0 + q * kRangeBlock + threadIdx.x;
+        if (i < n) {
+          a[q] = __ldg(tri.v0 + t[q]);
+          b[q] = __ldg(tri.v1 + t[q]);
+          d[q] = __ldg(tri.v2 + t[q]);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kRangeItems; ++q) {
+      const uint64_t i = b0 + q * kRangeBlock + threadIdx.x;
+      uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, c[q], 1);
+      uint32_t next = __shfl_down_sync(0xFFFFFFFFu, c[q], 1);
+      if (i < n) {
+        if (lane == 0) prev = i > 0 ? (uint32_t)(keys[i - 1] >> 32) : ~c[q];
+        if (lane == 31) next = i + 1 < n ? (uint32_t)(keys[i + 1] >> 32) : ~c[q];
+        if (i + 1 == n) next = ~c[q];
+        if (i == 0) prev = ~c[q];
+        if (prev != c[q]) ranges[c[q]].x = (uint32_t)i;
+        if (next != c[q]) ranges[c[q]].y = (uint32_t)i + 1;
+        // streaming (evict-first) stores: the output must not push the
+        // triangles being gathered out of L2
+        if (indices) __stcs(indices + i, t[q]);
+        if (rtri) {
+          __stcs(rtri + i, a[q]);
+          __stcs(rtri + (size_t)n + i, b[q]);
+          __stcs(rtri + 2 * (size_t)n + i, d[q]);
+        }
+      }
     }
   }
 }
@@ -507,6 +548,8 @@ LookbackState scan_state(shn_grid* g, uint64_t n, cudaStream_t st, shn_status* r
   return LookbackState{status, ticket, g->d_err};
 }
 
+int range_blocks(uint64_t n) { return grid_for(n, kRangeBlock * kRangeItems, 148 * 8); }
+
 // Emit grid: groups of 32 items, kUnitWarps groups per block step.
 int emit_blocks(uint64_t n) { return grid_for((n + 31) / 32, kUnitWarps, 148 * 8); }
 
@@ -598,7 +641,7 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
     if ((rc = ensure(g, (void**)&g->indices, &g->cap_refs, (size_t)std::max<uint32_t>(P, 1) * 4, st))) return rc;
     if ((rc = ensure(g, (void**)&g->rtri, &g->cap_rtri, (size_t)std::max<uint32_t>(P, 1) * 48, st))) return rc;
     cudaMemsetAsync(g->cells, 0, C * 8, st);
-    if (P) k_ranges<<<grid_for(P, 256, 148 * 16), 256, 0, st>>>(sortedTop, P, g->cells, g->indices, tri, g->rtri);
+    if (P) k_ranges<<<range_blocks(P), kRangeBlock, 0, st>>>(sortedTop, P, g->cells, g->indices, tri, g->rtri);
     g->num_refs = P;
     g->num_leaves = 0;
     g->top_pairs = sortedTop;
@@ -609,7 +652,7 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   if ((rc = ensure_buf(g, g->top_ranges, C * 8, st))) return rc;
   uint2* topRanges = (uint2*)g->top_ranges.ptr;
   cudaMemsetAsync(topRanges, 0, C * 8, st);
-  if (P) k_ranges<<<grid_for(P, 256, 148 * 16), 256, 0, st>>>(sortedTop, P, topRanges, nullptr, tri, nullptr);
+  if (P) k_ranges<<<range_blocks(P), kRangeBlock, 0, st>>>(sortedTop, P, topRanges, nullptr, tri, nullptr);
   uint32_t* d_L = g->d_err + 1;
   {
     LookbackState ls = scan_state(g, C, st, &rc);
@@ -650,7 +693,7 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   if ((rc = ensure(g, (void**)&g->indices, &g->cap_refs, (size_t)std::max<uint32_t>(R, 1) * 4, st))) return rc;
   if ((rc = ensure(g, (void**)&g->rtri, &g->cap_rtri, (size_t)std::max<uint32_t>(R, 1) * 48, st))) return rc;
   cudaMemsetAsync(g->leaves, 0, (size_t)Lc * 8, st);
-  if (R) k_ranges<<<grid_for(R, 256, 148 * 16), 256, 0, st>>>(sortedLeaf, R, g->leaves, g->indices, tri, g->rtri);
+  if (R) k_ranges<<<range_blocks(R), kRangeBlock, 0, st>>>(sortedLeaf, R, g->leaves, g->indices, tri, g->rtri);
   g->num_leaves = Lc;
   g->num_refs = R;
   g->top_pairs = sortedTop;
@@ -703,7 +746,7 @@ void launch_batch_emit(const float4* tri, uint32_t T, const uint32_t* tri_off, c
 void launch_ranges(const uint64_t* keys, uint32_t n, uint2* ranges, uint32_t* indices,
                    const float4* tri, uint32_t T, float4* rtri, cudaStream_t st) {
   const TriSoA ts{tri, tri + T, tri + 2 * (size_t)T};
-  if (n) k_ranges<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(keys, n, ranges, indices, ts, rtri);
+  if (n) k_ranges<<<range_blocks(n), kRangeBlock, 0, st>>>(keys, n, ranges, indices, ts, rtri);
 }
 
 }  // namespace shn

@@ -258,7 +258,7 @@ SHN_D void warp_emit_units(Unit* su, bool valid, uint32_t out, uint64_t* __restr
       if (q < L) {
         const uint32_t o = out + q;
         const uint32_t cell = sc + (q - sp) * ss;
-        if (o < cap) keys[o] = ((uint64_t)cell << 32) | sid;
+        if (o < cap) __stcs(keys + o, ((uint64_t)cell << 32) | sid);
         else atomicOr(err, kErrCapacity);
       }
     }

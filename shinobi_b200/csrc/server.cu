@@ -45,7 +45,7 @@ struct ServeAcc {
 };
 
 // Rays are AoS records of 8 floats: ox, oy, oz, dx, dy, dz, tmax, unused.
-__global__ void __launch_bounds__(kServeBlock) k_serve_trace(const ServeSeg* __restrict__ segs, uint32_t nseg,
+__global__ void __launch_bounds__(kServeBlock, 8) k_serve_trace(const ServeSeg* __restrict__ segs, uint32_t nseg,
                                                             const float4* __restrict__ rays, uint32_t n,
                                                             uint32_t* counter, uint32_t* __restrict__ otri,
                                                             float* __restrict__ ot) {

@@ -25,6 +25,7 @@ constexpr int kSortWarps = kSortBlock / 32;
 constexpr uint32_t kDigFlagAgg = 1u << 30;
 constexpr uint32_t kDigFlagPrefix = 2u << 30;
 constexpr uint32_t kDigValueMask = (1u << 30) - 1u;
+constexpr int kLookback = 8;
 
 __global__ void __launch_bounds__(kSortBlock) k_sort_hist(const uint64_t* __restrict__ keys,
                                                           uint32_t n, uint32_t lo_bit,
@@ -61,7 +62,7 @@ __global__ void __launch_bounds__(256) k_sort_hist_scan(uint32_t* hist) {
 
 SHN_D uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__global__ void __launch_bounds__(kSortBlock) k_onesweep(const uint64_t* __restrict__ in,
+__global__ void __launch_bounds__(kSortBlock, 3) k_onesweep(const uint64_t* __restrict__ in,
                                                          uint64_t* __restrict__ out, uint32_t n,
                                                          uint32_t shift,
                                                          const uint32_t* __restrict__ digit_base,
@@ -142,7 +143,7 @@ __global__ void __launch_bounds__(kSortBlock) k_onesweep(const uint64_t* __restr
   }
   __syncthreads();
 
-  // ---- per digit: warp prefixes, tile count, look-back across tiles ---------
+  // ---- per digit: warp prefixes and tile count; publish the tile count ------
   const uint32_t dgt = threadIdx.x;  // 256 threads <-> 256 digits
   uint32_t tcount = 0;
 #pragma unroll
@@ -152,38 +153,15 @@ __global__ void __launch_bounds__(kSortBlock) k_onesweep(const uint64_t* __restr
     tcount += c;
   }
   uint32_t* my = status + (uint64_t)tile * 256 + dgt;
-  uint32_t excl = 0;
-  if (tile == 0) {
-    st_release(my, kDigFlagPrefix | tcount);
-  } else {
-    st_release(my, kDigFlagAgg | tcount);
-    int64_t j = (int64_t)tile - 1;
-    while (j >= 0) {
-      const uint32_t* p = status + (uint64_t)j * 256 + dgt;
-      uint32_t w = 0, spins = 0;
-      while (((w = ld_acquire(p)) >> 30) == 0u) {
-        if (++spins > kSpinLimit) {
-          atomicOr(err, kErrLookbackTimeout);
-          w = kDigFlagPrefix;
-          break;
-        }
-        __nanosleep(20);
-      }
-      excl += w & kDigValueMask;
-      if ((w >> 30) == 2u) break;
-      --j;
-    }
-    st_release(my, kDigFlagPrefix | (excl + tcount));
-  }
+  st_release(my, (tile == 0 ? kDigFlagPrefix : kDigFlagAgg) | tcount);
   uint32_t tot;
   const uint32_t bstart = block_excl_scan<kSortBlock>(tcount, s_scan, &tot);
-  s_gbase[dgt] = digit_base[dgt] + excl - bstart;  // global index = s_gbase[d] + local index
   // s_whist[w][d] becomes the tile-local start of warp w's digit-d keys
 #pragma unroll
   for (int w = 0; w < kSortWarps; ++w) s_whist[w][dgt] += bstart;
   __syncthreads();
 
-  // ---- reorder in shared memory, then coalesced write-out -----------------
+  // ---- reorder the tile in shared memory (digit order, stable) -------------
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
     const uint32_t idx = warp * (32 * kSortItems) + k * 32 + lane;
@@ -192,11 +170,51 @@ __global__ void __launch_bounds__(kSortBlock) k_onesweep(const uint64_t* __restr
       s_keys[s_whist[warp][d] + rank[k]] = key[k];
     }
   }
+
+  // ---- look-back across tiles for this digit ----------------------------------
+  uint32_t excl = 0;
+  if (tile != 0) {
+    // kLookback predecessors per round trip: the status word carries flag
+    // and value together, so relaxed loads suffice and all of a round's
+    // loads are in flight at once.
+    int64_t j = (int64_t)tile - 1;
+    bool done = false;
+    while (!done) {
+      uint32_t w[kLookback];
+#pragma unroll
+      for (int q = 0; q < kLookback; ++q)
+        w[q] = (j - q >= 0) ? ld_relaxed(status + (uint64_t)(j - q) * 256 + dgt) : kDigFlagPrefix;
+#pragma unroll
+      for (int q = 0; q < kLookback; ++q) {
+        if (done) break;
+        uint32_t v = w[q];
+        if ((v >> 30) == 0u) {  // not published yet: poll this one
+          const uint32_t* p = status + (uint64_t)(j - q) * 256 + dgt;
+          uint32_t spins = 0;
+          while (((v = ld_relaxed(p)) >> 30) == 0u) {
+            if (++spins > kSpinLimit) {
+              atomicOr(err, kErrLookbackTimeout);
+              v = kDigFlagPrefix;
+              break;
+            }
+            __nanosleep(20);
+          }
+        }
+        excl += v & kDigValueMask;
+        if ((v >> 30) == 2u) done = true;
+      }
+      j -= kLookback;
+    }
+    st_release(my, kDigFlagPrefix | (excl + tcount));
+  }
+  s_gbase[dgt] = digit_base[dgt] + excl - bstart;  // global index = s_gbase[d] + local index
   __syncthreads();
+
+  // ---- coalesced write-out ---------------------------------------------------
   for (uint32_t i = threadIdx.x; i < count; i += kSortBlock) {
     const uint64_t k = s_keys[i];
     const uint32_t d = (uint32_t)(k >> shift) & 255u;
-    out[s_gbase[d] + i] = k;
+    __stcs(out + s_gbase[d] + i, k);
   }
 }
 

@@ -42,7 +42,7 @@ SHN_D void add_counts(unsigned long long* stats, uint32_t steps, uint32_t tests)
 }
 
 template <int KIND, bool ANY, bool STATS>
-__global__ void __launch_bounds__(kTraceBlock) k_trace_rays(GridView G, RaysView R, uint32_t n,
+__global__ void __launch_bounds__(kTraceBlock, 8) k_trace_rays(GridView G, RaysView R, uint32_t n,
                                                             uint32_t* counter, uint32_t* otri,
                                                             float* ot, float* ou, float* ov,
                                                             uint8_t* occ, unsigned long long* stats,
@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_rays(GridView G, RaysView
 }
 
 template <int KIND, bool STATS>
-__global__ void __launch_bounds__(kTraceBlock) k_trace_camera(GridView G, CamView cam,
+__global__ void __launch_bounds__(kTraceBlock, 8) k_trace_camera(GridView G, CamView cam,
                                                               uint32_t image_id, uint32_t n,
                                                               uint32_t* counter, uint32_t* otri,
                                                               float* ot, float* ou, float* ov,
@@ -114,7 +114,7 @@ struct AoParams {
 };
 
 template <int KIND, bool STATS>
-__global__ void __launch_bounds__(kTraceBlock) k_trace_ao(GridView G, AoParams A,
+__global__ void __launch_bounds__(kTraceBlock, 8) k_trace_ao(GridView G, AoParams A,
                                                           const uint32_t* __restrict__ ptri,
                                                           const float* __restrict__ pt,
                                                           const uint32_t* __restrict__ hit_idx,

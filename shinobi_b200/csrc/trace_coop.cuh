@@ -260,8 +260,10 @@ SHN_D bool wt_test_p(V3 org, float Sx, float Sy, float Sz, float4 p0, float4 p1,
 // Whole warp tests references [b, e) against one (warp-uniform) ray.
 // Closest: returns the packed argmin key (t bits << 32 | ref) in every lane,
 // or ~0 when nothing beats tbest.  Any: returns a hit ref or ~0.
-// Loads of the next 32-reference chunk are issued before the current chunk
-// is tested (register double buffering) to cover the L2 latency.
+// L2 latency is covered by the other resident warps: the kernels that run
+// this engine are limited to 64 registers (8 blocks of 128 threads per SM),
+// which measured faster than staging the next chunk in registers or in
+// shared memory (cp.async) at lower occupancy.
 template <bool ANY, int KX, int KY, int KZ>
 SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz, float tbest,
                             uint32_t b, uint32_t e, uint32_t& tests) {
