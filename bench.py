@@ -47,9 +47,10 @@ def parse():
     ap.add_argument("--cpu-sample-stride", type=int, default=64)
     ap.add_argument("--case", default="full", choices=["full", "small"],
                     help="small: 480x270 camera, for profiler captures (not a bench line)")
-    ap.add_argument("--workload", default="cluster", choices=["cluster", "batch", "serve"],
+    ap.add_argument("--workload", default="cluster", choices=["cluster", "batch", "serve", "pathtrace"],
                     help="cluster: the headline line; batch: 256-scene batched vs one launch per scene; "
-                         "serve: request stream with continuous batching vs one launch per request")
+                         "serve: request stream with continuous batching vs one launch per request; "
+                         "pathtrace: heightfield path tracer with compaction after every bounce")
     ap.add_argument("--scenes", type=int, default=256, help="batch workload: number of scenes")
     ap.add_argument("--requests", type=int, default=20000, help="serve workload: requests per rate")
     ap.add_argument("--rates", default="1000,5000,20000,50000", help="serve workload: arrival rates (req/s)")
@@ -230,6 +231,23 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+def max_over_ranks(x: float, dist, device="cuda") -> float:
+    """Max of a per-rank scalar over all ranks (the identity on one rank).  The
+    replicas share no data; this is the only collective of the bench."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world: int, units_per_rank: float, max_ms: float) -> float:
+    """Whole-job throughput in millions of units/s: every rank processed
+    units_per_rank, the job took the slowest rank's time."""
+    return world * units_per_rank / (max_ms * 1e-3) / 1e6
+
+
 def run_shinobi(args):
     import torch
 
@@ -304,11 +322,8 @@ def run_shinobi(args):
     per = np.array([[a.elapsed_time(b), b.elapsed_time(c), c.elapsed_time(d)] for a, b, c, d in times])
     step_ms = per.sum(axis=1)
     total_ms = float(step_ms.sum())
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
-    value = world * args.steps * rays_per_step / (total_ms * 1e-3) / 1e6
+    total_ms = max_over_ranks(total_ms, dist)
+    value = replica_value(world, args.steps * rays_per_step, total_ms)
     build_ms = float(per[:, 0].mean())
     prim_ms = float(per[:, 1].mean())
     ao_ms = float(per[:, 2].mean())
@@ -340,11 +355,8 @@ def run_shinobi(args):
         e_e.record()
         torch.cuda.synchronize()
         e2e_total += e_s.elapsed_time(e_e)
-    t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_total = float(t.item())
-    e2e_value = world * args.steps * rays_per_step / (e2e_total * 1e-3) / 1e6
+    e2e_total = max_over_ranks(e2e_total, dist)
+    e2e_value = replica_value(world, args.steps * rays_per_step, e2e_total)
     h2d = int(sc.vertices.nbytes)
     d2h = int(npix * 12)
 
@@ -552,6 +564,88 @@ def run_batch(args):
     bt.close()
 
 
+def run_pathtrace(args):
+    """Plain path tracer on the heightfield scene: 2048x1024 quads (Perlin height, seed 2, amplitude
+    0.1) + 1000 boxes, uniform grid lambda=5, 1920x1080 x 16 spp, depth 4, roulette from depth 2,
+    albedo 0.7, one area light, compaction after every bounce.  A step is one full render."""
+    import torch
+
+    import shinobi_b200 as shn
+    from shinobi_b200 import scenes
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    sc = scenes.heightfield_boxes(2048, 1024, nboxes=1000)
+    soup = shn.FaceSoup(sc.vertices, sc.indices)
+    grid = shn.Grid()
+    p = shn.grid_params(shn.SHN_GRID_UNIFORM, lambda_=5.0)
+    for _ in range(2):
+        grid.build(soup, p)
+    build_ms = float(np.median([grid.build(soup, p).info().build_ms for _ in range(3)]))
+    cam = scenes.CAMERA_HEIGHTFIELD
+    small = args.case == "small"
+    if small:
+        cam = scenes.Camera(cam.eye, cam.forward, cam.up, cam.fov_deg, 480, 270)
+    spp = 4 if small else 16
+    params = shn.pt_params(spp=spp, max_depth=4, rr_depth=2, albedo=0.7, seed=2)
+    stats = torch.zeros(params.max_depth + 1, dtype=torch.int32, device="cuda")
+    img = torch.empty(cam.res_x * cam.res_y * 3, dtype=torch.float32, device="cuda")
+    for _ in range(max(1, args.warmup)):
+        grid.pt_render(soup, cam, params, out=img)
+    torch.cuda.synchronize()
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    ms = []
+    for _ in range(args.steps):
+        stats.zero_()
+        a, b = ev(), ev()
+        a.record()
+        grid.pt_render(soup, cam, params, out=img, stats=stats)
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    clk = clocks.stop()
+    st = stats.cpu().numpy().astype(np.int64)
+    ext, shadow = int(st[:params.max_depth].sum()), int(st[params.max_depth])
+    rays = ext + shadow
+    step_ms = float(np.mean(ms))
+    # end to end: the scene's vertices from pinned host memory, the render, the image back
+    vtx_h = torch.from_numpy(np.ascontiguousarray(sc.vertices)).pin_memory()
+    vtx_d = torch.empty_like(vtx_h, device="cuda")
+    img_h = torch.empty(img.numel(), dtype=torch.float32).pin_memory()
+    e2e = []
+    for _ in range(max(1, min(args.steps, 3))):
+        a, b = ev(), ev()
+        a.record()
+        vtx_d.copy_(vtx_h, non_blocking=True)
+        soup.update_vertices(vtx_d)
+        grid.build(soup, p)
+        grid.pt_render(soup, cam, params, out=img)
+        img_h.copy_(img, non_blocking=True)
+        b.record()
+        torch.cuda.synchronize()
+        e2e.append(a.elapsed_time(b))
+    e2e_ms = float(np.mean(e2e))
+    line = {
+        "metric": METRIC, "value": rays / (step_ms * 1e-3) / 1e6, "unit": METRIC, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Perlin heightfield + lognormal boxes, resident in HBM)",
+        "config": {"workload": f"path tracer: {sc.num_triangles} tris (2048x1024 heightfield quads + 1000 boxes), "
+                               f"uniform grid lambda=5, {cam.res_x}x{cam.res_y} x {spp} spp, depth 4, "
+                               "roulette from depth 2, albedo 0.7, one area light, compaction after every bounce",
+                   "rays_per_step": rays, "extension_rays": ext, "shadow_rays": shadow,
+                   "paths_per_bounce": st[:params.max_depth].tolist(),
+                   "l2": "inputs larger than L2 (paths: 64 B x 33M per bounce)"},
+        "build_ms_per_mtri": build_ms / (sc.num_triangles / 1e6),
+        "e2e": {"value": rays / (e2e_ms * 1e-3) / 1e6, "unit": METRIC,
+                "h2d_bytes_per_step": int(vtx_h.numel() * 4), "d2h_bytes_per_step": int(img_h.numel() * 4),
+                "what": "vertex upload from pinned host memory + rebuild + render + image read-back"},
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_serve(args):
     """Served ray-query stream: 64 resident scenes, Poisson arrivals, closest/any mix, 2% updates."""
     import torch
@@ -651,6 +745,8 @@ def main():
         run_batch(args)
     elif args.workload == "serve":
         run_serve(args)
+    elif args.workload == "pathtrace":
+        run_pathtrace(args)
     else:
         run_shinobi(args)
 

@@ -1,0 +1,398 @@
+// C++ adapters with the reference's class and method names, forwarding to
+// the C ABI in shinobi_b200.h (header only; link libshinobi_b200.so).
+//
+// The reference composes its ray tracer from compile-time policies
+// (src/Engine/RayTracingTypes.h:76-128, src/Shinobi.h:49-116): a primitive
+// storage (FaceSoup), a builder (FastSimpleGridBuilder /
+// FastTwoLevelGridBuilder), a traverser + intersector pair running inside a
+// persistent trace kernel, and an integrator (DirectIlluminationIntegrator,
+// SimplePathTracer) driven by StaticRTEngine.  The classes below keep those
+// names and the host-side method names and argument meanings, so an engine
+// written against the reference's host interface moves over by changing its
+// includes and its typedefs.  Differences that a caller sees:
+//  * errors throw shinobi::Error (the reference aborts through cutil's
+//    CUDA_SAFE_CALL);
+//  * there is no global texture or constant state: grids are objects, any
+//    number of them may live at once, and every call names its grid;
+//  * traversal and intersection are fused in the library's kernels (the
+//    watertight test replaces Moller-Trumbore), so UniformGridTraverser /
+//    TwoLevelGridTraverser are host objects that launch a trace over a ray
+//    buffer instead of device functors;
+//  * FWObject is a minimal host mesh with the reference's accessors
+//    (src/Loaders/FWObject.hpp:40-285), without the OBJ reader.
+#pragma once
+
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <ostream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../shinobi_b200.h"
+
+// Same declaration as the CUDA runtime's (driver_types.h), so this header
+// needs no CUDA include path; streams are passed through as void*.
+struct CUstream_st;
+typedef CUstream_st* cudaStream_t;
+
+namespace shinobi {
+
+class Error : public std::runtime_error {
+ public:
+  Error(shn_status s, const std::string& what)
+      : std::runtime_error(what + ": " + shn_status_string(s)), status(s) {}
+  shn_status status;
+};
+
+inline void check(shn_status s, const char* what, const shn_ctx* ctx = nullptr) {
+  if (s == SHN_OK) return;
+  std::string w(what);
+  if (ctx) {
+    const char* e = shn_ctx_last_error(ctx);
+    if (e && *e) w += std::string(" (") + e + ")";
+  }
+  throw Error(s, w);
+}
+
+struct vec3f {
+  float x, y, z;
+};
+
+struct BBox {
+  vec3f min, max;
+};
+
+// ---- host mesh (src/Loaders/FWObject.hpp:40-285) ------------------------------
+class FWObject {
+ public:
+  struct Face {
+    size_t vert1, vert2, vert3;
+  };
+  typedef const Face* t_FaceIterator;
+
+  void allocateVertices(size_t n) { mVertices.resize(n); }
+  void allocateFaces(size_t n) { mFaces.resize(n); }
+  size_t getNumVertices() const { return mVertices.size(); }
+  size_t getNumFaces() const { return mFaces.size(); }
+  vec3f getVertex(size_t i) const { return mVertices[i]; }
+  vec3f& getVertex(size_t i) { return mVertices[i]; }
+  Face getFace(size_t i) const { return mFaces[i]; }
+  Face& getFace(size_t i) { return mFaces[i]; }
+  t_FaceIterator facesBegin() const { return mFaces.data(); }
+  t_FaceIterator facesEnd() const { return mFaces.data() + mFaces.size(); }
+
+ private:
+  std::vector<vec3f> mVertices;
+  std::vector<Face> mFaces;
+};
+
+// ---- device context ------------------------------------------------------------
+// The reference uses the current CUDA device implicitly; the adapters share
+// one library context per process unless a Context is passed explicitly.
+class Context {
+ public:
+  explicit Context(int device = 0, uint64_t hbm_budget_bytes = 0) {
+    check(shn_ctx_create(device, hbm_budget_bytes, &mCtx), "shn_ctx_create");
+  }
+  ~Context() { shn_ctx_destroy(mCtx); }
+  Context(const Context&) = delete;
+  Context& operator=(const Context&) = delete;
+  shn_ctx* get() const { return mCtx; }
+
+  static Context& instance() {
+    static Context c;
+    return c;
+  }
+
+ private:
+  shn_ctx* mCtx = nullptr;
+};
+
+// ---- primitive storage (src/Control/Structure/FaceSoup.h:41-346) ------------------
+class FaceSoup {
+ public:
+  explicit FaceSoup(Context& ctx = Context::instance()) : mCtx(&ctx) {}
+  ~FaceSoup() { cleanup(); }
+  FaceSoup(const FaceSoup&) = delete;
+  FaceSoup& operator=(const FaceSoup&) = delete;
+
+  // FaceSoup::upload (FaceSoup.h:171-247): triangles [aBegin, aEnd) of aData.
+  void upload(FWObject::t_FaceIterator aBegin, FWObject::t_FaceIterator aEnd, const FWObject& aData,
+              cudaStream_t aStream = 0) {
+    cleanup();
+    flatten(aData, &mVtx);
+    mIdx.clear();
+    for (FWObject::t_FaceIterator it = aBegin; it != aEnd; ++it) {
+      mIdx.push_back((uint32_t)it->vert1);
+      mIdx.push_back((uint32_t)it->vert2);
+      mIdx.push_back((uint32_t)it->vert3);
+    }
+    check(shn_scene_create(mCtx->get(), mVtx.data(), (uint32_t)(mVtx.size() / 3), mIdx.data(),
+                           (uint32_t)(mIdx.size() / 3), SHN_MEM_HOST, aStream, &mScene),
+          "FaceSoup::upload", mCtx->get());
+  }
+
+  // FaceSoup::uploadVertices (FaceSoup.h:249-339): vertices interpolated
+  // between two key frames, new bounds returned.
+  void uploadVertices(const FWObject& aKeyFrame1, const FWObject& aKeyFrame2, float aCoeff,
+                      cudaStream_t aStream, vec3f& oMinBound, vec3f& oMaxBound) {
+    if (!mScene) throw Error(SHN_ERR_NOT_BUILT, "FaceSoup::uploadVertices before upload");
+    const size_t nv = aKeyFrame1.getNumVertices();
+    if (aKeyFrame2.getNumVertices() != nv || 3 * nv != mVtx.size())
+      throw Error(SHN_ERR_INVALID, "FaceSoup::uploadVertices: vertex counts differ");
+    for (size_t i = 0; i < nv; ++i) {
+      const vec3f a = aKeyFrame1.getVertex(i), b = aKeyFrame2.getVertex(i);
+      mVtx[3 * i + 0] = a.x + aCoeff * (b.x - a.x);
+      mVtx[3 * i + 1] = a.y + aCoeff * (b.y - a.y);
+      mVtx[3 * i + 2] = a.z + aCoeff * (b.z - a.z);
+    }
+    check(shn_scene_update_vertices(mScene, mVtx.data(), (uint32_t)nv, SHN_MEM_HOST, aStream),
+          "FaceSoup::uploadVertices", mCtx->get());
+    const BBox b = getBounds();
+    oMinBound = b.min;
+    oMaxBound = b.max;
+  }
+
+  void cleanup() {
+    if (mScene) shn_scene_destroy(mScene);
+    mScene = nullptr;
+  }
+
+  BBox getBounds() const {
+    float b[6];
+    check(shn_scene_bounds(mScene, b), "FaceSoup::getBounds");
+    return BBox{{b[0], b[1], b[2]}, {b[3], b[4], b[5]}};
+  }
+  uint32_t getNumPrimitives() const { return mScene ? shn_scene_num_triangles(mScene) : 0u; }
+  shn_scene* handle() const { return mScene; }
+  Context& context() const { return *mCtx; }
+
+ private:
+  static void flatten(const FWObject& o, std::vector<float>* out) {
+    out->resize(3 * o.getNumVertices());
+    for (size_t i = 0; i < o.getNumVertices(); ++i) {
+      const vec3f v = o.getVertex(i);
+      (*out)[3 * i] = v.x;
+      (*out)[3 * i + 1] = v.y;
+      (*out)[3 * i + 2] = v.z;
+    }
+  }
+  Context* mCtx;
+  shn_scene* mScene = nullptr;
+  std::vector<float> mVtx;
+  std::vector<uint32_t> mIdx;
+};
+
+// ---- grids (src/Control/Structure/SimpleGrid.h, TwoLevelGrid.h) ---------------------
+class GridBase {
+ public:
+  explicit GridBase(Context& ctx) : mCtx(&ctx) { check(shn_grid_create(ctx.get(), &mGrid), "shn_grid_create"); }
+  ~GridBase() { shn_grid_destroy(mGrid); }
+  GridBase(const GridBase&) = delete;
+  GridBase& operator=(const GridBase&) = delete;
+
+  shn_grid_info info() const {
+    shn_grid_info i;
+    check(shn_grid_get_info(mGrid, &i), "grid info");
+    return i;
+  }
+  vec3f getResolution() const {
+    const shn_grid_info i = info();
+    return vec3f{(float)i.res[0], (float)i.res[1], (float)i.res[2]};
+  }
+  BBox bounds() const {
+    const shn_grid_info i = info();
+    return BBox{{i.bounds[0], i.bounds[1], i.bounds[2]}, {i.bounds[3], i.bounds[4], i.bounds[5]}};
+  }
+  shn_grid* handle() const { return mGrid; }
+  Context& context() const { return *mCtx; }
+
+ protected:
+  Context* mCtx;
+  shn_grid* mGrid = nullptr;
+};
+
+class SimpleGrid : public GridBase {
+ public:
+  explicit SimpleGrid(Context& ctx = Context::instance()) : GridBase(ctx) {}
+};
+
+class TwoLevelGrid : public GridBase {
+ public:
+  explicit TwoLevelGrid(Context& ctx = Context::instance()) : GridBase(ctx) {}
+};
+
+// ---- builders (src/Control/Algorithm/FastSimpleGridBuilder.h:44-470,
+//                FastTwoLevelGridBuilder.h:46-760) -------------------------------------
+template <class Grid, uint32_t KIND>
+class GridBuilderT {
+ public:
+  GridBuilderT() { shn_grid_params_default(KIND, &mParams); }
+
+  void setNumPrimitives(uint32_t aNum) { mNumPrimitives = aNum; }
+  // Parameters the reference fixes at compile time.
+  shn_grid_params& params() { return mParams; }
+
+  // init: uploads the faces into the storage (and measures the bounds).
+  void init(Grid& oGrid, FaceSoup& oFaceSoup, FWObject::t_FaceIterator aBegin,
+            FWObject::t_FaceIterator aEnd, const FWObject& aData) {
+    (void)oGrid;
+    oFaceSoup.upload(aBegin, aEnd, aData);
+    mNumPrimitives = oFaceSoup.getNumPrimitives();
+  }
+
+  // build: the whole grid construction on the default stream.
+  void build(Grid& oGrid, FaceSoup& oFaceSoup) { rebuild(oGrid, oFaceSoup, nullptr); }
+
+  // rebuild: construction over the storage's current vertices on aStream
+  // (the reference's dynamic-scene path).
+  void rebuild(Grid& oGrid, FaceSoup& oFaceSoup, cudaStream_t aStream) {
+    check(shn_grid_build(oGrid.handle(), oFaceSoup.handle(), &mParams, aStream), "grid build",
+          oGrid.context().get());
+    mLast = oGrid.info();
+  }
+
+  void cleanup() {}
+
+  void outputStats(std::ostream& os) const {
+    os << "Grid resolution: " << mLast.res[0] << " " << mLast.res[1] << " " << mLast.res[2] << "\n"
+       << "Number of references: " << mLast.num_refs << "\n";
+    if (KIND == SHN_GRID_TWO_LEVEL) os << "Number of leaf cells: " << mLast.num_leaves << "\n";
+    os << "Build time (ms): " << mLast.build_ms << "\n";
+  }
+
+ private:
+  uint32_t mNumPrimitives = 0;
+  shn_grid_params mParams;
+  shn_grid_info mLast{};
+};
+
+typedef GridBuilderT<SimpleGrid, SHN_GRID_UNIFORM> FastSimpleGridBuilder;
+typedef GridBuilderT<TwoLevelGrid, SHN_GRID_TWO_LEVEL> FastTwoLevelGridBuilder;
+
+// ---- traversers (SimpleGridTraverser.h:249-469, TwoLevelGridTraverser.h:430-828) ------
+// The reference's traverser + SimpleIntersector pair, fused: closest hit for
+// the *Traverser classes, any hit for the *ShadowTraverser classes.  Rays and
+// results are device SoA buffers (shn_rays / shn_hits).
+struct ClosestTraverser {
+  void traverse(const GridBase& aGrid, const shn_rays& aRays, uint32_t aNumRays, shn_hits& oHits,
+                cudaStream_t aStream = 0) const {
+    check(shn_trace_closest(aGrid.handle(), &aRays, aNumRays, &oHits, aStream), "traverse",
+          aGrid.context().get());
+  }
+};
+struct ShadowTraverser {
+  void traverse(const GridBase& aGrid, const shn_rays& aRays, uint32_t aNumRays, uint8_t* oOccluded,
+                cudaStream_t aStream = 0) const {
+    check(shn_trace_any(aGrid.handle(), &aRays, aNumRays, oOccluded, aStream), "traverse (any hit)",
+          aGrid.context().get());
+  }
+};
+typedef ClosestTraverser UniformGridTraverser;
+typedef ClosestTraverser TwoLevelGridTraverser;
+typedef ShadowTraverser UniformGridShadowTraverser;
+typedef ShadowTraverser TwoLevelGridShadowTraverser;
+
+// ---- camera (src/Primitive/Camera.h:34-70) --------------------------------------------
+class Camera {
+ public:
+  void init(const vec3f& aCenter, const vec3f& aForward, const vec3f& aUp, float aVertOpeningAngInGrad,
+            uint32_t aResX, uint32_t aResY) {
+    const float c[9] = {aCenter.x, aCenter.y, aCenter.z, aForward.x, aForward.y, aForward.z, aUp.x, aUp.y, aUp.z};
+    memcpy(mCam.eye, c, sizeof(mCam.eye));
+    memcpy(mCam.forward, c + 3, sizeof(mCam.forward));
+    memcpy(mCam.up, c + 6, sizeof(mCam.up));
+    mCam.fov_deg = aVertOpeningAngInGrad;
+    mCam.res_x = aResX;
+    mCam.res_y = aResY;
+  }
+  const shn_camera& params() const { return mCam; }
+  uint32_t resX() const { return mCam.res_x; }
+  uint32_t resY() const { return mCam.res_y; }
+
+ private:
+  shn_camera mCam{};
+};
+
+// ---- integrators (src/Integrator/DirectIlluminationIntegrator.h:197-362,
+//                   src/Integrator/SimplePathTracer.hpp:65-241) ------------------------
+// Device buffers (cudaMalloc'd by the caller) for one frame.
+struct FrameBuffer {
+  float* deviceData = nullptr;  // resX*resY floats (ambient occlusion) or *3 (radiance)
+  uint32_t resX = 0, resY = 0;
+};
+
+// Primary closest-hit rays, then ambient-occlusion any-hit rays per hit
+// pixel (the C1 shape of the reference's default integrator).
+class DirectIlluminationIntegrator {
+ public:
+  uint32_t numOcclusionSamples = 4;
+  float occlusionLength = 0.1f;
+  float originOffset = 1e-4f;
+  uint32_t seed = 1;
+
+  // tracePrimary: hits (device, resX*resY) for the camera.
+  void tracePrimary(const GridBase& aGrid, const Camera& aCamera, shn_hits& oHits, int aImageId,
+                    cudaStream_t aStream = 0) {
+    check(shn_trace_primary(aGrid.handle(), &aCamera.params(), (uint32_t)aImageId, &oHits, aStream),
+          "tracePrimary", aGrid.context().get());
+  }
+  // shade: occlusion rays from the primary hits; oFrame = visible fraction.
+  void shade(const GridBase& aGrid, const Camera& aCamera, const shn_hits& aPrimary, FrameBuffer& oFrame,
+             cudaStream_t aStream = 0) {
+    check(shn_trace_ao(aGrid.handle(), &aCamera.params(), &aPrimary, numOcclusionSamples, occlusionLength,
+                       originOffset, seed, oFrame.deviceData, nullptr, aStream),
+          "shade", aGrid.context().get());
+  }
+  void integrate(const GridBase& aGrid, const Camera& aCamera, shn_hits& oHits, FrameBuffer& oFrame,
+                 int aImageId, cudaStream_t aStream = 0) {
+    tracePrimary(aGrid, aCamera, oHits, aImageId, aStream);
+    shade(aGrid, aCamera, oHits, oFrame, aStream);
+  }
+  void cleanup() {}
+};
+
+// Wavefront path tracer with compaction after every bounce.
+class SimplePathTracer {
+ public:
+  SimplePathTracer() { shn_pt_params_default(&mParams); }
+  shn_pt_params& params() { return mParams; }
+  void integrate(const GridBase& aGrid, const FaceSoup& aStorage, const Camera& aCamera, FrameBuffer& oFrame,
+                 cudaStream_t aStream = 0, uint32_t* oBounceStats = nullptr) {
+    check(shn_pt_render(aGrid.handle(), aStorage.handle(), &aCamera.params(), &mParams, oFrame.deviceData,
+                        oBounceStats, aStream),
+          "SimplePathTracer::integrate", aGrid.context().get());
+  }
+  void cleanup() {}
+
+ private:
+  shn_pt_params mParams;
+};
+
+// ---- engine (src/Engine/StaticRTEngine.h:34-237) ---------------------------------------
+template <class Builder, class Grid>
+class StaticRTEngine {
+ public:
+  void init(const FWObject& aScene, Context& ctx = Context::instance()) {
+    mStorage.reset(new FaceSoup(ctx));
+    mGrid.reset(new Grid(ctx));
+    mBuilder.init(*mGrid, *mStorage, aScene.facesBegin(), aScene.facesEnd(), aScene);
+  }
+  void build() { mBuilder.build(*mGrid, *mStorage); }
+  void renderImage(DirectIlluminationIntegrator& aIntegrator, const Camera& aCamera, shn_hits& oHits,
+                   FrameBuffer& oFrame, int aImageId, cudaStream_t aStream = 0) {
+    aIntegrator.integrate(*mGrid, aCamera, oHits, oFrame, aImageId, aStream);
+  }
+  Builder& builder() { return mBuilder; }
+  Grid& grid() { return *mGrid; }
+  FaceSoup& storage() { return *mStorage; }
+
+ private:
+  Builder mBuilder;
+  std::unique_ptr<FaceSoup> mStorage;
+  std::unique_ptr<Grid> mGrid;
+};
+
+}  // namespace shinobi

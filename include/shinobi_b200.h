@@ -74,6 +74,9 @@ typedef struct shn_grid shn_grid;
  * scenes, grids and build workspaces comes from a stream-ordered pool that
  * the context owns. */
 shn_status shn_ctx_create(int device, uint64_t hbm_budget_bytes, shn_ctx** out);
+/* Releases the caller's handle.  Scenes, grids, batches and servers created
+ * on the context keep it alive: its memory pool is destroyed when the last
+ * of them is destroyed, in any order. */
 void shn_ctx_destroy(shn_ctx* ctx);
 const char* shn_status_string(shn_status s);
 const char* shn_ctx_last_error(const shn_ctx* ctx);
@@ -313,7 +316,9 @@ typedef struct shn_pt_params {
 void shn_pt_params_default(shn_pt_params* p);
 /* Wavefront path tracer: camera rays -> extend -> shade/next-event -> compact
  * after each bounce.  d_image: res_x*res_y*3 floats (mean radiance).  If
- * d_stats != NULL it receives per-bounce live-path counts (max_depth+1 uint32). */
+ * d_stats != NULL (max_depth+1 uint32, device) it receives the number of paths
+ * traced at each bounce d < max_depth, summed over all wavefront chunks, and
+ * in d_stats[max_depth] the number of next-event shadow rays traced. */
 shn_status shn_pt_render(const shn_grid* g, const shn_scene* s, const shn_camera* cam,
                          const shn_pt_params* p, float* d_image, uint32_t* d_stats, void* stream);
 
@@ -336,6 +341,12 @@ shn_status shn_exclusive_scan_u32(shn_ctx* ctx, const uint32_t* d_in, uint32_t* 
 #define SHN_SCAN_NOALLOC_MAX_N (1u << 24)
 shn_status shn_exclusive_scan_u32_noalloc(const uint32_t* d_in, uint32_t* d_out, uint32_t n,
                                           void* stream);
+/* Failure-detection self test: runs the look-back scan kernel with tile 0
+ * never published, so tile 1's bounded wait must run out (about a second)
+ * and report it.  Returns SHN_ERR_TIMEOUT when the wait ran out and the
+ * context is still usable (the expected result).  No counterpart in the
+ * reference. */
+shn_status shn_selftest_lookback_timeout(shn_ctx* ctx, void* stream);
 /* Stable compaction: d_out_idx[0..m) = indices i with d_flags[i] != 0, in
  * order; *d_count = m (device). */
 shn_status shn_compact_u32(shn_ctx* ctx, const uint32_t* d_flags, uint32_t n, uint32_t* d_out_idx,

@@ -17,6 +17,9 @@ STATUS = {
     5: "SHN_ERR_BUDGET", 6: "SHN_ERR_NOT_BUILT", 7: "SHN_ERR_BUSY", 8: "SHN_ERR_CANCELLED",
 }
 
+SHN_OK, SHN_ERR_INVALID, SHN_ERR_CUDA, SHN_ERR_OOM, SHN_ERR_TIMEOUT = 0, 1, 2, 3, 4
+SHN_ERR_BUDGET, SHN_ERR_NOT_BUILT, SHN_ERR_BUSY, SHN_ERR_CANCELLED = 5, 6, 7, 8
+
 SHN_MISS = 0xFFFFFFFF
 SHN_MEM_HOST = 0
 SHN_MEM_DEVICE = 1
@@ -124,6 +127,7 @@ SIGNATURES = {
     "shn_exclusive_scan_u32": ([vp, vp, vp, u32, vp], i32),
     "shn_exclusive_scan_u32_noalloc": ([vp, vp, u32, vp], i32),
     "shn_compact_u32": ([vp, vp, u32, vp, vp, vp], i32),
+    "shn_selftest_lookback_timeout": ([vp, vp], i32),
     "shn_sort_keys_u64": ([vp, vp, vp, u32, u32, u32, vp], i32),
 }
 

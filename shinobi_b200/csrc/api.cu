@@ -91,6 +91,19 @@ shn_status refresh_bounds(shn_scene* s, cudaStream_t st) {
 
 }  // namespace
 
+namespace shn {
+void ctx_retain(shn_ctx* c) { c->refs.fetch_add(1); }
+
+void ctx_release(shn_ctx* c) {
+  if (!c || c->refs.fetch_sub(1) != 1) return;
+  cudaSetDevice(c->device);
+  cudaDeviceSynchronize();
+  if (c->d_err) cudaFree(c->d_err);
+  if (c->pool) cudaMemPoolDestroy(c->pool);
+  delete c;
+}
+}  // namespace shn
+
 extern "C" {
 
 uint32_t shn_abi_version(void) { return SHN_ABI_VERSION; }
@@ -140,13 +153,7 @@ shn_status shn_ctx_create(int device, uint64_t hbm_budget_bytes, shn_ctx** out) 
   return SHN_OK;
 }
 
-void shn_ctx_destroy(shn_ctx* c) {
-  if (!c) return;
-  cudaDeviceSynchronize();
-  if (c->d_err) cudaFree(c->d_err);
-  if (c->pool) cudaMemPoolDestroy(c->pool);
-  delete c;
-}
+void shn_ctx_destroy(shn_ctx* c) { ctx_release(c); }
 
 const char* shn_ctx_last_error(const shn_ctx* c) { return c ? c->last_error.c_str() : ""; }
 
@@ -170,6 +177,7 @@ shn_status shn_scene_create(shn_ctx* ctx, const float* vtx, uint32_t nv, const u
   cudaStream_t st = (cudaStream_t)stream;
   shn_scene* s = new shn_scene();
   s->ctx = ctx;
+  ctx_retain(ctx);
   s->nv = nv;
   s->nt = nt;
   const size_t bv = std::max<size_t>(12 * (size_t)nv, 16), bi = std::max<size_t>(12 * (size_t)nt, 16),
@@ -225,7 +233,9 @@ void shn_scene_destroy(shn_scene* s) {
   dev_free(s->ctx, s->vtx, std::max<size_t>(12 * (size_t)s->nv, 16), st);
   dev_free(s->ctx, s->idx, std::max<size_t>(12 * (size_t)s->nt, 16), st);
   dev_free(s->ctx, s->tri, std::max<size_t>(48 * (size_t)s->nt, 16), st);
+  shn_ctx* c = s->ctx;
   delete s;
+  ctx_release(c);
 }
 
 // ---- grid --------------------------------------------------------------------------
@@ -249,6 +259,7 @@ shn_status shn_grid_create(shn_ctx* ctx, shn_grid** out) {
   if (!ctx || !out) return SHN_ERR_INVALID;
   shn_grid* g = new shn_grid();
   g->ctx = ctx;
+  ctx_retain(ctx);
   *out = g;
   return SHN_OK;
 }
@@ -315,6 +326,7 @@ void shn_grid_destroy(shn_grid* g) {
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
   delete g;
+  ctx_release(c);
 }
 
 // ---- primitives -------------------------------------------------------------------------

@@ -311,6 +311,7 @@ shn_status shn_batch_create(shn_ctx* ctx, uint32_t num_scenes, const float* vtx_
   cudaStream_t st = (cudaStream_t)stream;
   shn_batch* b = new shn_batch();
   b->ctx = ctx;
+  ctx_retain(ctx);
   b->ns = num_scenes;
   b->T = T;
   b->tri_off.assign(tri_offsets, tri_offsets + num_scenes + 1);
@@ -582,7 +583,9 @@ void shn_batch_destroy(shn_batch* b) {
   if (b->d_vtx_off) cudaFree(b->d_vtx_off);
   if (b->d_err) cudaFree(b->d_err);
   if (b->h_pinned) cudaFreeHost(b->h_pinned);
+  shn_ctx* c = b->ctx;
   delete b;
+  ctx_release(c);
 }
 
 }  // extern "C"

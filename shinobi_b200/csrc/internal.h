@@ -33,8 +33,10 @@ struct shn_ctx {
   std::mutex mu;
   std::string last_error;
   uint32_t* d_err = nullptr;    // device error word of context-level primitives
-  void* scratch = nullptr;      // small reusable workspace for primitives
-  size_t scratch_bytes = 0;
+  // One reference for the handle returned by shn_ctx_create and one per live
+  // scene / grid / batch / server: the context (and its memory pool) is torn
+  // down when the last of them is released, whatever the destruction order.
+  std::atomic<int> refs{1};
 };
 
 struct shn_scene {
@@ -79,6 +81,8 @@ namespace shn {
 // api.cu
 cudaError_t dev_alloc(shn_ctx* ctx, void** p, size_t bytes, cudaStream_t st);
 void dev_free(shn_ctx* ctx, void* p, size_t bytes, cudaStream_t st);
+void ctx_retain(shn_ctx* ctx);
+void ctx_release(shn_ctx* ctx);
 shn_status set_error(shn_ctx* ctx, shn_status s, const std::string& msg);
 shn_status cuda_status(shn_ctx* ctx, cudaError_t e, const char* where);
 

@@ -73,9 +73,11 @@ template <int KIND>
 __global__ void __launch_bounds__(kPtBlock) k_pt_bounce(GridView G, PtView P, PathRec* __restrict__ paths,
                                                         const uint32_t* d_n, uint32_t depth,
                                                         uint32_t* counter, uint32_t* __restrict__ alive,
-                                                        float4* __restrict__ slots, uint64_t g0) {
+                                                        float4* __restrict__ slots, uint64_t g0,
+                                                        uint32_t* d_shadow) {
   const uint32_t n = *d_n;
   const int lane = threadIdx.x & 31;
+  uint32_t shadow_rays = 0;
   while (true) {
     uint32_t b = 0;
     if (lane == 0) b = atomicAdd(counter, 32u);
@@ -115,6 +117,7 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_bounce(GridView G, PtView P, Pa
       if (cs > 0.f && cl > 0.f) {
         Hit sh{0.9999f, kMiss, 0.f, 0.f};
         trace_ray<KIND, true>(G, o, wv, sh);
+        ++shadow_rays;
         if (sh.tri == kMiss) {
           const float f = ((((P.albedo * 0.31830988618379067f) * cs) * cl) * P.larea) / d2;
           L = add(L, muls(mul(beta, P.lrad), f));
@@ -147,6 +150,10 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_bounce(GridView G, PtView P, Pa
     }
     alive[i] = live ? 1u : 0u;
     if (!live) slots[(uint64_t)s * P.npix + p - g0] = make_float4(L.x, L.y, L.z, 0.f);
+  }
+  if (d_shadow) {  // every lane leaves the loop at the same iteration
+    const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, shadow_rays);
+    if (lane == 0 && c) atomicAdd(d_shadow, c);
   }
 }
 
@@ -186,6 +193,7 @@ __global__ void k_pt_resolve(const float4* __restrict__ slots, uint32_t npix, ui
 }
 
 __global__ void k_copy_u32(const uint32_t* src, uint32_t* dst) { *dst = *src; }
+__global__ void k_add_u32(const uint32_t* src, uint32_t* dst) { *dst += *src; }
 
 }  // namespace
 
@@ -297,12 +305,15 @@ shn_status shn_pt_render(const shn_grid* g, const shn_scene* s, const shn_camera
     k_pt_camera<<<(count + 255) / 256, 256, 0, st>>>(P, g0, count, cur, d_n);
     for (uint32_t d = 0; d < prm->max_depth; ++d) {
       cudaMemsetAsync(counters, 0, 4, st);
-      if (d_stats && g0 == 0) k_copy_u32<<<1, 1, 0, st>>>(d_n, d_stats + d);
+      if (d_stats) k_add_u32<<<1, 1, 0, st>>>(d_n, d_stats + d);
+      uint32_t* d_shadow = d_stats ? d_stats + prm->max_depth : nullptr;
       float4* slot_base = (float4*)slots;
       if (g->kind == SHN_GRID_UNIFORM)
-        k_pt_bounce<0><<<blocks, kPtBlock, 0, st>>>(G, P, cur, d_n, d, counters, (uint32_t*)alive, slot_base, 0);
+        k_pt_bounce<0><<<blocks, kPtBlock, 0, st>>>(G, P, cur, d_n, d, counters, (uint32_t*)alive, slot_base, 0,
+                                                    d_shadow);
       else
-        k_pt_bounce<1><<<blocks, kPtBlock, 0, st>>>(G, P, cur, d_n, d, counters, (uint32_t*)alive, slot_base, 0);
+        k_pt_bounce<1><<<blocks, kPtBlock, 0, st>>>(G, P, cur, d_n, d, counters, (uint32_t*)alive, slot_base, 0,
+                                                    d_shadow);
       if (d + 1 < prm->max_depth) {
         cudaMemsetAsync(status, 0, bSt, st);
         LookbackState ls{(uint64_t*)status, (uint32_t*)((uint64_t*)status + tiles + 1), g->d_err};
@@ -312,7 +323,6 @@ shn_status shn_pt_render(const shn_grid* g, const shn_scene* s, const shn_camera
         std::swap(cur, nxt);
       }
     }
-    if (d_stats && g0 == 0) k_copy_u32<<<1, 1, 0, st>>>(d_n, d_stats + prm->max_depth);
   }
   k_pt_resolve<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>((const float4*)slots, (uint32_t)npix,
                                                                prm->spp, d_image);

@@ -67,3 +67,46 @@ void launch_compact(const uint32_t* flags, uint32_t n, uint32_t* out_idx, uint32
 }
 
 }  // namespace shn
+
+using namespace shn;
+
+extern "C" {
+
+// Failure-detection self test: a single block scans tile 1 of a two-tile
+// input while tile 0 is never published, so the block's look-back must give
+// up after its bounded wait and flag kErrLookbackTimeout.
+shn_status shn_selftest_lookback_timeout(shn_ctx* ctx, void* stream) {
+  if (!ctx) return SHN_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  const uint32_t n = 2 * kTile;
+  uint32_t *in = nullptr, *out = nullptr, *err = nullptr;
+  void* ws = nullptr;
+  cudaError_t e = dev_alloc(ctx, (void**)&in, n * 4, st);
+  if (e == cudaSuccess) e = dev_alloc(ctx, (void**)&out, (n + 1) * 4, st);
+  if (e == cudaSuccess) e = dev_alloc(ctx, (void**)&err, 4, st);
+  if (e == cudaSuccess) e = dev_alloc(ctx, &ws, scan_workspace_bytes(n), st);
+  shn_status rc = SHN_OK;
+  if (e != cudaSuccess) {
+    rc = cuda_status(ctx, e, "selftest alloc");
+  } else {
+    cudaMemsetAsync(in, 0, n * 4, st);
+    cudaMemsetAsync(err, 0, 4, st);
+    LookbackState ls = prep(ws, n, err, st);
+    const uint32_t one = 1u;  // the only block takes ticket 1: tile 0 never runs
+    cudaMemcpyAsync(ls.ticket, &one, 4, cudaMemcpyHostToDevice, st);
+    k_exclusive_scan<<<1, kBlock, 0, st>>>(in, out, n, ls);
+    uint32_t h = 0;
+    cudaMemcpyAsync(&h, err, 4, cudaMemcpyDeviceToHost, st);
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = cuda_status(ctx, e, "selftest");
+    else if (h & kErrLookbackTimeout) rc = set_error(ctx, SHN_ERR_TIMEOUT, "look-back wait gave up (expected)");
+  }
+  if (in) dev_free(ctx, in, n * 4, st);
+  if (out) dev_free(ctx, out, (n + 1) * 4, st);
+  if (err) dev_free(ctx, err, 4, st);
+  if (ws) dev_free(ctx, ws, scan_workspace_bytes(n), st);
+  cudaStreamSynchronize(st);
+  return rc;
+}
+
+}  // extern "C"

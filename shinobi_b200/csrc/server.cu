@@ -304,6 +304,7 @@ shn_status shn_server_create(shn_ctx* ctx, const shn_server_config* cfg, shn_ser
   *out = nullptr;
   shn_server* s = new shn_server();
   s->ctx = ctx;
+  ctx_retain(ctx);
   s->cfg = *cfg;
   s->slots.resize(cfg->num_slots);
   cudaStreamCreateWithFlags(&s->update_st, cudaStreamNonBlocking);
@@ -489,7 +490,9 @@ void shn_server_destroy(shn_server* s) {
     }
   }
   if (s->update_st) cudaStreamDestroy(s->update_st);
+  shn_ctx* c = s->ctx;
   delete s;
+  ctx_release(c);
 }
 
 }  // extern "C"

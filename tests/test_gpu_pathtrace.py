@@ -45,6 +45,7 @@ def test_pt_matches_oracle(gpu, kind):
     live = stats.cpu().numpy()
     assert live[0] == 96 * 54 * 8
     assert np.all(np.diff(live[:4]) <= 0) and live[3] > 0   # compaction shrinks the wavefront
+    assert 0 < live[4] <= live[:4].sum()                     # next-event shadow rays
 
 
 def test_pt_large_wave_chunks(gpu):
