@@ -706,17 +706,28 @@ def run_serve(args):
             r.out_tri = C_void_p(out_tri.data_ptr() + 4 * a)
             r.out_t = C_void_p(out_t.data_ptr() + 4 * a)
             reqs.append(r)
+        # warm-up: a short schedule with updates (first launches of every kernel, pool growth)
+        wn = min(400, n_req)
+        srv.run_schedule(reqs[:wn], np.arange(wn, dtype=np.float64) * 1e-4)
+        srv.drain()
         per_rate = {}
         for rate in [float(x) for x in args.rates.split(",")]:
             gaps = rng.exponential(1.0 / rate, n_req)
             arr = np.cumsum(gaps) - gaps[0]
             srv.stats(reset=True)
             res = srv.run_schedule(reqs, arr)
+            rec = srv.records()
             st = srv.stats(reset=True)
+            q_lat = rec["latency_us"][rec["kind"] != shn._abi.SHN_REQ_UPDATE] / 1e3
+            u_lat = rec["latency_us"][rec["kind"] == shn._abi.SHN_REQ_UPDATE] / 1e3
             per_rate[str(int(rate))] = {"p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3,
                                         "mrays_per_s": st["mrays_per_s"], "launches": st["launches"],
                                         "requests": st["requests"], "failed": int((res != 0).sum()),
-                                        "wall_s": st["wall_s"], "offered_mrays_per_s": float(counts[~is_upd].sum()) / arr[-1] / 1e6}
+                                        "wall_s": st["wall_s"], "offered_mrays_per_s": float(counts[~is_upd].sum()) / arr[-1] / 1e6,
+                                        "query_p50_ms": float(np.percentile(q_lat, 50)) if q_lat.size else None,
+                                        "query_p99_ms": float(np.percentile(q_lat, 99)) if q_lat.size else None,
+                                        "update_p50_ms": float(np.percentile(u_lat, 50)) if u_lat.size else None,
+                                        "update_p99_ms": float(np.percentile(u_lat, 99)) if u_lat.size else None}
         results["coalesced" if coalesce else "plain"] = per_rate
         srv.close()
         ctx.close()

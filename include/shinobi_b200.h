@@ -146,6 +146,8 @@ shn_status shn_grid_get_info(const shn_grid* g, shn_grid_info* out);
  * num_refs (uniform).  Synchronises. */
 shn_status shn_grid_export(const shn_grid* g, uint32_t* cells, uint32_t* leaves, uint32_t* indices,
                            uint64_t* top_pairs);
+/* Frees the grid's device memory (stream-ordered, pool); every launch that
+ * reads the grid must have completed. */
 void shn_grid_destroy(shn_grid* g);
 
 /* ---- traversal -------------------------------------------------------------- */
@@ -292,6 +294,17 @@ shn_status shn_server_wait(shn_server* s, uint64_t ticket, uint32_t timeout_ms, 
 shn_status shn_server_poll(shn_server* s, uint64_t ticket, shn_status* result);
 shn_status shn_server_drain(shn_server* s, uint32_t timeout_ms);
 shn_status shn_server_get_stats(shn_server* s, shn_server_stats* out, int reset);
+/* Per-request records since the last stats reset, in completion order:
+ * submit time (steady clock, seconds), latency, kind, scene, rays, status.
+ * Copies min(max_records, *count) of them; *count = how many exist. */
+typedef struct shn_request_record {
+  double submit_s;
+  double latency_us;
+  uint32_t kind, scene, num_rays;
+  int32_t status;
+} shn_request_record;
+shn_status shn_server_get_records(shn_server* s, uint32_t max_records, shn_request_record* out,
+                                  uint32_t* count);
 /* Load generator: submits reqs[i] at arrival_s[i] seconds after the call
  * (from the calling thread), then waits for all; results (optional) per request. */
 shn_status shn_server_run_schedule(shn_server* s, uint32_t n, const shn_request* reqs,

@@ -484,6 +484,17 @@ class Server:
         self.ctx.check(self.ctx.lib.shn_server_get_stats(self.handle, C.byref(st), int(reset)), "shn_server_get_stats")
         return {k: getattr(st, k) for k, _ in _abi.ServerStats._fields_}
 
+    def records(self):
+        """Per-request records since the last stats reset (completion order) as a numpy
+        structured array: submit_s, latency_us, kind, scene, num_rays, status."""
+        n = C.c_uint32()
+        self.ctx.check(self.ctx.lib.shn_server_get_records(self.handle, 0, None, C.byref(n)), "records")
+        buf = (_abi.RequestRecord * max(1, n.value))()
+        self.ctx.check(self.ctx.lib.shn_server_get_records(self.handle, n.value, buf, C.byref(n)), "records")
+        dt = np.dtype([("submit_s", "f8"), ("latency_us", "f8"), ("kind", "u4"), ("scene", "u4"),
+                       ("num_rays", "u4"), ("status", "i4")])
+        return np.frombuffer(bytes(buf), dtype=dt, count=n.value).copy()
+
     def drain(self, timeout_ms=600000):
         self.ctx.check(self.ctx.lib.shn_server_drain(self.handle, timeout_ms), "shn_server_drain")
 

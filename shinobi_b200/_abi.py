@@ -74,6 +74,11 @@ class ServerStats(C.Structure):
                 ("mrays_per_s", C.c_double)]
 
 
+class RequestRecord(C.Structure):
+    _fields_ = [("submit_s", C.c_double), ("latency_us", C.c_double), ("kind", u32), ("scene", u32),
+                ("num_rays", u32), ("status", C.c_int32)]
+
+
 SHN_REQ_CLOSEST = 0
 SHN_REQ_ANY = 1
 SHN_REQ_UPDATE = 2
@@ -128,6 +133,7 @@ SIGNATURES = {
     "shn_exclusive_scan_u32_noalloc": ([vp, vp, u32, vp], i32),
     "shn_compact_u32": ([vp, vp, u32, vp, vp, vp], i32),
     "shn_selftest_lookback_timeout": ([vp, vp], i32),
+    "shn_server_get_records": ([vp, u32, vp, vp], i32),
     "shn_sort_keys_u64": ([vp, vp, vp, u32, u32, u32, vp], i32),
 }
 

@@ -64,12 +64,19 @@ shn_status copy_in(shn_ctx* ctx, void* dst, const void* src, size_t bytes, uint3
   return e == cudaSuccess ? SHN_OK : cuda_status(ctx, e, "copy");
 }
 
+// Branch-free reductions (vectorised by the host compiler): any exponent
+// field of all ones marks an inf/NaN coordinate; the largest index must be
+// below nv.
 shn_status validate_host(shn_ctx* ctx, const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt) {
-  for (size_t i = 0; i < 3 * (size_t)nv; ++i)
-    if (!std::isfinite(vtx[i])) return set_error(ctx, SHN_ERR_INVALID, "non-finite vertex coordinate");
-  if (idx)
-    for (size_t i = 0; i < 3 * (size_t)nt; ++i)
-      if (idx[i] >= nv) return set_error(ctx, SHN_ERR_INVALID, "triangle index out of range");
+  const uint32_t* bits = reinterpret_cast<const uint32_t*>(vtx);
+  uint32_t bad = 0;
+  for (size_t i = 0; i < 3 * (size_t)nv; ++i) bad |= (uint32_t)((bits[i] & 0x7F800000u) == 0x7F800000u);
+  if (bad) return set_error(ctx, SHN_ERR_INVALID, "non-finite vertex coordinate");
+  if (idx && nt) {
+    uint32_t mx = 0;
+    for (size_t i = 0; i < 3 * (size_t)nt; ++i) mx = idx[i] > mx ? idx[i] : mx;
+    if (mx >= nv) return set_error(ctx, SHN_ERR_INVALID, "triangle index out of range");
+  }
   return SHN_OK;
 }
 
@@ -94,12 +101,33 @@ shn_status refresh_bounds(shn_scene* s, cudaStream_t st) {
 namespace shn {
 void ctx_retain(shn_ctx* c) { c->refs.fetch_add(1); }
 
+uint32_t* pinned_take(shn_ctx* c) {
+  std::lock_guard<std::mutex> lk(c->pin_mu);
+  if (c->pin_free.empty()) {
+    constexpr size_t kSlab = 64 << 10;
+    void* slab = nullptr;
+    if (cudaMallocHost(&slab, kSlab) != cudaSuccess) return nullptr;
+    c->pin_slabs.push_back(slab);
+    for (size_t off = 0; off < kSlab; off += 64) c->pin_free.push_back((uint32_t*)((char*)slab + off));
+  }
+  uint32_t* p = c->pin_free.back();
+  c->pin_free.pop_back();
+  return p;
+}
+
+void pinned_give(shn_ctx* c, uint32_t* p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(c->pin_mu);
+  c->pin_free.push_back(p);
+}
+
 void ctx_release(shn_ctx* c) {
   if (!c || c->refs.fetch_sub(1) != 1) return;
   cudaSetDevice(c->device);
   cudaDeviceSynchronize();
   if (c->d_err) cudaFree(c->d_err);
   if (c->pool) cudaMemPoolDestroy(c->pool);
+  for (void* slab : c->pin_slabs) cudaFreeHost(slab);
   delete c;
 }
 }  // namespace shn
@@ -321,8 +349,8 @@ void shn_grid_destroy(shn_grid* g) {
   dev_free(c, g->rtri, g->cap_rtri, st);
   DevBuf* bufs[] = {&g->offs_tri, &g->offs_pair, &g->scan, &g->top_ranges, &g->keys[0], &g->keys[1], &g->keys[2], &g->sortws};
   for (DevBuf* b : bufs) dev_free(c, b->ptr, b->bytes, st);
-  if (g->d_err) cudaFree(g->d_err);
-  if (g->h_pinned) cudaFreeHost(g->h_pinned);
+  dev_free(c, g->d_err, 64, st);
+  pinned_give(c, g->h_pinned);
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
   delete g;

@@ -598,8 +598,16 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   g->src_tri = s->tri;
   g->src_nt = s->nt;
   if (!g->d_err) {
-    if (cudaMalloc(&g->d_err, 64) != cudaSuccess) return set_error(ctx, SHN_ERR_OOM, "err word");
-    if (cudaMallocHost(&g->h_pinned, 64) != cudaSuccess) return set_error(ctx, SHN_ERR_OOM, "pinned");
+    // stream-ordered pool memory and a pinned block from the context's slab:
+    // no device-wide synchronisation while other streams are running
+    cudaError_t e = dev_alloc(ctx, (void**)&g->d_err, 64, st);
+    if (e != cudaSuccess) {
+      g->d_err = nullptr;
+      return e == cudaErrorNotPermitted ? set_error(ctx, SHN_ERR_BUDGET, "HBM budget exceeded")
+                                        : set_error(ctx, SHN_ERR_OOM, "err word");
+    }
+    g->h_pinned = pinned_take(ctx);
+    if (!g->h_pinned) return set_error(ctx, SHN_ERR_OOM, "pinned");
     cudaEventCreate(&g->ev0);
     cudaEventCreate(&g->ev1);
   }

@@ -37,6 +37,12 @@ struct shn_ctx {
   // scene / grid / batch / server: the context (and its memory pool) is torn
   // down when the last of them is released, whatever the destruction order.
   std::atomic<int> refs{1};
+  // 64-byte pinned host blocks for status read-backs, carved from slabs so
+  // that creating or destroying a grid never calls cudaMallocHost /
+  // cudaFreeHost (both synchronise the whole device).
+  std::mutex pin_mu;
+  std::vector<void*> pin_slabs;
+  std::vector<uint32_t*> pin_free;
 };
 
 struct shn_scene {
@@ -81,6 +87,8 @@ namespace shn {
 // api.cu
 cudaError_t dev_alloc(shn_ctx* ctx, void** p, size_t bytes, cudaStream_t st);
 void dev_free(shn_ctx* ctx, void* p, size_t bytes, cudaStream_t st);
+uint32_t* pinned_take(shn_ctx* ctx);
+void pinned_give(shn_ctx* ctx, uint32_t* p);
 void ctx_retain(shn_ctx* ctx);
 void ctx_release(shn_ctx* ctx);
 shn_status set_error(shn_ctx* ctx, shn_status s, const std::string& msg);

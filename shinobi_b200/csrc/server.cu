@@ -29,6 +29,7 @@ namespace shn {
 namespace {
 
 constexpr int kServeBlock = 128;
+constexpr int kUpdaters = 8;  // concurrent scene replacements (distinct slots)
 
 struct ServeSeg {
   uint32_t ray_begin;
@@ -99,12 +100,21 @@ struct ServeLaunch {
   std::vector<ServeReq*> reqs;
   std::vector<uint32_t> begin;
   uint32_t nrays = 0;
+  uint64_t seq = 0;             // launch number (launches complete in issue order)
   bool busy = false;
 };
 
 struct ServeSlot {
   shn_scene* scene = nullptr;
   shn_grid* grid = nullptr;
+  uint32_t pending = 0;         // updates of this slot handed to the updater, not yet applied
+};
+
+// A replaced scene/grid pair, freed once every launch issued before the
+// replacement (seq <= after_seq) has completed.
+struct ServeRetired {
+  ServeSlot pair;
+  uint64_t after_seq = 0;
 };
 
 struct shn_server {
@@ -118,12 +128,24 @@ struct shn_server {
   uint64_t next_ticket = 1;
   bool stop = false;
   std::thread worker, completer;
+  std::vector<std::thread> updaters;     // scene replacements of different slots run concurrently
+  std::vector<cudaStream_t> upd_streams;
   ServeLaunch L[2];
   std::deque<int> inflight;
   int blocks = 0;
   cudaStream_t update_st = nullptr;
+  // asynchronous scene updates (continuous-batching mode)
+  std::condition_variable cv_upd;
+  std::deque<ServeReq*> upd_q;
+  bool stop_upd = false;
+  std::vector<ServeRetired> retired;
+  std::vector<uint8_t> blocked;  // per slot, scratch of one queue scan
+  uint64_t work_gen = 0;         // bumped when a request arrives or an update is applied
+  uint32_t upd_outstanding = 0;  // updates handed to the updater and not yet applied
+  uint64_t launch_seq = 0, done_seq = 0;
   // stats
   std::vector<double> lat_us;
+  std::vector<shn_request_record> records;  // per request, completion order
   uint64_t rays_done = 0, launches = 0, requests_done = 0, updates_done = 0;
   double t_first = 0.0, t_last = 0.0;
   uint64_t max_requests_per_launch = 0;
@@ -137,14 +159,23 @@ void complete(shn_server* s, ServeReq* r, shn_status st) {
   r->done = true;
   r->t_done = now_s();
   s->lat_us.push_back((r->t_done - r->t_submit) * 1e6);
+  shn_request_record rec;
+  rec.submit_s = r->t_submit;
+  rec.latency_us = (r->t_done - r->t_submit) * 1e6;
+  rec.kind = r->r.kind;
+  rec.scene = r->r.scene;
+  rec.num_rays = r->r.kind == SHN_REQ_UPDATE ? 0u : r->r.num_rays;
+  rec.status = st;
+  s->records.push_back(rec);
   s->requests_done++;
   if (r->r.kind != SHN_REQ_UPDATE) s->rays_done += r->r.num_rays;
   s->t_last = r->t_done;
   s->cv_done.notify_all();
 }
 
-shn_status load_slot(shn_server* s, uint32_t slot, const float* vtx, uint32_t nv, const uint32_t* idx,
-                     uint32_t nt, float lambda, cudaStream_t st) {
+// New scene + uniform grid for a slot, built and synchronised on st.
+shn_status build_slot(shn_server* s, const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                      float lambda, cudaStream_t st, ServeSlot* out) {
   shn_scene* sc = nullptr;
   shn_status rc = shn_scene_create(s->ctx, vtx, nv, idx, nt, SHN_MEM_HOST, st, &sc);
   if (rc) return rc;
@@ -160,105 +191,255 @@ shn_status load_slot(shn_server* s, uint32_t slot, const float* vtx, uint32_t nv
     return rc;
   }
   cudaStreamSynchronize(st);
-  ServeSlot old = s->slots[slot];
-  s->slots[slot].scene = sc;
-  s->slots[slot].grid = g;
-  if (old.grid) shn_grid_destroy(old.grid);
-  if (old.scene) shn_scene_destroy(old.scene);
+  out->scene = sc;
+  out->grid = g;
   return SHN_OK;
 }
 
-void worker_main(shn_server* s) {
+void free_pair(const ServeSlot& p) {
+  if (p.grid) shn_grid_destroy(p.grid);
+  if (p.scene) shn_scene_destroy(p.scene);
+}
+
+// Replaces the slot's pair immediately (no launch may be using it).
+shn_status load_slot(shn_server* s, uint32_t slot, const float* vtx, uint32_t nv, const uint32_t* idx,
+                     uint32_t nt, float lambda, cudaStream_t st) {
+  ServeSlot fresh;
+  shn_status rc = build_slot(s, vtx, nv, idx, nt, lambda, st, &fresh);
+  if (rc) return rc;
+  ServeSlot old = s->slots[slot];
+  s->slots[slot].scene = fresh.scene;
+  s->slots[slot].grid = fresh.grid;
+  free_pair(old);
+  return SHN_OK;
+}
+
+// Retired pairs whose launches have all completed (caller holds s->mu;
+// free the returned pairs after unlocking).
+std::vector<ServeSlot> take_retired(shn_server* s) {
+  std::vector<ServeSlot> out;
+  size_t w = 0;
+  for (size_t i = 0; i < s->retired.size(); ++i) {
+    if (s->retired[i].after_seq <= s->done_seq) out.push_back(s->retired[i].pair);
+    else s->retired[w++] = s->retired[i];
+  }
+  s->retired.resize(w);
+  return out;
+}
+
+// Continuous-batching mode: scene replacements run here, off the launch
+// path.  The new pair is built while launches continue; it replaces the old
+// one at once for every request of that slot behind the update, and the old
+// pair is retired until the launches that captured it have completed.
+void updater_main(shn_server* s, int index) {
   cudaSetDevice(s->ctx->device);
+  const cudaStream_t ust = s->upd_streams[index];
   std::unique_lock<std::mutex> lk(s->mu);
-  int next_slot = 0;
+  while (true) {
+    s->cv_upd.wait(lk, [&] { return s->stop_upd || !s->upd_q.empty(); });
+    if (s->upd_q.empty()) {
+      if (s->stop_upd) break;
+      continue;
+    }
+    ServeReq* r = s->upd_q.front();
+    s->upd_q.pop_front();
+    const shn_request q = r->r;
+    lk.unlock();
+    ServeSlot fresh;
+    const shn_status rc = build_slot(s, q.vtx, q.nv, q.idx, q.nt, q.lambda, ust, &fresh);
+    lk.lock();
+    ServeSlot& sl = s->slots[q.scene];
+    if (rc == SHN_OK) {
+      ServeRetired old;
+      old.pair.scene = sl.scene;
+      old.pair.grid = sl.grid;
+      old.after_seq = s->launch_seq;
+      s->retired.push_back(old);
+      sl.scene = fresh.scene;
+      sl.grid = fresh.grid;
+    }
+    sl.pending--;
+    s->upd_outstanding--;
+    s->updates_done++;
+    complete(s, r, rc);
+    s->work_gen++;
+    s->cv_work.notify_all();
+    std::vector<ServeSlot> dead = take_retired(s);
+    lk.unlock();
+    for (const ServeSlot& p : dead) free_pair(p);
+    lk.lock();
+  }
+}
+
+// Issues one launch for the requests in la (segment table, ray uploads, the
+// trace, result read-backs, completion event).  Caller holds the lock; it
+// is released while the copies and the launch are enqueued.
+void issue_launch(shn_server* s, ServeLaunch& la, int slot_index, std::unique_lock<std::mutex>& lk) {
+  for (size_t k = 0; k < la.reqs.size(); ++k) {
+    const ServeReq* r = la.reqs[k];
+    const shn_grid* g = s->slots[r->r.scene].grid;
+    ServeSeg& sg = la.h_segs[k];
+    sg.ray_begin = la.begin[k];
+    sg.anyhit = r->r.kind == SHN_REQ_ANY ? 1u : 0u;
+    sg.g.g = g->geom;
+    sg.g.kind = g->kind;
+    sg.g.cells = g->cells;
+    sg.g.leaves = g->leaves;
+    sg.g.rv0 = g->rtri;
+    sg.g.rv1 = g->rtri + g->num_refs;
+    sg.g.rv2 = g->rtri + 2 * g->num_refs;
+  }
+  s->max_requests_per_launch = std::max<uint64_t>(s->max_requests_per_launch, la.reqs.size());
+  la.busy = true;
+  la.seq = ++s->launch_seq;
+  const uint32_t nseg = (uint32_t)la.reqs.size();
+  const uint32_t total = la.nrays;
+  lk.unlock();
+  cudaMemcpyAsync(la.d_segs, la.h_segs, sizeof(ServeSeg) * nseg, cudaMemcpyHostToDevice, la.st);
+  for (size_t k = 0; k < la.reqs.size(); ++k) {
+    const shn_request& q = la.reqs[k]->r;
+    cudaMemcpyAsync(la.d_rays + 2 * (size_t)la.begin[k], q.rays, 32 * (size_t)q.num_rays,
+                    cudaMemcpyHostToDevice, la.st);
+  }
+  cudaMemsetAsync(la.d_counter, 0, 4, la.st);
+  k_serve_trace<<<s->blocks, kServeBlock, 0, la.st>>>(la.d_segs, nseg, la.d_rays, total, la.d_counter,
+                                                      la.d_tri, la.d_t);
+  for (size_t k = 0; k < la.reqs.size(); ++k) {
+    const shn_request& q = la.reqs[k]->r;
+    if (q.out_tri)
+      cudaMemcpyAsync(q.out_tri, la.d_tri + la.begin[k], 4 * (size_t)q.num_rays, cudaMemcpyDeviceToHost, la.st);
+    if (q.out_t)
+      cudaMemcpyAsync(q.out_t, la.d_t + la.begin[k], 4 * (size_t)q.num_rays, cudaMemcpyDeviceToHost, la.st);
+  }
+  cudaEventRecord(la.ev_done, la.st);
+  lk.lock();
+  s->launches++;
+  s->inflight.push_back(slot_index);
+  s->cv_done.notify_all();
+}
+
+// Plain path: requests one at a time in arrival order, one launch each,
+// nothing overlaps; an update waits for the launch before it and runs inline.
+void worker_plain(shn_server* s, std::unique_lock<std::mutex>& lk) {
   while (true) {
     s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
     if (s->queue.empty() && s->stop) break;
     ServeReq* head = s->queue.front();
+    s->queue.pop_front();
+    if (head->r.scene >= s->slots.size()) {
+      complete(s, head, SHN_ERR_INVALID);
+      continue;
+    }
     if (head->r.kind == SHN_REQ_UPDATE) {
-      // every launch queued before the update must finish first
-      s->cv_launch.wait(lk, [&] { return s->inflight.empty(); });
-      s->queue.pop_front();
       const shn_request& q = head->r;
       lk.unlock();
-      shn_status rc = (q.scene < s->slots.size())
-                          ? load_slot(s, q.scene, q.vtx, q.nv, q.idx, q.nt, q.lambda, s->update_st)
-                          : SHN_ERR_INVALID;
+      const shn_status rc = load_slot(s, q.scene, q.vtx, q.nv, q.idx, q.nt, q.lambda, s->update_st);
       lk.lock();
       s->updates_done++;
       complete(s, head, rc);
       continue;
     }
-    // a free launch slot
+    if (!s->slots[head->r.scene].grid) {
+      complete(s, head, SHN_ERR_INVALID);
+      continue;
+    }
+    ServeLaunch& la = s->L[0];
+    la.reqs.assign(1, head);
+    la.begin.assign(1, 0u);
+    la.nrays = head->r.num_rays;
+    issue_launch(s, la, 0, lk);
+    s->cv_launch.wait(lk, [&] { return s->inflight.empty(); });
+  }
+}
+
+// Continuous batching: every pass packs the queued requests that may run now
+// into the next free launch slot (up to max_batch_rays / max_requests_per_launch),
+// across scenes, in arrival order.  Requests of a slot with an update in
+// progress wait for it (and keep their order); an update is handed to the
+// updater only once every earlier request of its slot has been packed, and
+// after the launch holding them captured the slot's current grid.
+void worker_coalesced(shn_server* s, std::unique_lock<std::mutex>& lk) {
+  int next_slot = 0;
+  uint64_t idle_gen = ~0ull;
+  std::vector<uint32_t> touched;
+  std::vector<ServeReq*> dispatch;
+  while (true) {
+    s->cv_work.wait(lk, [&] {
+      return (s->stop && s->queue.empty()) || (!s->queue.empty() && s->work_gen != idle_gen);
+    });
+    if (s->queue.empty()) break;  // stop requested and nothing left
+    const uint64_t gen = s->work_gen;
     s->cv_launch.wait(lk, [&] { return !s->L[next_slot].busy; });
     ServeLaunch& la = s->L[next_slot];
     la.reqs.clear();
     la.begin.clear();
+    dispatch.clear();
+    touched.clear();
     uint32_t total = 0;
-    while (!s->queue.empty()) {
-      ServeReq* r = s->queue.front();
-      if (r->r.kind == SHN_REQ_UPDATE) break;
-      if (!la.reqs.empty() && (!s->cfg.coalesce || total + r->r.num_rays > s->cfg.max_batch_rays ||
-                               la.reqs.size() >= s->cfg.max_requests_per_launch))
-        break;
-      s->queue.pop_front();
-      if (r->r.scene >= s->slots.size() || !s->slots[r->r.scene].grid) {
+    for (auto it = s->queue.begin(); it != s->queue.end();) {
+      ServeReq* r = *it;
+      const uint32_t k = r->r.scene;
+      if (k >= s->slots.size()) {
         complete(s, r, SHN_ERR_INVALID);
+        it = s->queue.erase(it);
         continue;
       }
+      if (r->r.kind == SHN_REQ_UPDATE) {
+        const bool go = !s->blocked[k] && s->slots[k].pending == 0;
+        if (!s->blocked[k]) {
+          s->blocked[k] = 1;
+          touched.push_back(k);
+        }
+        if (go) {
+          s->slots[k].pending++;
+          s->upd_outstanding++;
+          dispatch.push_back(r);
+          it = s->queue.erase(it);
+        } else {
+          ++it;
+        }
+        continue;
+      }
+      if (s->blocked[k] || s->slots[k].pending) {
+        if (!s->blocked[k]) {
+          s->blocked[k] = 1;
+          touched.push_back(k);
+        }
+        ++it;
+        continue;
+      }
+      if (!s->slots[k].grid) {
+        complete(s, r, SHN_ERR_INVALID);
+        it = s->queue.erase(it);
+        continue;
+      }
+      if (!la.reqs.empty() && (total + r->r.num_rays > s->cfg.max_batch_rays ||
+                               la.reqs.size() >= s->cfg.max_requests_per_launch))
+        break;
       la.begin.push_back(total);
       la.reqs.push_back(r);
       total += r->r.num_rays;
+      it = s->queue.erase(it);
     }
-    if (la.reqs.empty()) continue;
-    la.busy = true;
-    la.nrays = total;
-    // segment table (grid views of the scenes as of now)
-    for (size_t k = 0; k < la.reqs.size(); ++k) {
-      const ServeReq* r = la.reqs[k];
-      const shn_grid* g = s->slots[r->r.scene].grid;
-      ServeSeg& sg = la.h_segs[k];
-      sg.ray_begin = la.begin[k];
-      sg.anyhit = r->r.kind == SHN_REQ_ANY ? 1u : 0u;
-      sg.g.g = g->geom;
-      sg.g.kind = g->kind;
-      sg.g.cells = g->cells;
-      sg.g.leaves = g->leaves;
-      sg.g.rv0 = g->rtri;
-      sg.g.rv1 = g->rtri + g->num_refs;
-      sg.g.rv2 = g->rtri + 2 * g->num_refs;
+    for (uint32_t k : touched) s->blocked[k] = 0;
+    if (!la.reqs.empty()) {
+      la.nrays = total;
+      issue_launch(s, la, next_slot, lk);
+      next_slot ^= 1;
     }
-    s->max_requests_per_launch = std::max<uint64_t>(s->max_requests_per_launch, la.reqs.size());
-    const uint32_t nseg = (uint32_t)la.reqs.size();
-    lk.unlock();
-    cudaMemcpyAsync(la.d_segs, la.h_segs, sizeof(ServeSeg) * nseg, cudaMemcpyHostToDevice, la.st);
-    for (size_t k = 0; k < la.reqs.size(); ++k) {
-      const shn_request& q = la.reqs[k]->r;
-      cudaMemcpyAsync(la.d_rays + 2 * (size_t)la.begin[k], q.rays, 32 * (size_t)q.num_rays,
-                      cudaMemcpyHostToDevice, la.st);
+    if (!dispatch.empty()) {
+      for (ServeReq* r : dispatch) s->upd_q.push_back(r);
+      s->cv_upd.notify_all();
     }
-    cudaMemsetAsync(la.d_counter, 0, 4, la.st);
-    k_serve_trace<<<s->blocks, kServeBlock, 0, la.st>>>(la.d_segs, nseg, la.d_rays, total, la.d_counter,
-                                                        la.d_tri, la.d_t);
-    for (size_t k = 0; k < la.reqs.size(); ++k) {
-      const shn_request& q = la.reqs[k]->r;
-      if (q.out_tri)
-        cudaMemcpyAsync(q.out_tri, la.d_tri + la.begin[k], 4 * (size_t)q.num_rays, cudaMemcpyDeviceToHost, la.st);
-      if (q.out_t)
-        cudaMemcpyAsync(q.out_t, la.d_t + la.begin[k], 4 * (size_t)q.num_rays, cudaMemcpyDeviceToHost, la.st);
-    }
-    cudaEventRecord(la.ev_done, la.st);
-    lk.lock();
-    s->launches++;
-    s->inflight.push_back(next_slot);
-    s->cv_done.notify_all();
-    if (!s->cfg.coalesce) {
-      // plain path: one request, one launch, nothing overlaps
-      s->cv_launch.wait(lk, [&] { return s->inflight.empty(); });
-    }
-    next_slot ^= 1;
+    if (la.reqs.empty() && dispatch.empty()) idle_gen = gen;  // nothing can run until something changes
   }
+}
+
+void worker_main(shn_server* s) {
+  cudaSetDevice(s->ctx->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  if (s->cfg.coalesce) worker_coalesced(s, lk);
+  else worker_plain(s, lk);
 }
 
 void completer_main(shn_server* s) {
@@ -279,9 +460,16 @@ void completer_main(shn_server* s) {
     for (ServeReq* r : la.reqs) complete(s, r, st);
     la.reqs.clear();
     la.busy = false;
+    s->done_seq = la.seq;
     s->inflight.pop_front();
     s->cv_launch.notify_all();
     s->cv_work.notify_all();
+    std::vector<ServeSlot> dead = take_retired(s);
+    if (!dead.empty()) {
+      lk.unlock();
+      for (const ServeSlot& p : dead) free_pair(p);
+      lk.lock();
+    }
   }
 }
 
@@ -307,6 +495,7 @@ shn_status shn_server_create(shn_ctx* ctx, const shn_server_config* cfg, shn_ser
   ctx_retain(ctx);
   s->cfg = *cfg;
   s->slots.resize(cfg->num_slots);
+  s->blocked.assign(cfg->num_slots, 0);
   cudaStreamCreateWithFlags(&s->update_st, cudaStreamNonBlocking);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_serve_trace, kServeBlock, 0);
@@ -329,6 +518,12 @@ shn_status shn_server_create(shn_ctx* ctx, const shn_server_config* cfg, shn_ser
   }
   s->worker = std::thread(worker_main, s);
   s->completer = std::thread(completer_main, s);
+  for (int i = 0; i < kUpdaters; ++i) {
+    cudaStream_t us = nullptr;
+    cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking);
+    s->upd_streams.push_back(us);
+  }
+  for (int i = 0; i < kUpdaters; ++i) s->updaters.emplace_back(updater_main, s, i);
   *out = s;
   return SHN_OK;
 }
@@ -365,6 +560,7 @@ shn_status shn_server_submit(shn_server* s, const shn_request* r, uint64_t* tick
   if (s->t_first == 0.0) s->t_first = q->t_submit;
   s->reqs[q->ticket] = q;
   s->queue.push_back(q);
+  s->work_gen++;
   *ticket = q->ticket;
   s->cv_work.notify_one();
   return SHN_OK;
@@ -392,7 +588,7 @@ shn_status shn_server_drain(shn_server* s, uint32_t timeout_ms) {
   if (!s) return SHN_ERR_INVALID;
   std::unique_lock<std::mutex> lk(s->mu);
   const bool ok = s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms),
-                                      [&] { return s->queue.empty() && s->inflight.empty(); });
+                                      [&] { return s->queue.empty() && s->inflight.empty() && s->upd_outstanding == 0; });
   return ok ? SHN_OK : SHN_ERR_BUSY;
 }
 
@@ -419,10 +615,21 @@ shn_status shn_server_get_stats(shn_server* s, shn_server_stats* out, int reset)
   out->mrays_per_s = out->wall_s > 0 ? s->rays_done / out->wall_s / 1e6 : 0.0;
   if (reset) {
     s->lat_us.clear();
+    s->records.clear();
     s->rays_done = s->launches = s->requests_done = s->updates_done = 0;
     s->t_first = s->t_last = 0.0;
     s->max_requests_per_launch = 0;
   }
+  return SHN_OK;
+}
+
+shn_status shn_server_get_records(shn_server* s, uint32_t max_records, shn_request_record* out,
+                                  uint32_t* count) {
+  if (!s || !count || (max_records && !out)) return SHN_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  const uint32_t n = (uint32_t)std::min<size_t>(max_records, s->records.size());
+  if (n) memcpy(out, s->records.data(), n * sizeof(shn_request_record));
+  *count = (uint32_t)s->records.size();
   return SHN_OK;
 }
 
@@ -466,15 +673,20 @@ void shn_server_destroy(shn_server* s) {
   if (s->worker.joinable()) s->worker.join();
   {
     std::lock_guard<std::mutex> lk(s->mu);
+    s->stop_upd = true;
+  }
+  s->cv_upd.notify_all();
+  for (std::thread& t : s->updaters)
+    if (t.joinable()) t.join();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
     s->cv_done.notify_all();
   }
   if (s->completer.joinable()) s->completer.join();
   cudaDeviceSynchronize();
   for (auto& kv : s->reqs) delete kv.second;
-  for (auto& sl : s->slots) {
-    if (sl.grid) shn_grid_destroy(sl.grid);
-    if (sl.scene) shn_scene_destroy(sl.scene);
-  }
+  for (auto& r : s->retired) free_pair(r.pair);
+  for (auto& sl : s->slots) free_pair(sl);
   for (int i = 0; i < 2; ++i) {
     ServeLaunch& la = s->L[i];
     dev_free(s->ctx, la.d_rays, 32 * (size_t)s->cfg.max_batch_rays, la.st);
@@ -490,6 +702,7 @@ void shn_server_destroy(shn_server* s) {
     }
   }
   if (s->update_st) cudaStreamDestroy(s->update_st);
+  for (cudaStream_t us : s->upd_streams) cudaStreamDestroy(us);
   shn_ctx* c = s->ctx;
   delete s;
   ctx_release(c);
