@@ -499,9 +499,11 @@ def run_batch(args):
     ms = []
     for _ in range(args.steps):
         a, b = ev(), ev()
+        torch.cuda.nvtx.range_push("shn_batch_step")   # profiler filter: --nvtx-include shn_batch_step/
         a.record()
         bt.replay()
         b.record()
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         ms.append(a.elapsed_time(b))
     batched_ms = float(np.mean(ms))
@@ -599,9 +601,11 @@ def run_pathtrace(args):
     for _ in range(args.steps):
         stats.zero_()
         a, b = ev(), ev()
+        torch.cuda.nvtx.range_push("shn_pathtrace_step")
         a.record()
         grid.pt_render(soup, cam, params, out=img, stats=stats)
         b.record()
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         ms.append(a.elapsed_time(b))
     clk = clocks.stop()
