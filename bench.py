@@ -480,7 +480,7 @@ def run_batch(args):
     bt = shn.Batch.__new__(shn.Batch)
     bt.ctx, bt.handle, bt.num_scenes, bt.tri_offsets = ctx, h, ns, to
     t0 = time.perf_counter()
-    cands = np.array([2.0, 3.0, 5.0, 8.0], np.float32)
+    cands = np.array([0.5, 0.75, 1.0, 1.5, 2.0, 3.0], np.float32)
     chosen = bt.autotune(cands, expected_rays=rays.astype(np.uint32), sample_rays=16384)
     t_tune = time.perf_counter() - t0
     bt.build()
