@@ -78,12 +78,14 @@ SHN_D bool wt_test(const RayWT& r, float4 p0, float4 p1, float4 p2, float tmin, 
   float U = __fmaf_rn(Cx, By, -(Cy * Bx));
   float V = __fmaf_rn(Ax, Cy, -(Ay * Cx));
   float W = __fmaf_rn(Bx, Ay, -(By * Ax));
-  if (U == 0.f || V == 0.f || W == 0.f) {
+  // exact zero of an edge function -> recompute in double; mixed signs -> miss
+  // (min/max skip a NaN operand exactly as or-chains of comparisons do)
+  if (fminf(fminf(fabsf(U), fabsf(V)), fabsf(W)) == 0.f) {
     U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
     V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
     W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
   }
-  if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
+  if (fminf(fminf(U, V), W) < 0.f && fmaxf(fmaxf(U, V), W) > 0.f) return false;
   const float det = U + V + W;
   if (det == 0.f) return false;
   const float T = __fmaf_rn(W, r.Sz * Ckz, __fmaf_rn(V, r.Sz * Bkz, U * (r.Sz * Akz)));

@@ -242,12 +242,15 @@ SHN_D bool wt_test_p(V3 org, float Sx, float Sy, float Sz, float4 p0, float4 p1,
   float U = __fmaf_rn(Cx, By, -(Cy * Bx));
   float V = __fmaf_rn(Ax, Cy, -(Ay * Cx));
   float W = __fmaf_rn(Bx, Ay, -(By * Ax));
-  if (U == 0.f || V == 0.f || W == 0.f) {
+  // "some edge function is exactly zero" and "the signs differ", written with
+  // min/max (fminf/fmaxf skip a NaN operand exactly as the or-chains of
+  // comparisons do, so the outcome is that of the generic wt_test)
+  if (fminf(fminf(fabsf(U), fabsf(V)), fabsf(W)) == 0.f) {
     U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
     V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
     W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
   }
-  if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
+  if (fminf(fminf(U, V), W) < 0.f && fmaxf(fmaxf(U, V), W) > 0.f) return false;
   const float det = U + V + W;
   if (det == 0.f) return false;
   const float T = __fmaf_rn(W, Sz * Ckz, __fmaf_rn(V, Sz * Bkz, U * (Sz * Akz)));
@@ -270,13 +273,17 @@ SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz,
   const int lane = threadIdx.x & 31;
   uint64_t key = ~0ull;
   float tb = tbest;
-  for (uint32_t base = b; base < e; base += 32) {
+  const float4* q0 = G.rv0 + b + lane;
+  const float4* q1 = G.rv1 + b + lane;
+  const float4* q2 = G.rv2 + b + lane;
+  uint32_t tested_end = e;
+  for (uint32_t base = b; base < e; base += 32, q0 += 32, q1 += 32, q2 += 32) {
     const uint32_t it = base + lane;
     bool hit = false;
     if (it < e) {
-      const float4 p0 = __ldg(G.rv0 + it);
-      const float4 p1 = __ldg(G.rv1 + it);
-      const float4 p2 = __ldg(G.rv2 + it);
+      const float4 p0 = __ldg(q0);
+      const float4 p1 = __ldg(q1);
+      const float4 p2 = __ldg(q2);
       float t;
       if (wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, p0, p1, p2, kEps, tb, t)) {
         tb = t;
@@ -284,9 +291,12 @@ SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz,
         hit = true;
       }
     }
-    tests += min(32u, e - base);
-    if (ANY && __any_sync(0xFFFFFFFFu, hit)) break;
+    if (ANY && __any_sync(0xFFFFFFFFu, hit)) {
+      tested_end = min(e, base + 32u);
+      break;
+    }
   }
+  tests += tested_end - b;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const uint64_t other = __shfl_xor_sync(0xFFFFFFFFu, key, o);
