@@ -479,16 +479,7 @@ shn_status shn_batch_autotune(shn_batch* b, const float* candidates, uint32_t nu
     sc.ctx = ctx;
     sc.nt = nt;
     sc.nv = 0;
-    float4* view = nullptr;
-    e = dev_alloc(ctx, (void**)&view, 48 * (size_t)nt, st);
-    if (e != cudaSuccess) {
-      rc = alloc_err(b, e, "autotune scene");
-      break;
-    }
-    for (int k = 0; k < 3; ++k)
-      cudaMemcpyAsync(view + (size_t)k * nt, b->tri + (size_t)k * b->T + b->tri_off[s], 16 * (size_t)nt,
-                      cudaMemcpyDeviceToDevice, st);
-    sc.tri = view;
+    sc.tri = b->tri + 3 * (size_t)b->tri_off[s];  // the scene's records, in place
     memcpy(sc.bounds, &b->bounds[6 * s], 24);
     double best_cost = 1e300;
     for (uint32_t c = 0; c < num_candidates; ++c) {
@@ -514,7 +505,6 @@ shn_status shn_batch_autotune(shn_batch* b, const float* candidates, uint32_t nu
         best[s] = candidates[c];
       }
     }
-    dev_free(ctx, view, 48 * (size_t)nt, st);
   }
   shn_grid_destroy(g);
   cudaEventDestroy(e0);

@@ -33,16 +33,19 @@ constexpr int kScanBlock = 256;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanBlock * kScanItems;
 
-struct TriSoA {
-  const float4* v0;
-  const float4* v1;
-  const float4* v2;
+// Scene triangles, one 48-byte record per triangle: v0 (w = triangle id
+// bits), v1, v2.  A record spans at most two 32-byte sectors, so the gather
+// of a triangle by id (reference-ordered copy, AO and path-tracer normals)
+// touches 2 sectors instead of 3 for three separate arrays.
+struct TriArr {
+  const float4* p;
 };
 
-SHN_D void load_tri(const TriSoA& t, uint32_t i, V3& a, V3& b, V3& c) {
-  a = f4v(__ldg(t.v0 + i));
-  b = f4v(__ldg(t.v1 + i));
-  c = f4v(__ldg(t.v2 + i));
+SHN_D void load_tri(const TriArr& t, uint32_t i, V3& a, V3& b, V3& c) {
+  const float4* r = t.p + 3 * (size_t)i;
+  a = f4v(__ldg(r));
+  b = f4v(__ldg(r + 1));
+  c = f4v(__ldg(r + 2));
 }
 
 SHN_D void tri_bounds(V3 a, V3 b, V3 c, V3& bmin, V3& bmax) {
@@ -168,7 +171,7 @@ SHN_D void leaf_unit(V3 a, V3 b, V3 c, const Geom& g, uint32_t topCell, uint32_t
 
 // ---- unit makers: item index -> unit ------------------------------------------------
 struct TopMaker {
-  TriSoA tri;
+  TriArr tri;
   Geom g;
   SHN_D bool operator()(uint32_t t, Unit& U) const {
     V3 a, b, c;
@@ -179,7 +182,7 @@ struct TopMaker {
 };
 
 struct LeafMaker {
-  TriSoA tri;
+  TriArr tri;
   const uint64_t* top;  // sorted (top cell << 32 | tri)
   const uint2* cells;   // top cell words
   Geom g;
@@ -246,9 +249,10 @@ __global__ void k_pack_triangles(const float* __restrict__ vtx, const uint32_t* 
     const float* a = vtx + 3 * (size_t)i0;
     const float* b = vtx + 3 * (size_t)i1;
     const float* c = vtx + 3 * (size_t)i2;
-    tri[t] = make_float4(a[0], a[1], a[2], __uint_as_float(t));
-    tri[nt + (size_t)t] = make_float4(b[0], b[1], b[2], 0.f);
-    tri[2 * (size_t)nt + t] = make_float4(c[0], c[1], c[2], 0.f);
+    float4* r = tri + 3 * (size_t)t;
+    r[0] = make_float4(a[0], a[1], a[2], __uint_as_float(t));
+    r[1] = make_float4(b[0], b[1], b[2], 0.f);
+    r[2] = make_float4(c[0], c[1], c[2], 0.f);
   }
 }
 
@@ -304,7 +308,7 @@ constexpr int kRangeBlock = 256;
 
 __global__ void __launch_bounds__(kRangeBlock) k_ranges(const uint64_t* __restrict__ keys, uint32_t n,
                                                         uint2* __restrict__ ranges,
-                                                        uint32_t* __restrict__ indices, TriSoA tri,
+                                                        uint32_t* __restrict__ indices, TriArr tri,
                                                         float4* __restrict__ rtri) {
   const int lane = threadIdx.x & 31;
   constexpr uint32_t kStep = kRangeBlock * kRangeItems;
@@ -323,9 +327,10 @@ __global__ void __launch_bounds__(kRangeBlock) k_ranges(const uint64_t* __restri
       for (int q = 0; q < kRangeItems; ++q) {
         const uint64_t i = b0 + q * kRangeBlock + threadIdx.x;
         if (i < n) {
-          a[q] = __ldg(tri.v0 + t[q]);
-          b[q] = __ldg(tri.v1 + t[q]);
-          d[q] = __ldg(tri.v2 + t[q]);
+          const float4* r = tri.p + 3 * (size_t)t[q];
+          a[q] = __ldg(r);
+          b[q] = __ldg(r + 1);
+          d[q] = __ldg(r + 2);
         }
       }
     }
@@ -401,9 +406,10 @@ __global__ void k_batch_pack(const float* __restrict__ vtx, const uint32_t* __re
     const float* a = vtx + 3 * (size_t)i0;
     const float* b = vtx + 3 * (size_t)i1;
     const float* c = vtx + 3 * (size_t)i2;
-    tri[t] = make_float4(a[0], a[1], a[2], __uint_as_float(t));
-    tri[T + (size_t)t] = make_float4(b[0], b[1], b[2], 0.f);
-    tri[2 * (size_t)T + t] = make_float4(c[0], c[1], c[2], 0.f);
+    float4* r = tri + 3 * (size_t)t;
+    r[0] = make_float4(a[0], a[1], a[2], __uint_as_float(t));
+    r[1] = make_float4(b[0], b[1], b[2], 0.f);
+    r[2] = make_float4(c[0], c[1], c[2], 0.f);
   }
 }
 
@@ -416,7 +422,7 @@ __global__ void k_batch_bounds(const float4* __restrict__ tri, const uint32_t* _
     V3 mn = mk(FLT_MAX, FLT_MAX, FLT_MAX), mx = mk(-FLT_MAX, -FLT_MAX, -FLT_MAX);
     if (valid) {
       for (int k = 0; k < 3; ++k) {
-        const V3 p = f4v(tri[(size_t)k * T + t]);
+        const V3 p = f4v(tri[3 * (size_t)t + k]);
         mn = vmin(mn, p);
         mx = vmax(mx, p);
       }
@@ -448,7 +454,7 @@ __global__ void k_batch_bounds_decode(uint32_t* io, uint32_t n) {
 }
 
 struct BatchMaker {
-  TriSoA tri;
+  TriArr tri;
   const uint32_t* tri_off;
   const BatchScene* scenes;
   uint32_t ns;
@@ -613,7 +619,7 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   }
   cudaMemsetAsync(g->d_err, 0, 64, st);
   cudaEventRecord(g->ev0, st);
-  const TriSoA tri{s->tri, s->tri + nt, s->tri + 2 * (size_t)nt};
+  const TriArr tri{s->tri};
   shn_status rc;
 
   // ---- counts + offsets ------------------------------------------------------
@@ -738,14 +744,14 @@ void launch_batch_count(const float4* tri, uint32_t T, const uint32_t* tri_off, 
   uint64_t* status = (uint64_t*)scan_ws;
   cudaMemsetAsync(status, 0, (tiles + 2) * 8, st);
   LookbackState ls{status, (uint32_t*)(status + tiles + 1), err};
-  const TriSoA ts{tri, tri + T, tri + 2 * (size_t)T};
+  const TriArr ts{tri};
   k_count_units<<<(unsigned)tiles, kScanBlock, 0, st>>>(BatchMaker{ts, tri_off, scenes, ns}, T, ls, offs);
 }
 
 void launch_batch_emit(const float4* tri, uint32_t T, const uint32_t* tri_off, const BatchScene* scenes,
                        uint32_t ns, const uint32_t* offs, uint64_t* keys, uint32_t capacity,
                        uint32_t* err, cudaStream_t st) {
-  const TriSoA ts{tri, tri + T, tri + 2 * (size_t)T};
+  const TriArr ts{tri};
   if (T)
     k_emit_units<<<emit_blocks(T), kScanBlock, 0, st>>>(BatchMaker{ts, tri_off, scenes, ns}, T, offs, keys,
                                                        capacity, err);
@@ -753,7 +759,7 @@ void launch_batch_emit(const float4* tri, uint32_t T, const uint32_t* tri_off, c
 
 void launch_ranges(const uint64_t* keys, uint32_t n, uint2* ranges, uint32_t* indices,
                    const float4* tri, uint32_t T, float4* rtri, cudaStream_t st) {
-  const TriSoA ts{tri, tri + T, tri + 2 * (size_t)T};
+  const TriArr ts{tri};
   if (n) k_ranges<<<range_blocks(n), kRangeBlock, 0, st>>>(keys, n, ranges, indices, ts, rtri);
 }
 

@@ -50,7 +50,7 @@ struct shn_scene {
   uint32_t nv = 0, nt = 0;
   float* vtx = nullptr;      // 3*nv
   uint32_t* idx = nullptr;   // 3*nt
-  float4* tri = nullptr;     // 3*nt: v0[nt], v1[nt], v2[nt] (w of v0 = tri id bits)
+  float4* tri = nullptr;     // 3*nt: per triangle a 48-byte record v0, v1, v2 (w of v0 = tri id bits)
   float bounds[6] = {0, 0, 0, 0, 0, 0};
   size_t bytes = 0;
 };

@@ -97,9 +97,10 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_bounce(GridView G, PtView P, Pa
     if (h.tri == kMiss) {
       L = add(L, mul(beta, P.bg));
     } else {
-      const V3 v0 = f4v(__ldg(P.stri + h.tri));
-      const V3 v1 = f4v(__ldg(P.stri + P.snt + h.tri));
-      const V3 v2 = f4v(__ldg(P.stri + 2 * (size_t)P.snt + h.tri));
+      const float4* rec = P.stri + 3 * (size_t)h.tri;
+      const V3 v0 = f4v(__ldg(rec));
+      const V3 v1 = f4v(__ldg(rec + 1));
+      const V3 v2 = f4v(__ldg(rec + 2));
       const V3 e1 = sub(v1, v0);
       V3 nn = normalize(cross(e1, sub(v2, v0)));
       if (dot(nn, dir) > 0.f) nn = mk(-nn.x, -nn.y, -nn.z);

@@ -109,7 +109,7 @@ struct AoParams {
   CamView cam;
   uint32_t image_id, spp, seed;
   float len, offset;
-  const float4* stri;  // scene triangles v0[nt], v1[nt], v2[nt]
+  const float4* stri;  // scene triangles, 48-byte records (v0, v1, v2)
   uint32_t snt;
 };
 
@@ -131,9 +131,10 @@ __global__ void __launch_bounds__(kTraceBlock, 8) k_trace_ao(GridView G, AoParam
         const uint32_t tri = ptri[p];
         const float t = pt[p];
         const V3 d = primary_dir(A.cam, p, A.image_id);
-        const V3 v0 = f4v(__ldg(A.stri + tri));
-        const V3 v1 = f4v(__ldg(A.stri + A.snt + tri));
-        const V3 v2 = f4v(__ldg(A.stri + 2 * (size_t)A.snt + tri));
+        const float4* rec = A.stri + 3 * (size_t)tri;
+        const V3 v0 = f4v(__ldg(rec));
+        const V3 v1 = f4v(__ldg(rec + 1));
+        const V3 v2 = f4v(__ldg(rec + 2));
         const V3 e1 = sub(v1, v0);
         V3 nn = normalize(cross(e1, sub(v2, v0)));
         if (dot(nn, d) > 0.f) nn = mk(-nn.x, -nn.y, -nn.z);
