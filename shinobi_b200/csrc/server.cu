@@ -29,7 +29,7 @@ namespace shn {
 namespace {
 
 constexpr int kServeBlock = 128;
-constexpr int kUpdaters = 8;  // concurrent scene replacements (distinct slots)
+constexpr int kUpdaters = 16;  // concurrent scene replacements (distinct slots)
 
 struct ServeSeg {
   uint32_t ray_begin;
