@@ -25,6 +25,7 @@
 namespace shn {
 
 constexpr uint32_t kCoopThreshold = 32;
+constexpr int kCoopBlock = 128;  // threads per block of every kernel that runs the engine
 
 // Reference-ordered triangle arrays of one grid.
 struct Refs {
@@ -277,7 +278,35 @@ SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz,
   const float4* q1 = G.rv1 + b + lane;
   const float4* q2 = G.rv2 + b + lane;
   uint32_t tested_end = e;
-  for (uint32_t base = b; base < e; base += 32, q0 += 32, q1 += 32, q2 += 32) {
+  uint32_t base = b;
+  if (!ANY) {
+    // closest hit: two references per lane per step (independent tests in
+    // flight); the lane-local minimum is updated in reference order, so the
+    // warp's argmin over (t, reference) is that of the sequential loop
+    for (; base + 32 < e; base += 64, q0 += 64, q1 += 64, q2 += 64) {
+      const uint32_t it = base + lane, it2 = it + 32;
+      const float4 a0 = __ldg(q0), a1 = __ldg(q1), a2 = __ldg(q2);
+      const bool has2 = it2 < e;
+      float4 c0 = a0, c1 = a1, c2 = a2;
+      if (has2) {
+        c0 = __ldg(q0 + 32);
+        c1 = __ldg(q1 + 32);
+        c2 = __ldg(q2 + 32);
+      }
+      float t;
+      if (it < e && wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, a0, a1, a2, kEps, tb, t)) {
+        tb = t;
+        key = ((uint64_t)__float_as_uint(t) << 32) | it;
+      }
+      if (has2 && wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, c0, c1, c2, kEps, tb, t)) {
+        tb = t;
+        key = ((uint64_t)__float_as_uint(t) << 32) | it2;
+      }
+    }
+  }
+  // any hit (stops after the first 32-reference chunk holding a hit), and the
+  // last chunk of a closest-hit range
+  for (; base < e; base += 32, q0 += 32, q1 += 32, q2 += 32) {
     const uint32_t it = base + lane;
     bool hit = false;
     if (it < e) {
@@ -359,6 +388,7 @@ SHN_D void lane_result(const Refs& G, const Lane& L, Hit& h) {
 // tests) consumes its result.  n rays are taken from *counter (pre-zeroed).
 template <int KIND, bool ANY, class Acc, class Src, class Sink>
 SHN_D void warp_trace_acc(const Acc& acc, uint32_t n, uint32_t* counter, Src&& src, Sink&& sink) {
+  __shared__ Lane lane_park[kCoopBlock];
   const int lane = threadIdx.x & 31;
   const uint32_t lt = (1u << lane) - 1u;
   Lane L;
@@ -407,31 +437,38 @@ SHN_D void warp_trace_acc(const Acc& acc, uint32_t n, uint32_t* counter, Src&& s
     const bool big = pending && (L.e - L.b > kCoopThreshold);
     if (pending && !big) lane_range<ANY>(acc.refs(scene), L, tests);
     uint32_t bmask = __ballot_sync(0xFFFFFFFFu, big);
-    while (bmask) {
-      const int j = __ffs(bmask) - 1;
-      bmask &= bmask - 1;
-      const V3 org = mk(__shfl_sync(0xFFFFFFFFu, L.org.x, j), __shfl_sync(0xFFFFFFFFu, L.org.y, j),
-                        __shfl_sync(0xFFFFFFFFu, L.org.z, j));
-      const float Sx = __shfl_sync(0xFFFFFFFFu, L.Sx, j);
-      const float Sy = __shfl_sync(0xFFFFFFFFu, L.Sy, j);
-      const float Sz = __shfl_sync(0xFFFFFFFFu, L.Sz, j);
-      const uint32_t perm = __shfl_sync(0xFFFFFFFFu, L.perm, j);
-      const float tb = __shfl_sync(0xFFFFFFFFu, L.tbest, j);
-      const uint32_t b = __shfl_sync(0xFFFFFFFFu, L.b, j);
-      const uint32_t e = __shfl_sync(0xFFFFFFFFu, L.e, j);
-      const uint32_t sj = __shfl_sync(0xFFFFFFFFu, scene, j);
-      const uint32_t aj = __shfl_sync(0xFFFFFFFFu, L.anyhit, j);
-      const Refs R = acc.refs(sj);
-      uint32_t wt = 0;
-      const uint64_t key = (ANY || aj) ? warp_range<true>(R, perm, org, Sx, Sy, Sz, tb, b, e, wt)
-                                       : warp_range<false>(R, perm, org, Sx, Sy, Sz, tb, b, e, wt);
-      if (lane == j) {
-        tests += wt;
-        if (key != ~0ull) {
-          L.tbest = __uint_as_float((uint32_t)(key >> 32));
-          L.best = (uint32_t)key;
+    if (bmask) {
+      // The lanes' traversal state waits in shared memory while the warp tests
+      // the large ranges, so the test loop has the registers to itself.
+      Lane* park = lane_park + (threadIdx.x & ~31u);
+      park[lane] = L;
+      __syncwarp();
+      while (bmask) {
+        const int j = __ffs(bmask) - 1;
+        bmask &= bmask - 1;
+        const Lane& Lj = park[j];
+        const V3 org = Lj.org;
+        const float Sx = Lj.Sx, Sy = Lj.Sy, Sz = Lj.Sz;
+        const uint32_t perm = Lj.perm;
+        const float tb = Lj.tbest;
+        const uint32_t b = Lj.b, e = Lj.e;
+        const uint32_t aj = Lj.anyhit;
+        const uint32_t sj = __shfl_sync(0xFFFFFFFFu, scene, j);
+        const Refs R = acc.refs(sj);
+        uint32_t wt = 0;
+        const uint64_t key = (ANY || aj) ? warp_range<true>(R, perm, org, Sx, Sy, Sz, tb, b, e, wt)
+                                         : warp_range<false>(R, perm, org, Sx, Sy, Sz, tb, b, e, wt);
+        if (lane == j) {
+          tests += wt;
+          if (key != ~0ull) {
+            park[j].tbest = __uint_as_float((uint32_t)(key >> 32));
+            park[j].best = (uint32_t)key;
+          }
         }
+        __syncwarp();
       }
+      L = park[lane];
+      __syncwarp();
     }
   }
 }
