@@ -114,7 +114,7 @@ struct AoParams {
 };
 
 template <int KIND, bool STATS>
-__global__ void __launch_bounds__(kTraceBlock, 8) k_trace_ao(GridView G, AoParams A,
+__global__ void __launch_bounds__(kTraceBlock, 9) k_trace_ao(GridView G, AoParams A,
                                                           const uint32_t* __restrict__ ptri,
                                                           const float* __restrict__ pt,
                                                           const uint32_t* __restrict__ hit_idx,
