@@ -1,10 +1,11 @@
 // Sort-based uniform and two-level grid construction for sm_100a.
 //
 // Pipeline (uniform grid, and the top level of the two-level grid):
-//   k_count_units       exact per-triangle cell counts (bbox range + plane
-//                       test, by row intervals: rows.cuh) fused with a
-//                       decoupled look-back exclusive scan -> per-triangle
-//                       output offsets and the pair total
+//   k_count_groups      exact per-triangle cell counts (bbox range + plane
+//                       test, by row intervals: rows.cuh), warps pulling
+//                       32 triangles at a time
+//   k_scan_inplace      decoupled look-back exclusive scan of the counts ->
+//                       per-triangle output offsets and the pair total
 //   k_emit_units        packed (cell << 32 | tri) keys, triangle order
 //   onesweep_sort       stable 8-bit-digit LSD sort on the cell bits
 //   k_ranges            [begin,end) per cell, indices[] and the
@@ -12,7 +13,7 @@
 // Two-level leaf stage:
 //   k_leaf_cells_scan   leaf resolution per top cell fused with the scan of
 //                       leaf-cell counts -> TwoLevelGridCell words
-//   k_count_units       exact leaf-cell counts per sorted top pair + scan
+//   k_count_groups + k_scan_inplace: exact leaf-cell counts per sorted top pair
 //   k_emit_units        (leafId << 32 | tri) keys
 //   onesweep_sort + k_ranges on the leaf keys.
 //
@@ -200,26 +201,37 @@ struct LeafMaker {
 // ---- generic count (fused with the offsets scan) and emit kernels --------------------
 constexpr int kUnitWarps = kScanBlock / 32;
 
-// Exact pair count of every item, exclusive-scanned into offs[0..n], with
-// offs[n] = total.  Each warp produces 32 consecutive items at a time.
+// Exact pair count of every item into counts[i].  Warps take 32 items at a
+// time from a global counter: no block-wide barrier, so warps whose items
+// span many rows do not hold up the others (the tile-fused form above spent
+// most of its time waiting at the tile barrier).
 template <class Maker>
-__global__ void __launch_bounds__(kScanBlock) k_count_units(Maker mk, uint32_t n, LookbackState st,
-                                                           uint32_t* offs) {
-  __shared__ TileScanSmem<kScanBlock, kScanItems> sm;
+__global__ void __launch_bounds__(kScanBlock) k_count_groups(Maker mk, uint32_t n, uint32_t* __restrict__ counts,
+                                                            uint32_t* group_counter) {
   __shared__ Unit su[kUnitWarps][32];
   __shared__ uint32_t acc[kUnitWarps][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t tile = tile_begin(st, sm);
-  const uint64_t base = (uint64_t)tile * kScanTile;
-  for (int k = 0; k < kScanItems; ++k) {
-    const int li = (warp * kScanItems + k) * 32 + lane;
-    const uint64_t i = base + li;
-    const bool valid = i < n && mk((uint32_t)i, su[warp][lane]);
+  const uint32_t groups = (n + 31u) / 32u;
+  while (true) {
+    uint32_t gidx = 0;
+    if (lane == 0) gidx = atomicAdd(group_counter, 1u);
+    gidx = __shfl_sync(0xFFFFFFFFu, gidx, 0);
+    if (gidx >= groups) break;
+    const uint32_t i = gidx * 32u + lane;
+    const bool valid = i < n && mk(i, su[warp][lane]);
     __syncwarp();
-    sm.items[pad_idx(li)] = warp_count_units(su[warp], acc[warp], valid);
+    const uint32_t c = warp_count_units(su[warp], acc[warp], valid);
+    if (i < n) counts[i] = c;
     __syncwarp();
   }
-  tile_finish(st, n, tile, sm, [&](uint32_t i, uint32_t ex) { offs[i] = ex; }, offs + n);
+}
+
+// In-place exclusive scan: data[0..n) -> prefixes, data[n] = total.  Each
+// tile reads all of its items before it writes any.
+__global__ void __launch_bounds__(kScanBlock) k_scan_inplace(uint32_t* data, uint32_t n, LookbackState st) {
+  __shared__ TileScanSmem<kScanBlock, kScanItems> sm;
+  tile_scan<kScanBlock, kScanItems>(
+      st, n, sm, [&](uint32_t i) { return data[i]; }, [&](uint32_t i, uint32_t ex) { data[i] = ex; }, data + n);
 }
 
 // Keys of every item at offs[item]: 32 items per warp step, coalesced stores.
@@ -472,6 +484,20 @@ int grid_for(uint64_t n, int block, int max_blocks) {
   return (int)std::max<uint64_t>(1, std::min<uint64_t>(b, (uint64_t)max_blocks));
 }
 
+// Exact counts of n items into offs[0..n) then the in-place scan: offs[i] =
+// first output slot of item i, offs[n] = total.  ws: (tiles + 2) * 8 bytes
+// (look-back status, scan ticket, count group counter), zeroed here.
+template <class Maker>
+void launch_counts(Maker mk, uint32_t n, uint32_t* offs, void* ws, uint32_t* err, cudaStream_t st) {
+  const size_t tiles = ((size_t)n + kScanTile - 1) / kScanTile;
+  uint64_t* status = (uint64_t*)ws;
+  cudaMemsetAsync(status, 0, (tiles + 2) * 8, st);
+  uint32_t* ticket = (uint32_t*)(status + tiles + 1);
+  const int blocks = grid_for((n + 31) / 32, kUnitWarps, 148 * 7);
+  k_count_groups<<<blocks, kScanBlock, 0, st>>>(mk, n, offs, ticket + 1);
+  k_scan_inplace<<<(unsigned)tiles, kScanBlock, 0, st>>>(offs, n, LookbackState{status, ticket, err});
+}
+
 shn_status ensure(shn_grid* g, void** p, size_t* cap, size_t bytes, cudaStream_t st) {
   if (*cap >= bytes && *p) return SHN_OK;
   if (*p) dev_free(g->ctx, *p, *cap, st);
@@ -627,9 +653,8 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   uint32_t* offs = (uint32_t*)g->offs_tri.ptr;
   uint32_t P = 0;
   if (nt) {
-    LookbackState ls = scan_state(g, nt, st, &rc);
-    if (rc) return rc;
-    k_count_units<<<scan_tiles(nt), kScanBlock, 0, st>>>(TopMaker{tri, g->geom}, nt, ls, offs);
+    if ((rc = ensure_buf(g, g->scan, (((size_t)nt + kScanTile - 1) / kScanTile + 2) * 8, st))) return rc;
+    launch_counts(TopMaker{tri, g->geom}, nt, offs, g->scan.ptr, g->d_err, st);
     const uint32_t* src[1] = {offs + nt};
     if ((rc = read_words(g, src, 1, &P, st))) return rc;
   }
@@ -678,10 +703,8 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   if ((rc = ensure_buf(g, g->offs_pair, ((size_t)P + 1) * 4, st))) return rc;
   uint32_t* pairOffs = (uint32_t*)g->offs_pair.ptr;
   if (P) {
-    LookbackState ls = scan_state(g, P, st, &rc);
-    if (rc) return rc;
-    k_count_units<<<scan_tiles(P), kScanBlock, 0, st>>>(LeafMaker{tri, sortedTop, g->cells, g->geom}, P, ls,
-                                                       pairOffs);
+    if ((rc = ensure_buf(g, g->scan, (((size_t)P + kScanTile - 1) / kScanTile + 2) * 8, st))) return rc;
+    launch_counts(LeafMaker{tri, sortedTop, g->cells, g->geom}, P, pairOffs, g->scan.ptr, g->d_err, st);
   } else {
     cudaMemsetAsync(pairOffs, 0, 4, st);
   }
@@ -740,12 +763,8 @@ void launch_batch_count(const float4* tri, uint32_t T, const uint32_t* tri_off, 
     cudaMemsetAsync(offs, 0, 4, st);
     return;
   }
-  const size_t tiles = ((size_t)T + kScanTile - 1) / kScanTile;
-  uint64_t* status = (uint64_t*)scan_ws;
-  cudaMemsetAsync(status, 0, (tiles + 2) * 8, st);
-  LookbackState ls{status, (uint32_t*)(status + tiles + 1), err};
   const TriArr ts{tri};
-  k_count_units<<<(unsigned)tiles, kScanBlock, 0, st>>>(BatchMaker{ts, tri_off, scenes, ns}, T, ls, offs);
+  launch_counts(BatchMaker{ts, tri_off, scenes, ns}, T, offs, scan_ws, err, st);
 }
 
 void launch_batch_emit(const float4* tri, uint32_t T, const uint32_t* tri_off, const BatchScene* scenes,
