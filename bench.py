@@ -34,6 +34,11 @@ sys.path.insert(0, ROOT)
 METRIC = "Mrays/s"
 N_TRIS = 1 << 20
 AO_SPP, AO_LEN, AO_OFFSET, AO_SEED = 4, 0.1, 1e-4, 1
+# direct illumination (DirectIlluminationIntegrator::shade): 4 shadow rays per hit to a
+# 0.1 x 0.1 light 0.2 above the cluster, facing down
+DI_SPP, DI_SEED = 4, 1
+DI_LIGHT = dict(position=(-0.05, 0.2, -0.05), edge1=(0.1, 0.0, 0.0), edge2=(0.0, 0.0, 0.1),
+                normal=(0.0, -1.0, 0.0), intensity=(10.0, 10.0, 10.0))
 LAMBDA_TOP, LAMBDA_LEAF = 1.0 / 16.0, 4.0
 
 
@@ -47,8 +52,10 @@ def parse():
     ap.add_argument("--cpu-sample-stride", type=int, default=64)
     ap.add_argument("--case", default="full", choices=["full", "small"],
                     help="small: 480x270 camera, for profiler captures (not a bench line)")
-    ap.add_argument("--workload", default="cluster", choices=["cluster", "batch", "serve", "pathtrace"],
-                    help="cluster: the headline line; batch: 256-scene batched vs one launch per scene; "
+    ap.add_argument("--workload", default="cluster", choices=["cluster", "direct", "batch", "serve", "pathtrace"],
+                    help="cluster: the headline line; direct: the cluster frame shaded by an area light "
+                         "(4 shadow rays per hit) instead of ambient occlusion; "
+                         "batch: 256-scene batched vs one launch per scene; "
                          "serve: request stream with continuous batching vs one launch per request; "
                          "pathtrace: heightfield path tracer with compaction after every bounce")
     ap.add_argument("--scenes", type=int, default=256, help="batch workload: number of scenes")
@@ -57,13 +64,18 @@ def parse():
     return ap.parse_args()
 
 
-def workload_config(extra=None):
+def workload_config(extra=None, direct=False):
     c = {"workload": "two-level grid rebuild + 1920x1080 primary + 4 AO rays/hit",
          "scene": "cluster_in_field: 1,048,576 tris (90% in r=0.05 sphere, offsets 0.002; 10% in [-50,50]^3, offsets 0.5), seed 1",
          "grid": "two-level, lambda_top=1/16 (divisor 1, min res 2), lambda_leaf=4, leaf threshold 16",
          "camera": "eye (0,0,-0.25), +z, 45 deg vertical FOV, 1920x1080, 1 spp",
          "ao": "4 cosine rays per hit, length 0.1, origin offset 1e-4, Philox4x32-10 seed 1",
          "l2": "flushed between timed steps (256 MiB write, outside the timed region)"}
+    if direct:
+        c["workload"] = "two-level grid rebuild + 1920x1080 primary + 4 area-light shadow rays/hit + shading"
+        del c["ao"]
+        c["direct"] = ("4 shadow segments per hit to a uniform point of the 0.1x0.1 light at y=0.2 "
+                       "(normal -y, intensity 10), Philox4x32-10 seed 1; diffuse 0.7; frame + progressive final image")
     if extra:
         c.update(extra)
     return c
@@ -162,7 +174,7 @@ def profile_traffic():
 
 
 # ---------------------------------------------------------------------------
-def cpu_baseline(sc, cam, stride: int, use_reference_build: bool):
+def cpu_baseline(sc, cam, stride: int, use_reference_build: bool, direct: bool = False):
     """Oracle port (or reference build + port traversal) on a bounded sample, host cores."""
     import oracle
     from shinobi_b200 import scenes  # noqa: F401
@@ -182,8 +194,14 @@ def cpu_baseline(sc, cam, stride: int, use_reference_build: bool):
     sel = np.arange(0, org.shape[0], stride)
     t1 = time.perf_counter()
     tri, t, _, _, _ = oracle.trace_closest(g, org[sel], d[sel])
-    ro, rd, _ = oracle.ao_rays(sc.vertices, sc.indices, org[sel], d[sel], tri, t, AO_SPP, AO_SEED, AO_OFFSET)
-    oracle.trace_any(g, ro, rd, np.full(ro.shape[0], AO_LEN, np.float32))
+    if direct:
+        # timing only: the sample's rays are numbered by their position in the sample
+        ro, rd, _ = oracle.direct_rays(org[sel], d[sel], tri, t, DI_SPP, DI_SEED, 0, DI_LIGHT)
+        occ, _ = oracle.trace_any(g, ro, rd, np.full(ro.shape[0], 0.9999, np.float32))
+        oracle.shade_direct(sc.vertices, sc.indices, org[sel], d[sel], tri, t, DI_SPP, DI_SEED, 0, DI_LIGHT, occ)
+    else:
+        ro, rd, _ = oracle.ao_rays(sc.vertices, sc.indices, org[sel], d[sel], tri, t, AO_SPP, AO_SEED, AO_OFFSET)
+        oracle.trace_any(g, ro, rd, np.full(ro.shape[0], AO_LEN, np.float32))
     t_trace = time.perf_counter() - t1
     sample_rays = sel.size + ro.shape[0]
     # full-frame estimate: every pixel traced, AO rays in proportion to the sample's hit rate
@@ -193,7 +211,7 @@ def cpu_baseline(sc, cam, stride: int, use_reference_build: bool):
         "value": full_rays / full_time / 1e6, "unit": METRIC, "cores": threads,
         "kind": "reference" if use_reference_build else "port",
         "sample": (f"full grid build ({'reference TwoLevelGridBuilderHost::hostBuild, 1 thread' if use_reference_build else 'oracle two-level build, 1 thread'}, "
-                   f"{t_build:.2f} s) + every {stride}th pixel's primary ray and its AO rays "
+                   f"{t_build:.2f} s) + every {stride}th pixel's primary ray and its {'shadow rays and shading' if direct else 'AO rays'} "
                    f"({sample_rays} rays, {t_trace:.2f} s on {threads} threads), scaled to the full frame"),
         "build_ms_per_mtri": t_build * 1e3 / (sc.num_triangles / 1e6),
         "sample_seconds": t_build + t_trace,
@@ -209,12 +227,13 @@ def run_reference(args):
     cam = scenes.CAMERA_CLUSTER
     # per-step sample sized so the whole run stays within a few minutes
     stride = max(64, 32 * (args.steps + args.warmup))
+    direct = args.workload == "direct"
     for _ in range(args.warmup):
-        cpu_baseline(sc, cam, stride * 4, True)
+        cpu_baseline(sc, cam, stride * 4, True, direct=direct)
     vals, secs = [], 0.0
     last = None
     for _ in range(args.steps):
-        last = cpu_baseline(sc, cam, stride, True)
+        last = cpu_baseline(sc, cam, stride, True, direct=direct)
         vals.append(last["value"])
         secs += last["sample_seconds"]
     v = float(np.mean(vals))
@@ -222,7 +241,7 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Philox4x32-10 scene)",
-            "config": workload_config({"cpu_sample": last["sample"]}),
+            "config": workload_config({"cpu_sample": last["sample"]}, direct=direct),
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": last["cores"], "kind": "reference",
                              "sample": last["sample"]},
             "build_ms_per_mtri": last["build_ms_per_mtri"],
@@ -283,8 +302,17 @@ def run_shinobi(args):
                         lambda_leaf=LAMBDA_LEAF, leaf_threshold=16)
     g = shn.Grid(ctx)
     hits = shn.alloc_hits(npix)
-    ao = torch.empty(npix, dtype=torch.float32, device="cuda")
+    direct = args.workload == "direct"
+    ao = torch.empty(npix * (3 if direct else 1), dtype=torch.float32, device="cuda")
+    final = torch.zeros(npix * 3, dtype=torch.float32, device="cuda") if direct else None
+    dip = shn.di_params(light=DI_LIGHT, samples=DI_SPP, seed=DI_SEED) if direct else None
     nao = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def shade():
+        if direct:
+            g.shade_direct(cam, hits, dip, frame=ao, final=final, num_rays=nao)
+        else:
+            g.trace_ao(cam, hits, AO_SPP, AO_LEN, AO_OFFSET, AO_SEED, out=ao, num_rays=nao)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
@@ -296,7 +324,7 @@ def run_shinobi(args):
         e1.record()
         g.trace_primary(cam, out=hits)
         e2.record()
-        g.trace_ao(cam, hits, AO_SPP, AO_LEN, AO_OFFSET, AO_SEED, out=ao, num_rays=nao)
+        shade()
         e3.record()
         if times is not None:
             times.append((e0, e1, e2, e3))
@@ -332,7 +360,7 @@ def run_shinobi(args):
     hv = torch.from_numpy(sc.vertices).pin_memory()
     h_tri = torch.empty(npix, dtype=torch.int32).pin_memory()
     h_t = torch.empty(npix, dtype=torch.float32).pin_memory()
-    h_ao = torch.empty(npix, dtype=torch.float32).pin_memory()
+    h_ao = torch.empty(ao.numel(), dtype=torch.float32).pin_memory()
     vnp = hv.numpy()
 
     def e2e_step():
@@ -358,7 +386,7 @@ def run_shinobi(args):
     e2e_total = max_over_ranks(e2e_total, dist)
     e2e_value = replica_value(world, args.steps * rays_per_step, e2e_total)
     h2d = int(sc.vertices.nbytes)
-    d2h = int(npix * 12)
+    d2h = int(npix * 8 + ao.numel() * 4)
 
     # ---- roofline of the dominant kernel (work counters, untimed pass) ---------
     cnt = torch.zeros(2, dtype=torch.int64, device="cuda")
@@ -368,14 +396,15 @@ def run_shinobi(args):
     torch.cuda.synchronize()
     prim_steps, prim_tests = [int(x) for x in cnt.cpu().tolist()]
     cnt.zero_()
-    g.trace_ao(cam, hits, AO_SPP, AO_LEN, AO_OFFSET, AO_SEED, out=ao, num_rays=nao)
+    shade()
     torch.cuda.synchronize()
     ao_steps, ao_tests = [int(x) for x in cnt.cpu().tolist()]
     ctx.lib.shn_grid_set_stats(g.handle, None)
     fp32 = fp32_peak_tflops(torch)
     # dominant kernel: the longer of the two trace kernels
     if ao_ms >= prim_ms:
-        kname, kms, ksteps, ktests = "k_trace_ao<two-level>", ao_ms, ao_steps, ao_tests
+        kname = "k_trace_direct<two-level>" if direct else "k_trace_ao<two-level>"
+        kms, ksteps, ktests = ao_ms, ao_steps, ao_tests
     else:
         kname, kms, ksteps, ktests = "k_trace_camera<two-level>", prim_ms, prim_steps, prim_tests
     work = 10.0 * ksteps + 40.0 * ktests  # FP32 ops per launch (cell visit 10, triangle test 40)
@@ -400,9 +429,10 @@ def run_shinobi(args):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Philox4x32-10 scene, resident in HBM)",
-        "config": workload_config({"rays_per_step": rays_per_step, "parallelism": f"replicas x{world}"}),
+        "config": workload_config({"rays_per_step": rays_per_step, "parallelism": f"replicas x{world}"},
+                                  direct=direct),
         "build_ms_per_mtri": build_ms / (N_TRIS / 1e6),
-        "phase_ms": {"build": build_ms, "primary": prim_ms, "ao": ao_ms},
+        "phase_ms": {"build": build_ms, "primary": prim_ms, ("direct" if direct else "ao"): ao_ms},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {
             "bound": "fp32", "kernel": kname, "achieved": achieved, "peak": fp32, "unit": "TFLOP/s",
@@ -420,7 +450,7 @@ def run_shinobi(args):
     # kernels launched per step: build (uniform count+emit+sort+ranges, leaf stage) + primary + AO (compact, trace, finalize)
     line["gpu_launches"] = args.steps * launches_per_step(P, R, C0, L)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(sc, cam, args.cpu_sample_stride, False)
+        line["cpu_baseline"] = cpu_baseline(sc, cam, args.cpu_sample_stride, False, direct=direct)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -433,9 +463,9 @@ def launches_per_step(P, R, C0, L):
             return 0
         passes = (max(1, (cells - 1).bit_length()) + 7) // 8
         return 2 + passes
-    build = (1 + 1 + sort_launches(P, C0) + 1      # count-scan, emit, sort, top ranges
-             + 1 + 1 + 1 + sort_launches(R, L) + 1)  # leaf cells scan, leaf count scan, emit, sort, ranges
-    return build + 1 + 3                               # primary; AO compact + trace + finalize
+    build = (2 + 1 + sort_launches(P, C0) + 1      # count + scan, emit, sort, top ranges
+             + 1 + 2 + 1 + sort_launches(R, L) + 1)  # leaf cells scan, leaf count + scan, emit, sort, ranges
+    return build + 1 + 3                               # primary; compact + trace + finalize (AO or shading)
 
 
 def run_batch(args):

@@ -324,14 +324,35 @@ struct FrameBuffer {
   uint32_t resX = 0, resY = 0;
 };
 
-// Primary closest-hit rays, then ambient-occlusion any-hit rays per hit
-// pixel (the C1 shape of the reference's default integrator).
+// AreaLightSource (src/Primitive/LightSource.hpp:35-51): a parallelogram
+// position + a*edge1 + b*edge2, emitting towards -normal.
+struct AreaLightSource {
+  vec3f position{-0.05f, 0.2f, -0.05f}, normal{0.f, -1.f, 0.f}, intensity{10.f, 10.f, 10.f},
+      edge1{0.1f, 0.f, 0.f}, edge2{0.f, 0.f, 0.1f};
+};
+
+// MaterialContainer (src/Primitive/Material.h:36-46) with the per-face
+// material ids of FaceSoup::getMaterialId (src/Control/Structure/FaceSoup.h:165).
+// Device pointers owned by the caller; null diffuse = defaultDiffuse everywhere.
+struct MaterialContainer {
+  const float* diffuseDevice = nullptr;        // 4 floats per material (.w unused)
+  uint32_t numMaterials = 0;
+  const uint32_t* faceMaterialDevice = nullptr;  // per triangle; null = material 0
+  vec3f defaultDiffuse{0.7f, 0.7f, 0.7f};
+};
+
+// DirectIlluminationIntegrator: primary closest-hit rays, then
+// numOcclusionSamples shadow rays per hit pixel to the area light and the
+// per-pixel shading of computeDirectIllumination with the progressive blend
+// into the final image.  ambientOcclusion() is the C1 form: cosine-weighted
+// any-hit rays of occlusionLength, one visibility fraction per pixel.
 class DirectIlluminationIntegrator {
  public:
-  uint32_t numOcclusionSamples = 4;
+  uint32_t numOcclusionSamples = 4;  // NUMOCCLUSIONSAMPLES
+  uint32_t seed = 1;
+  AreaLightSource lightSource;
   float occlusionLength = 0.1f;
   float originOffset = 1e-4f;
-  uint32_t seed = 1;
 
   // tracePrimary: hits (device, resX*resY) for the camera.
   void tracePrimary(const GridBase& aGrid, const Camera& aCamera, shn_hits& oHits, int aImageId,
@@ -339,17 +360,45 @@ class DirectIlluminationIntegrator {
     check(shn_trace_primary(aGrid.handle(), &aCamera.params(), (uint32_t)aImageId, &oHits, aStream),
           "tracePrimary", aGrid.context().get());
   }
-  // shade: occlusion rays from the primary hits; oFrame = visible fraction.
-  void shade(const GridBase& aGrid, const Camera& aCamera, const shn_hits& aPrimary, FrameBuffer& oFrame,
-             cudaStream_t aStream = 0) {
-    check(shn_trace_ao(aGrid.handle(), &aCamera.params(), &aPrimary, numOcclusionSamples, occlusionLength,
-                       originOffset, seed, oFrame.deviceData, nullptr, aStream),
+  // shade: oFrameBuffer = this image's radiance (RGB per pixel); oFinalImage
+  // (may have null deviceData) = running mean over image ids 0..aImageId.
+  void shade(const GridBase& aGrid, const Camera& aCamera, const shn_hits& aPrimary,
+             const MaterialContainer& aMaterials, FrameBuffer& oFrameBuffer, FrameBuffer& oFinalImage,
+             int aImageId, cudaStream_t aStream = 0) {
+    shn_di_params p;
+    shn_di_params_default(&p);
+    const vec3f* lv[5] = {&lightSource.position, &lightSource.edge1, &lightSource.edge2, &lightSource.normal,
+                          &lightSource.intensity};
+    float* dst[5] = {p.light.position, p.light.edge1, p.light.edge2, p.light.normal, p.light.intensity};
+    for (int i = 0; i < 5; ++i) {
+      dst[i][0] = lv[i]->x;
+      dst[i][1] = lv[i]->y;
+      dst[i][2] = lv[i]->z;
+    }
+    p.samples = numOcclusionSamples;
+    p.seed = seed;
+    p.image_id = (uint32_t)aImageId;
+    p.tri_material = aMaterials.faceMaterialDevice;
+    p.diffuse = aMaterials.diffuseDevice;
+    p.num_materials = aMaterials.numMaterials;
+    p.default_diffuse[0] = aMaterials.defaultDiffuse.x;
+    p.default_diffuse[1] = aMaterials.defaultDiffuse.y;
+    p.default_diffuse[2] = aMaterials.defaultDiffuse.z;
+    check(shn_shade_direct(aGrid.handle(), &aCamera.params(), &aPrimary, &p, oFrameBuffer.deviceData,
+                           oFinalImage.deviceData, nullptr, aStream),
           "shade", aGrid.context().get());
   }
-  void integrate(const GridBase& aGrid, const Camera& aCamera, shn_hits& oHits, FrameBuffer& oFrame,
-                 int aImageId, cudaStream_t aStream = 0) {
+  void integrate(const GridBase& aGrid, const Camera& aCamera, shn_hits& oHits, const MaterialContainer& aMaterials,
+                 FrameBuffer& oFrameBuffer, FrameBuffer& oFinalImage, int aImageId, cudaStream_t aStream = 0) {
     tracePrimary(aGrid, aCamera, oHits, aImageId, aStream);
-    shade(aGrid, aCamera, oHits, oFrame, aStream);
+    shade(aGrid, aCamera, oHits, aMaterials, oFrameBuffer, oFinalImage, aImageId, aStream);
+  }
+  // ambientOcclusion: oFrame = visible fraction of the occlusion rays per pixel.
+  void ambientOcclusion(const GridBase& aGrid, const Camera& aCamera, const shn_hits& aPrimary, FrameBuffer& oFrame,
+                        cudaStream_t aStream = 0) {
+    check(shn_trace_ao(aGrid.handle(), &aCamera.params(), &aPrimary, numOcclusionSamples, occlusionLength,
+                       originOffset, seed, oFrame.deviceData, nullptr, aStream),
+          "ambientOcclusion", aGrid.context().get());
   }
   void cleanup() {}
 };
@@ -382,8 +431,9 @@ class StaticRTEngine {
   }
   void build() { mBuilder.build(*mGrid, *mStorage); }
   void renderImage(DirectIlluminationIntegrator& aIntegrator, const Camera& aCamera, shn_hits& oHits,
-                   FrameBuffer& oFrame, int aImageId, cudaStream_t aStream = 0) {
-    aIntegrator.integrate(*mGrid, aCamera, oHits, oFrame, aImageId, aStream);
+                   const MaterialContainer& aMaterials, FrameBuffer& oFrameBuffer, FrameBuffer& oFinalImage,
+                   int aImageId, cudaStream_t aStream = 0) {
+    aIntegrator.integrate(*mGrid, aCamera, oHits, aMaterials, oFrameBuffer, oFinalImage, aImageId, aStream);
   }
   Builder& builder() { return mBuilder; }
   Grid& grid() { return *mGrid; }

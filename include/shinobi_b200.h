@@ -31,7 +31,8 @@
  *       src/Control/Algorithm/TwoLevelGridTraverser.h:677-828)
  *  - trace<RegularPrimaryRayGenerator,...>          -> shn_trace_primary
  *      (src/Engine/RayTracingKernels.h:37-136, src/Engine/RayGenerators.h:36-61)
- *  - DirectIlluminationIntegrator::shade occlusion  -> shn_trace_ao
+ *  - DirectIlluminationIntegrator::shade occlusion  -> shn_trace_ao (ambient occlusion)
+ *    and shn_shade_direct (area light + computeDirectIllumination)
  *      (src/Integrator/DirectIlluminationIntegrator.h:254-315)
  *  - SimplePathTracer / render megakernel           -> shn_pt_render
  *      (src/Integrator/SimplePathTracer.hpp:65-241, src/Shinobi.h:152-230)
@@ -190,6 +191,49 @@ shn_status shn_trace_primary(const shn_grid* g, const shn_camera* cam, uint32_t 
 shn_status shn_trace_ao(const shn_grid* g, const shn_camera* cam, const shn_hits* primary,
                         uint32_t spp, float length, float offset, uint32_t seed, float* d_ao,
                         uint32_t* d_num_rays, void* stream);
+
+/* Direct illumination from one parallelogram light (DirectIlluminationIntegrator::shade
+ * and computeDirectIllumination, src/Integrator/DirectIlluminationIntegrator.h:46-168,
+ * src/Integrator/DirectIlluminationIntegrator.h:254-338; AreaLightSource,
+ * src/Primitive/LightSource.hpp:35-51; MaterialContainer, src/Primitive/Material.h:36-46).
+ * Per primary hit pixel p and sample s < samples:
+ *   origin  = eye + (t - 1e-5) * d          (SimpleRayBuffer::store, src/Engine/RayBuffers.h:52-55)
+ *   L       = position + r1 * edge1 + r2 * edge2 - origin, (r1, r2) from the
+ *             Philox4x32-10 counter (p, s, image_id, 0x444C) keyed by seed
+ *   any-hit shadow segment with t in (1e-5, 0.9999)   (OcclusionRayBuffer::store, src/Engine/RayBuffers.h:156-168)
+ *   value_s = 0 if blocked, else intensity * |edge1 x edge2| * diffuse(material(tri))
+ *             * max(0, -normal_light . L^) * max(0, n . L^) / (L . L), n the
+ *             unflipped geometric normal of the hit triangle;
+ * pixels without a hit take `background` for every sample.
+ * frame[p] = sum_s value_s / samples (RGB, 3 floats per pixel), and
+ * final[p] = final[p] * (1 - w) + frame[p] * w with w = 1 / (image_id + 1).
+ * tri_material (per scene triangle) may be NULL: material 0 everywhere; diffuse
+ * (4 floats per material, .w unused) may be NULL: default_diffuse everywhere.
+ * Material ids >= num_materials read material 0.  d_final may be NULL.
+ * If d_num_rays != NULL it receives the number of shadow rays traced (device). */
+typedef struct shn_area_light {
+  float position[3];   /* corner */
+  float edge1[3], edge2[3];
+  float normal[3];     /* the light emits towards -normal */
+  float intensity[3];
+} shn_area_light;
+
+typedef struct shn_di_params {
+  shn_area_light light;
+  uint32_t samples;              /* shadow rays per pixel (NUMOCCLUSIONSAMPLES = 4) */
+  uint32_t seed;
+  uint32_t image_id;             /* progressive accumulation index */
+  const uint32_t* tri_material;  /* device, per scene triangle, or NULL */
+  const float* diffuse;          /* device, 4 floats per material, or NULL */
+  uint32_t num_materials;
+  float default_diffuse[3];
+  float background[3];           /* BACKGROUND_R/G/B, src/CUDAConfig.h:57-59 */
+} shn_di_params;
+
+void shn_di_params_default(shn_di_params* p);
+shn_status shn_shade_direct(const shn_grid* g, const shn_camera* cam, const shn_hits* primary,
+                            const shn_di_params* p, float* d_frame, float* d_final,
+                            uint32_t* d_num_rays, void* stream);
 
 /* Work counters: when d_counters (2 x uint64, device) is non-NULL, later
  * trace calls on this grid run counting variants of their kernels and add

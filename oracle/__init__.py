@@ -77,6 +77,9 @@ def lib():
         L.orc_primary_rays.argtypes = [vp, u32, u32, u32, vp, vp, vp]
         L.orc_ao_rays.argtypes = [vp, vp] + [vp] * 8 + [u32, u32, u32, f32] + [vp] * 7
         L.orc_ao_rays.restype = u32
+        L.orc_direct_rays.argtypes = [vp] * 8 + [u32, u32, u32, u32, vp] + [vp] * 7
+        L.orc_direct_rays.restype = u32
+        L.orc_shade_direct.argtypes = [vp] * 10 + [u32, u32, u32, u32] + [vp] * 3 + [u32] + [vp] * 5
         L.orc_pt_render.argtypes = [vp, vp, vp, u32, u32, u32, u32, u32, f32, vp, vp, vp, vp, vp, f32, u32, vp]
         L.orc_compact.argtypes = [vp, u32, vp]
         L.orc_compact.restype = u32
@@ -297,6 +300,43 @@ def ao_rays(vtx, idx, org, dirs, tri, t, spp: int, seed: int, offset: float):
     ro = np.stack(outs[0:3], axis=1)
     rd = np.stack(outs[3:6], axis=1)
     return ro, rd, outs[6]
+
+
+def _light15(light) -> np.ndarray:
+    return np.concatenate([_f32(light[k]) for k in ("position", "edge1", "edge2", "normal", "intensity")])
+
+
+def direct_rays(org, dirs, tri, t, spp: int, seed: int, image_id: int, light):
+    """Shadow segments of the hit pixels; returns (org, dir, pixel) in pixel-major order."""
+    org, dirs, tri, t = _f32(org), _f32(dirs), _u32(tri), _f32(t)
+    n = org.shape[0]
+    m_max = int(np.count_nonzero(tri != MISS)) * spp
+    outs = [np.zeros(m_max, np.float32) for _ in range(6)] + [np.zeros(m_max, np.uint32)]
+    cols = [np.ascontiguousarray(org[:, k]) for k in range(3)] + [np.ascontiguousarray(dirs[:, k]) for k in range(3)]
+    m = lib().orc_direct_rays(*[_p(c) for c in cols], _p(tri), _p(t), n, spp, seed, image_id,
+                              _p(_light15(light)), *[_p(o) for o in outs])
+    assert m == m_max
+    return np.stack(outs[0:3], axis=1), np.stack(outs[3:6], axis=1), outs[6]
+
+
+def shade_direct(vtx, idx, org, dirs, tri, t, spp, seed, image_id, light, occ, tri_material=None,
+                 diffuse=None, default_diffuse=(0.7, 0.7, 0.7), background=(0.15, 0.2, 0.3), final=None):
+    """(frame (n,3), final (n,3) or None) with the semantics of shn_shade_direct;
+    occ = blocked flags of direct_rays' segments, in its order."""
+    vtx, idx, org, dirs, tri, t = _f32(vtx), _u32(idx), _f32(org), _f32(dirs), _u32(tri), _f32(t)
+    n = org.shape[0]
+    cols = [np.ascontiguousarray(org[:, k]) for k in range(3)] + [np.ascontiguousarray(dirs[:, k]) for k in range(3)]
+    occ = np.ascontiguousarray(occ, dtype=np.uint8)
+    tm = _u32(tri_material) if tri_material is not None else None
+    df = _f32(diffuse).reshape(-1) if diffuse is not None else None
+    nmat = df.size // 4 if df is not None else 0
+    frame = np.zeros(3 * n, np.float32)
+    fin = _f32(final).reshape(-1).copy() if final is not None else None
+    lib().orc_shade_direct(_p(vtx), _p(idx), *[_p(c) for c in cols], _p(tri), _p(t), n, spp, seed, image_id,
+                           _p(_light15(light)), _p(tm) if tm is not None else None,
+                           _p(df) if df is not None else None, nmat, _p(_f32(default_diffuse)),
+                           _p(_f32(background)), _p(occ), _p(frame), _p(fin) if fin is not None else None)
+    return frame.reshape(n, 3), (fin.reshape(n, 3) if fin is not None else None)
 
 
 def pt_render(g: Grid, cam, spp, max_depth, rr_depth, albedo, light_pos, light_e1, light_e2,

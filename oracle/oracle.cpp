@@ -910,6 +910,107 @@ uint32_t orc_ao_rays(const float* vtx, const uint32_t* idx, const float* ox, con
   return m;
 }
 
+// Direct illumination from a parallelogram light (DirectIlluminationIntegrator::shade,
+// src/Integrator/DirectIlluminationIntegrator.h:254-315).  light15 = position,
+// edge1, edge2, normal, intensity.  Shadow segment of sample s of hit pixel p:
+// origin = o + (t - 1e-5) d, the stored hit point of SimpleRayBuffer::store
+// (src/Engine/RayBuffers.h:52-55); direction = a uniform point of the light
+// (AreaLightSource::getPoint, src/Primitive/LightSource.hpp:40-43) minus the
+// origin, its (r1, r2) from Philox4x32-10 with counter (p, s, image_id, 0x444C)
+// and key (seed, 0) in place of AreaLightShadowRayGenerator's KISS generator
+// (src/Engine/RayGenerators.h:106-139).  The segment is blocked by a hit with
+// t in (1e-5, 0.9999) (OcclusionRayBuffer::store, src/Engine/RayBuffers.h:156-168).
+static void di_segment(V3 org, V3 d, float t, const float* light15, uint32_t p, uint32_t s,
+                       uint32_t image_id, uint32_t seed, V3& o, V3& L) {
+  const V3 LP = mk(light15[0], light15[1], light15[2]), E1 = mk(light15[3], light15[4], light15[5]),
+           E2 = mk(light15[6], light15[7], light15[8]);
+  o = add(org, muls(d, t - 1e-5f));
+  uint32_t c[4] = {p, s, image_id, 0x444Cu};
+  philox(c, seed, 0u);
+  const V3 lp = add(add(LP, muls(E1, u01(c[0]))), muls(E2, u01(c[1])));
+  L = sub(lp, o);
+}
+
+// Shadow segments of every hit pixel, pixel-major over hit pixels, spp per
+// pixel; returns the number written.
+uint32_t orc_direct_rays(const float* ox, const float* oy, const float* oz, const float* dx,
+                         const float* dy, const float* dz, const uint32_t* tri, const float* t,
+                         uint32_t n, uint32_t spp, uint32_t seed, uint32_t image_id,
+                         const float* light15, float* rox, float* roy, float* roz, float* rdx,
+                         float* rdy, float* rdz, uint32_t* rpix) {
+  uint32_t m = 0;
+  for (uint32_t p = 0; p < n; ++p) {
+    if (tri[p] == kMiss) continue;
+    for (uint32_t s = 0; s < spp; ++s) {
+      V3 o, L;
+      di_segment(mk(ox[p], oy[p], oz[p]), mk(dx[p], dy[p], dz[p]), t[p], light15, p, s, image_id, seed, o, L);
+      rox[m] = o.x; roy[m] = o.y; roz[m] = o.z;
+      rdx[m] = L.x; rdy[m] = L.y; rdz[m] = L.z;
+      rpix[m] = p;
+      ++m;
+    }
+  }
+  return m;
+}
+
+// computeDirectIllumination (src/Integrator/DirectIlluminationIntegrator.h:46-168):
+// per unblocked sample intensity * area * diffuse * max(0, -n_light . L^) *
+// max(0, n . L^) / (L . L) with n the unflipped geometric normal, summed as
+// value / spp in sample order; pixels without a hit sum background / spp.
+// occ holds the blocked flags of orc_direct_rays' segments in its order.  The
+// final image blends with weight 1 / (image_id + 1).  Material ids >=
+// num_materials read material 0; diffuse == nullptr means ddef everywhere.
+void orc_shade_direct(const float* vtx, const uint32_t* idx, const float* ox, const float* oy,
+                      const float* oz, const float* dx, const float* dy, const float* dz,
+                      const uint32_t* tri, const float* t, uint32_t n, uint32_t spp, uint32_t seed,
+                      uint32_t image_id, const float* light15, const uint32_t* tri_mat,
+                      const float* diffuse, uint32_t nmat, const float* ddef, const float* bg,
+                      const uint8_t* occ, float* frame, float* fin) {
+  const V3 E1 = mk(light15[3], light15[4], light15[5]), E2 = mk(light15[6], light15[7], light15[8]);
+  const V3 LN = mk(light15[9], light15[10], light15[11]), LI = mk(light15[12], light15[13], light15[14]);
+  const V3 lc = cross(E1, E2);
+  const float larea = sqrtf(dot(lc, lc));
+  const V3 BG = mk(bg[0], bg[1], bg[2]);
+  const float inv_s = 1.0f / (float)spp;
+  uint32_t k = 0;
+  for (uint32_t p = 0; p < n; ++p) {
+    V3 rad = mk(0.f, 0.f, 0.f);
+    if (tri[p] == kMiss) {
+      for (uint32_t s = 0; s < spp; ++s) rad = add(rad, muls(BG, inv_s));
+    } else {
+      const Tri tr = load_tri(vtx, idx, tri[p]);
+      const V3 nrm = normalize(cross(sub(tr.v[1], tr.v[0]), sub(tr.v[2], tr.v[0])));
+      V3 diff = mk(ddef[0], ddef[1], ddef[2]);
+      if (diffuse) {
+        uint32_t m = tri_mat ? tri_mat[tri[p]] : 0u;
+        if (m >= nmat) m = 0u;
+        diff = mk(diffuse[4 * m], diffuse[4 * m + 1], diffuse[4 * m + 2]);
+      }
+      const V3 kk = mul(muls(LI, larea), diff);
+      for (uint32_t s = 0; s < spp; ++s, ++k) {
+        if (occ[k]) continue;
+        V3 o, L;
+        di_segment(mk(ox[p], oy[p], oz[p]), mk(dx[p], dy[p], dz[p]), t[p], light15, p, s, image_id, seed, o, L);
+        const V3 ln = normalize(L);
+        const float att = 1.0f / dot(L, L);
+        const float a = fmaxf(0.f, -dot(LN, ln));
+        const float b = fmaxf(0.f, dot(nrm, ln));
+        rad = add(rad, muls(muls(muls(muls(kk, a), b), att), inv_s));
+      }
+    }
+    frame[3 * p] = rad.x;
+    frame[3 * p + 1] = rad.y;
+    frame[3 * p + 2] = rad.z;
+    if (fin) {
+      const float wn = 1.0f / (float)(image_id + 1u);
+      const float wo = 1.0f - wn;
+      fin[3 * p] = fin[3 * p] * wo + rad.x * wn;
+      fin[3 * p + 1] = fin[3 * p + 1] * wo + rad.y * wn;
+      fin[3 * p + 2] = fin[3 * p + 2] * wo + rad.z * wn;
+    }
+  }
+}
+
 // Path tracer, path by path (the CUDA side runs it as a wavefront with
 // compaction; results are per path and independent of the schedule).
 // Semantics: SimplePathTracer (src/Integrator/SimplePathTracer.hpp:65-241)

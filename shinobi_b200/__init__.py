@@ -9,7 +9,7 @@ goes to the CUDA library and raises ``ShinobiError`` on failure.
 Names follow the reference's operator surface: a ``FaceSoup`` holds the
 triangles (FaceSoup<frame>), ``Grid.build`` plays FastSimpleGridBuilder /
 FastTwoLevelGridBuilder, ``Grid.trace_*`` play the grid traversers with the
-intersector, and ``Grid.trace_primary`` / ``Grid.trace_ao`` the ray
+intersector, and ``Grid.trace_primary`` / ``Grid.trace_ao`` / ``Grid.shade_direct`` the ray
 generators with the trace<> kernel.
 """
 from __future__ import annotations
@@ -180,6 +180,33 @@ def pt_params(**kw) -> _abi.PtParams:
     return p
 
 
+def di_params(light=None, tri_material=None, diffuse=None, **kw) -> _abi.DiParams:
+    """Direct-illumination parameters (defaults: 4 shadow rays per pixel, seed 1,
+    a 0.1 x 0.1 light facing down at y = 0.2, diffuse 0.7, the reference's
+    background).  ``light`` is a dict of AreaLight fields; ``tri_material``
+    (uint32 per triangle) and ``diffuse`` ((num_materials, 4) float32) are
+    device tensors that must stay alive until the call's work has run."""
+    p = _abi.DiParams()
+    _abi.load().shn_di_params_default(C.byref(p))
+    for k, v in (light or {}).items():
+        arr = getattr(p.light, k)
+        for i, x in enumerate(v):
+            arr[i] = x
+    if tri_material is not None:
+        p.tri_material = _ptr(tri_material)
+    if diffuse is not None:
+        p.diffuse = _ptr(diffuse)
+        p.num_materials = int(diffuse.shape[0])
+    for k, v in kw.items():
+        if isinstance(v, (tuple, list)):
+            arr = getattr(p, k)
+            for i, x in enumerate(v):
+                arr[i] = x
+        else:
+            setattr(p, k, v)
+    return p
+
+
 def camera_struct(cam) -> _abi.Camera:
     c = _abi.Camera()
     for k in range(3):
@@ -290,6 +317,22 @@ class Grid:
                                                  offset, seed, _ptr(out), _ptr(num_rays),
                                                  _stream(stream)), "shn_trace_ao")
         return out
+
+    def shade_direct(self, cam, primary: HitBuffers, params=None, frame=None, final=None, num_rays=None,
+                     stream=None):
+        """Area-light direct illumination of the primary hits; returns the
+        (res_y, res_x, 3) frame (device).  ``final``, when given, receives the
+        progressive blend with weight 1 / (image_id + 1)."""
+        torch = _torch()
+        p = params or di_params()
+        frame = frame if frame is not None else torch.empty(cam.res_y, cam.res_x, 3, dtype=torch.float32,
+                                                            device="cuda")
+        c = camera_struct(cam)
+        h = primary.struct()
+        self.ctx.check(self.ctx.lib.shn_shade_direct(self.handle, C.byref(c), C.byref(h), C.byref(p),
+                                                     _ptr(frame), _ptr(final), _ptr(num_rays),
+                                                     _stream(stream)), "shn_shade_direct")
+        return frame
 
     def pt_render(self, scene: FaceSoup, cam, params=None, out=None, stats=None, stream=None):
         """Wavefront path tracer; returns the (res_y, res_x, 3) mean-radiance image (device)."""

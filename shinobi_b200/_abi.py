@@ -57,6 +57,17 @@ class PtParams(C.Structure):
                 ("light_radiance", f32 * 3), ("background", f32 * 3), ("offset", f32), ("seed", u32)]
 
 
+class AreaLight(C.Structure):
+    _fields_ = [("position", f32 * 3), ("edge1", f32 * 3), ("edge2", f32 * 3), ("normal", f32 * 3),
+                ("intensity", f32 * 3)]
+
+
+class DiParams(C.Structure):
+    _fields_ = [("light", AreaLight), ("samples", u32), ("seed", u32), ("image_id", u32),
+                ("tri_material", vp), ("diffuse", vp), ("num_materials", u32),
+                ("default_diffuse", f32 * 3), ("background", f32 * 3)]
+
+
 class ServerConfig(C.Structure):
     _fields_ = [("num_slots", u32), ("max_batch_rays", u32), ("max_requests_per_launch", u32),
                 ("max_queue", u32), ("coalesce", u32)]
@@ -127,6 +138,8 @@ SIGNATURES = {
     "shn_server_get_stats": ([vp, C.POINTER(ServerStats), i32], i32),
     "shn_server_run_schedule": ([vp, u32, vp, vp, vp], i32),
     "shn_server_destroy": ([vp], None),
+    "shn_di_params_default": ([C.POINTER(DiParams)], None),
+    "shn_shade_direct": ([vp, C.POINTER(Camera), C.POINTER(Hits), C.POINTER(DiParams), vp, vp, vp, vp], i32),
     "shn_pt_params_default": ([C.POINTER(PtParams)], None),
     "shn_pt_render": ([vp, vp, C.POINTER(Camera), C.POINTER(PtParams), vp, vp, vp], i32),
     "shn_exclusive_scan_u32": ([vp, vp, vp, u32, vp], i32),

@@ -3,7 +3,8 @@
 // batches per warp, src/Engine/RayTracingKernels.h:60-100) and traces them to
 // completion.  Variants: SoA rays (closest / any), in-kernel camera rays
 // (RegularPrimaryRayGenerator) and in-kernel ambient-occlusion rays
-// generated from compacted primary hits.
+// generated from compacted primary hits, and the shadow segments of direct
+// illumination from an area light with their per-pixel shading.
 #include "internal.h"
 #include "trace.cuh"
 #include "trace_coop.cuh"
@@ -172,6 +173,110 @@ __global__ void k_ao_finalize(const uint32_t* __restrict__ ptri, const uint32_t*
   uint32_t c = 0;
   for (uint32_t s = 0; s < spp; ++s) c += occ[b + s];
   ao[p] = 1.0f - (float)c / (float)spp;
+}
+
+// Direct illumination from a parallelogram light (DirectIlluminationIntegrator::shade,
+// src/Integrator/DirectIlluminationIntegrator.h:254-315, and computeDirectIllumination,
+// src/Integrator/DirectIlluminationIntegrator.h:46-168).
+struct DiParams {
+  CamView cam;
+  V3 lpos, le1, le2, lnrm, lint, ddef, bg;
+  float larea;
+  uint32_t spp, seed, image_id, nmat;
+  const float4* stri;        // scene triangles, 48-byte records (v0, v1, v2)
+  const uint32_t* tri_mat;   // per scene triangle, or null
+  const float4* diffuse;     // per material, or null
+};
+
+// Shadow segment of sample s of hit pixel p: the origin is the stored hit point
+// eye + (t - EPS) d (SimpleRayBuffer::store, src/Engine/RayBuffers.h:52-55), the
+// direction runs to a uniform point of the light (AreaLightShadowRayGenerator,
+// src/Engine/RayGenerators.h:106-139; AreaLightSource::getPoint,
+// src/Primitive/LightSource.hpp:40-43); Philox replaces the KISS generator.
+SHN_D void di_segment(const DiParams& P, uint32_t p, uint32_t s, float t, V3& o, V3& L) {
+  const V3 d = primary_dir(P.cam, p, P.image_id);
+  o = add(P.cam.eye, muls(d, t - 1e-5f));
+  const uint4 w = philox4x32(make_uint4(p, s, P.image_id, 0x444Cu), P.seed, 0u);
+  const V3 lp = add(add(P.lpos, muls(P.le1, u01(w.x))), muls(P.le2, u01(w.y)));
+  L = sub(lp, o);
+}
+
+template <int KIND, bool STATS>
+__global__ void __launch_bounds__(kTraceBlock, 9) k_trace_direct(GridView G, DiParams P,
+                                                              const float* __restrict__ pt,
+                                                              const uint32_t* __restrict__ hit_idx,
+                                                              const uint32_t* d_m, uint32_t* counter,
+                                                              uint8_t* __restrict__ occ,
+                                                              unsigned long long* stats,
+                                                              uint32_t* err) {
+  const uint32_t n = (*d_m) * P.spp;
+  warp_trace<KIND, true>(
+      G, n, counter,
+      [&](uint32_t r, V3& o, V3& dir, float& tmax) {
+        const uint32_t k = r / P.spp, s = r - k * P.spp;
+        const uint32_t p = hit_idx[k];
+        di_segment(P, p, s, pt[p], o, dir);
+        tmax = 0.9999f;
+      },
+      [&](uint32_t r, const Hit& h, uint32_t steps, uint32_t tests) {
+        occ[r] = h.tri != kMiss ? 1 : 0;
+        add_counts<STATS>(stats, steps, tests);
+      });
+}
+
+// Per pixel: the mean over samples of the light's contribution
+// (computeDirectIllumination, src/Integrator/DirectIlluminationIntegrator.h:97-159),
+// then the progressive blend into the final image.
+__global__ void __launch_bounds__(256) k_shade_direct(DiParams P, const uint32_t* __restrict__ ptri,
+                                                      const float* __restrict__ pt,
+                                                      const uint32_t* __restrict__ pos,
+                                                      const uint8_t* __restrict__ occ, uint32_t n,
+                                                      const uint32_t* d_m, float* __restrict__ frame,
+                                                      float* __restrict__ fin, uint32_t* d_num_rays) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p == 0 && d_num_rays) *d_num_rays = (*d_m) * P.spp;
+  if (p >= n) return;
+  const float inv_s = 1.0f / (float)P.spp;
+  const uint32_t tri = ptri[p];
+  V3 rad = mk(0.f, 0.f, 0.f);
+  if (tri == kMiss) {
+    for (uint32_t s = 0; s < P.spp; ++s) rad = add(rad, muls(P.bg, inv_s));
+  } else {
+    const float t = pt[p];
+    const float4* rec = P.stri + 3 * (size_t)tri;
+    const V3 v0 = f4v(__ldg(rec));
+    const V3 nrm = normalize(cross(sub(f4v(__ldg(rec + 1)), v0), sub(f4v(__ldg(rec + 2)), v0)));
+    V3 diff = P.ddef;
+    if (P.diffuse) {
+      uint32_t m = P.tri_mat ? __ldg(P.tri_mat + tri) : 0u;
+      if (m >= P.nmat) m = 0u;
+      diff = f4v(__ldg(P.diffuse + m));
+    }
+    const V3 k = mul(muls(P.lint, P.larea), diff);
+    const uint8_t* oc = occ + (size_t)pos[p] * P.spp;
+    for (uint32_t s = 0; s < P.spp; ++s) {
+      if (oc[s]) continue;
+      V3 o, L;
+      di_segment(P, p, s, t, o, L);
+      const V3 ln = normalize(L);
+      const float att = 1.0f / dot(L, L);
+      const float a = fmaxf(0.f, -dot(P.lnrm, ln));
+      const float b = fmaxf(0.f, dot(nrm, ln));
+      rad = add(rad, muls(muls(muls(muls(k, a), b), att), inv_s));
+    }
+  }
+  float* f = frame + 3 * (size_t)p;
+  f[0] = rad.x;
+  f[1] = rad.y;
+  f[2] = rad.z;
+  if (fin) {
+    const float wn = 1.0f / (float)(P.image_id + 1u);
+    const float wo = 1.0f - wn;
+    float* g = fin + 3 * (size_t)p;
+    g[0] = g[0] * wo + rad.x * wn;
+    g[1] = g[1] * wo + rad.y * wn;
+    g[2] = g[2] * wo + rad.z * wn;
+  }
 }
 
 template <class K>
@@ -395,6 +500,89 @@ shn_status shn_trace_ao(const shn_grid* g, const shn_camera* cam, const shn_hits
 #undef SHN_LAUNCH_AO
   k_ao_finalize<<<(n + 255) / 256, 256, 0, st>>>(primary->tri, pos, occ, n, spp, d_m, d_ao, d_num_rays);
   return check_launch(g->ctx, "trace_ao");
+}
+
+void shn_di_params_default(shn_di_params* p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  const float pos[3] = {-0.05f, 0.2f, -0.05f}, e1[3] = {0.1f, 0.f, 0.f}, e2[3] = {0.f, 0.f, 0.1f},
+              nrm[3] = {0.f, -1.f, 0.f}, inten[3] = {10.f, 10.f, 10.f};
+  memcpy(p->light.position, pos, 12);
+  memcpy(p->light.edge1, e1, 12);
+  memcpy(p->light.edge2, e2, 12);
+  memcpy(p->light.normal, nrm, 12);
+  memcpy(p->light.intensity, inten, 12);
+  p->samples = 4;
+  p->seed = 1;
+  for (int i = 0; i < 3; ++i) p->default_diffuse[i] = 0.7f;
+  p->background[0] = 0.15f;
+  p->background[1] = 0.2f;
+  p->background[2] = 0.3f;
+}
+
+shn_status shn_shade_direct(const shn_grid* g, const shn_camera* cam, const shn_hits* primary,
+                            const shn_di_params* prm, float* d_frame, float* d_final,
+                            uint32_t* d_num_rays, void* stream) {
+  if (!g || !cam || !primary || !primary->tri || !primary->t || !prm || !d_frame || prm->samples == 0)
+    return SHN_ERR_INVALID;
+  if (!g->built) return set_error(g->ctx, SHN_ERR_NOT_BUILT, "grid not built");
+  if (!g->src_tri) return set_error(g->ctx, SHN_ERR_INVALID, "grid has no scene");
+  if (prm->diffuse && prm->num_materials == 0)
+    return set_error(g->ctx, SHN_ERR_INVALID, "diffuse table without materials");
+  const uint64_t n64 = (uint64_t)cam->res_x * cam->res_y;
+  if (n64 == 0) return SHN_OK;
+  if (n64 > (1u << 24) || n64 * prm->samples >= (1ull << 32))
+    return set_error(g->ctx, SHN_ERR_INVALID, "too many shadow rays");
+  const uint32_t n = (uint32_t)n64;
+  cudaStream_t st = (cudaStream_t)stream;
+  Scratch S{g->ctx, st};
+  uint32_t* counter = S.get<uint32_t>(4);
+  uint32_t* hit_idx = S.get<uint32_t>(n);
+  uint32_t* pos = S.get<uint32_t>(n);
+  uint8_t* occ = S.get<uint8_t>((size_t)n * prm->samples);
+  const size_t tiles = (n + 2047) / 2048;
+  uint64_t* status = S.get<uint64_t>(tiles + 2);
+  if (S.err != cudaSuccess) return set_error(g->ctx, SHN_ERR_OOM, "direct-illumination scratch");
+  cudaMemsetAsync(counter, 0, 16, st);
+  cudaMemsetAsync(status, 0, (tiles + 2) * 8, st);
+  LookbackState ls{status, (uint32_t*)(status + tiles + 1), g->d_err};
+  uint32_t* d_m = counter + 1;
+  k_compact_hits<<<(unsigned)tiles, 256, 0, st>>>(primary->tri, n, hit_idx, pos, d_m, ls);
+  const GridView G = view_of(g);
+  const shn_area_light& l = prm->light;
+  DiParams P;
+  P.cam = make_camera(cam);
+  P.lpos = mk(l.position[0], l.position[1], l.position[2]);
+  P.le1 = mk(l.edge1[0], l.edge1[1], l.edge1[2]);
+  P.le2 = mk(l.edge2[0], l.edge2[1], l.edge2[2]);
+  P.lnrm = mk(l.normal[0], l.normal[1], l.normal[2]);
+  P.lint = mk(l.intensity[0], l.intensity[1], l.intensity[2]);
+  const V3 ln = cross(P.le1, P.le2);
+  P.larea = sqrtf(dot(ln, ln));  // AreaLightSource::getArea, src/Primitive/LightSource.hpp:45-48
+  P.ddef = mk(prm->default_diffuse[0], prm->default_diffuse[1], prm->default_diffuse[2]);
+  P.bg = mk(prm->background[0], prm->background[1], prm->background[2]);
+  P.spp = prm->samples;
+  P.seed = prm->seed;
+  P.image_id = prm->image_id;
+  P.nmat = prm->num_materials;
+  P.stri = g->src_tri;
+  P.tri_mat = prm->tri_material;
+  P.diffuse = (const float4*)prm->diffuse;
+#define SHN_LAUNCH_DI(K, S)                                                                          \
+  {                                                                                                  \
+    static int blocks = persistent_blocks(k_trace_direct<K, S>, g->ctx->num_sms);                    \
+    k_trace_direct<K, S><<<blocks, kTraceBlock, 0, st>>>(G, P, primary->t, hit_idx, d_m, counter,   \
+                                                       occ, g->stats, g->d_err);                     \
+  }
+  if (g->kind == SHN_GRID_UNIFORM) {
+    if (g->stats) SHN_LAUNCH_DI(0, true) else SHN_LAUNCH_DI(0, false)
+  } else {
+    if (g->stats) SHN_LAUNCH_DI(1, true) else SHN_LAUNCH_DI(1, false)
+  }
+#undef SHN_LAUNCH_DI
+  k_shade_direct<<<(n + 255) / 256, 256, 0, st>>>(P, primary->tri, primary->t, pos, occ, n, d_m, d_frame,
+                                                  d_final, d_num_rays);
+  return check_launch(g->ctx, "shade_direct");
 }
 
 }  // extern "C"

@@ -1,10 +1,11 @@
 // Drives the C++ adapters (include/shinobi/shinobi.hpp) the way an engine
 // written against the reference's host interface would: FWObject ->
-// FaceSoup::upload -> Fast*GridBuilder::init/build -> DirectIllumination
-// Integrator::tracePrimary.  Usage:
+// FaceSoup::upload -> Fast*GridBuilder::init/build -> StaticRTEngine::renderImage
+// (DirectIlluminationIntegrator::tracePrimary + shade).  Usage:
 //   adapter_example <scene.bin> <out.bin> <kind 0|1> <res_x> <res_y>
 // scene.bin: uint32 nv, uint32 nt, nv*3 float, nt*3 uint32.
-// out.bin:   res_x*res_y uint32 triangle ids, then res_x*res_y float t.
+// out.bin:   res_x*res_y uint32 triangle ids, res_x*res_y float t, then the
+//            res_x*res_y*3 float direct-illumination frame.
 // Exit code 3 (after printing "no device") when no CUDA device is usable.
 #include <cstdio>
 #include <cstdlib>
@@ -37,19 +38,37 @@ static int run(shinobi::FWObject& obj, const char* out_path, uint32_t rx, uint32
   cudaMalloc((void**)&d_tri, 4 * n);
   cudaMalloc((void**)&d_t, 4 * n);
   shn_hits hits{d_tri, d_t, nullptr, nullptr};
+  float* d_frame = nullptr;
+  float* d_final = nullptr;
+  cudaMalloc((void**)&d_frame, 12 * n);
+  cudaMalloc((void**)&d_final, 12 * n);
+  cudaMemset(d_final, 0, 12 * n);
   shinobi::DirectIlluminationIntegrator integ;
-  integ.tracePrimary(engine.grid(), cam, hits, 0);
+  integ.lightSource.position = shinobi::vec3f{0.3f, 1.2f, 0.3f};
+  integ.lightSource.edge1 = shinobi::vec3f{0.4f, 0.f, 0.f};
+  integ.lightSource.edge2 = shinobi::vec3f{0.f, 0.f, 0.4f};
+  integ.lightSource.intensity = shinobi::vec3f{4.f, 4.f, 4.f};
+  shinobi::MaterialContainer materials;
+  shinobi::FrameBuffer frame{d_frame, rx, ry}, final_image{d_final, rx, ry};
+  engine.renderImage(integ, cam, hits, materials, frame, final_image, 0);
   cudaDeviceSynchronize();
   std::vector<uint32_t> tri(n);
-  std::vector<float> t(n);
+  std::vector<float> t(n), rgb(3 * n), acc(3 * n);
   cudaMemcpy(tri.data(), d_tri, 4 * n, cudaMemcpyDeviceToHost);
   cudaMemcpy(t.data(), d_t, 4 * n, cudaMemcpyDeviceToHost);
+  cudaMemcpy(rgb.data(), d_frame, 12 * n, cudaMemcpyDeviceToHost);
+  cudaMemcpy(acc.data(), d_final, 12 * n, cudaMemcpyDeviceToHost);
   cudaFree(d_tri);
   cudaFree(d_t);
+  cudaFree(d_frame);
+  cudaFree(d_final);
+  for (size_t i = 0; i < 3 * n; ++i)
+    if (acc[i] != rgb[i]) return 4;  // image 0: the final image equals the frame
   FILE* f = fopen(out_path, "wb");
   if (!f) return 1;
   fwrite(tri.data(), 4, n, f);
   fwrite(t.data(), 4, n, f);
+  fwrite(rgb.data(), 4, 3 * n, f);
   fclose(f);
   engine.builder().outputStats(std::cout);
   return 0;

@@ -1,7 +1,8 @@
 """The C++ adapters (include/shinobi/shinobi.hpp) with the reference's class
 and method names: tests/cpp/adapter_example.cpp must compile against the
 header and the library, fail cleanly without a device, and on a GPU produce
-the oracle's primary hits for a uniform and a two-level grid."""
+the oracle's primary hits and direct-illumination frame for a uniform and a
+two-level grid."""
 import os
 import shutil
 import struct
@@ -64,7 +65,8 @@ def test_adapter_primary_hits_match_oracle(tmp_path, gpu, kind):
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, (r.stdout, r.stderr)
     raw = np.fromfile(tmp_path / "o.bin", np.uint32)
-    tri, t = raw[: rx * ry], raw[rx * ry:].view(np.float32)
+    n = rx * ry
+    tri, t, rgb = raw[:n], raw[n:2 * n].view(np.float32), raw[2 * n:].view(np.float32).reshape(n, 3)
     b = oracle.bounds(sc.vertices, sc.indices)
     if kind == 0:
         g = oracle.build_uniform(sc.vertices, sc.indices, b, oracle.resolution(sc.num_triangles, b, 5.0))
@@ -77,4 +79,11 @@ def test_adapter_primary_hits_match_oracle(tmp_path, gpu, kind):
     assert np.count_nonzero(rt != oracle.MISS) > 1000
     assert np.array_equal(tri, rt)
     assert np.array_equal(t.view(np.uint32), rtt.view(np.uint32))
+    light = dict(position=(0.3, 1.2, 0.3), edge1=(0.4, 0.0, 0.0), edge2=(0.0, 0.0, 0.4),
+                 normal=(0.0, -1.0, 0.0), intensity=(4.0, 4.0, 4.0))
+    ro, rd, _ = oracle.direct_rays(o, d, rt, rtt, 4, 1, 0, light)
+    occ, _ = oracle.trace_any(g, ro, rd, np.full(ro.shape[0], 0.9999, np.float32))
+    frame, _ = oracle.shade_direct(sc.vertices, sc.indices, o, d, rt, rtt, 4, 1, 0, light, occ)
+    assert np.array_equal(rgb.view(np.uint32), frame.view(np.uint32))
+    assert (frame > 0).any()
     assert "Grid resolution" in r.stdout
