@@ -89,7 +89,8 @@ __global__ void __launch_bounds__(kBatchTraceBlock, 8) k_batch_trace(GridView G,
                                                                  uint32_t ns, uint32_t n, uint32_t* counter,
                                                                  uint32_t* otri, float* ot, float* ou,
                                                                  float* ov, uint8_t* occ) {
-  warp_trace_acc<0, ANY>(
+  // incoherent rays rarely share a cell range: no grouping (measured slower here)
+  warp_trace_acc<0, ANY, false>(
       BatchAccW{A, refs_of(G)}, n, counter,
       [&](uint32_t i, V3& o, V3& d, float& tmax, uint32_t& scene, uint32_t&) {
         uint32_t lo = 0, hi = ns;

@@ -50,7 +50,8 @@ __global__ void __launch_bounds__(kServeBlock, 8) k_serve_trace(const ServeSeg* 
                                                             const float4* __restrict__ rays, uint32_t n,
                                                             uint32_t* counter, uint32_t* __restrict__ otri,
                                                             float* __restrict__ ot) {
-  warp_trace_acc<0, false>(
+  // incoherent request rays rarely share a cell range: no grouping
+  warp_trace_acc<0, false, false>(
       ServeAcc{segs}, n, counter,
       [&](uint32_t i, V3& o, V3& d, float& tmax, uint32_t& seg, uint32_t& anyhit) {
         uint32_t lo = 0, hi = nseg;

@@ -12,6 +12,8 @@
 //    reference's HybridIntersector work donation
 //    (src/Intersector/HybridIntersector.hpp:472-704) and keeps lanes busy
 //    when one ray sits in a cell with tens of thousands of references.
+//    When several lanes wait on the same large range, each 32-reference chunk
+//    is loaded once and tested against all of their rays (group_range).
 // Lanes whose ray has finished take a new ray from the global pool at the
 // top of the loop (persistent threads with per-lane replenishment).
 //
@@ -20,6 +22,8 @@
 // hit is the argmin of (t, reference index) over the tested references, the
 // same winner the sequential strict-< loop keeps, so results are identical.
 #pragma once
+#include <type_traits>
+
 #include "trace.cuh"
 
 namespace shn {
@@ -54,7 +58,31 @@ struct Lane {
   uint32_t anyhit;        // runtime any-hit flag (mixed launches)
 };
 
-SHN_D RayWT lane_ray(const Lane& L) {
+// The same state for kernels that test shared ranges as a group: the first
+// eight words hold what a group test reads of another lane's ray (origin and
+// shear, then the permutation and the bound) as two 16-byte words.  The
+// kernels without grouping keep the layout above, measured faster for them.
+struct __align__(16) LaneG {
+  V3 org;
+  float Sx;
+  float Sy, Sz;
+  uint32_t perm;
+  float tbest;
+  uint32_t best;
+  V3 rcp;
+  V3 cell, tMax;
+  float tEntry;
+  int vis, cap;
+  V3 sc, sMax, scs, cres;
+  uint32_t lb;
+  int vis2;
+  uint32_t b, e;
+  uint32_t st;
+  uint32_t anyhit;
+};
+
+template <class LT>
+SHN_D RayWT lane_ray(const LT& L) {
   RayWT r;
   r.org = L.org;
   r.kx = L.perm & 3;
@@ -66,8 +94,8 @@ SHN_D RayWT lane_ray(const Lane& L) {
   return r;
 }
 
-template <int KIND>
-SHN_D void lane_init(const Geom& g, Lane& L, V3 org, V3 dir, float tmax) {
+template <int KIND, class LT>
+SHN_D void lane_init(const Geom& g, LT& L, V3 org, V3 dir, float tmax) {
   L.org = org;
   L.rcp = divv(mk(1.f, 1.f, 1.f), dir);
   const RayWT w = wt_setup(org, dir);
@@ -114,9 +142,9 @@ SHN_D void lane_init(const Geom& g, Lane& L, V3 org, V3 dir, float tmax) {
 
 // Runs the lane's state machine until it has a non-empty range to test
 // (returns true, range in L.b/L.e) or the ray is finished (returns false).
-template <int KIND, bool ANY>
+template <int KIND, bool ANY, class LT>
 SHN_D bool lane_advance(const Geom& g, const uint2* __restrict__ cells, const uint2* __restrict__ leaves,
-                        Lane& L, uint32_t& steps) {
+                        LT& L, uint32_t& steps) {
   while (true) {
     switch (L.st) {
       case ST_TOP: {
@@ -229,10 +257,9 @@ SHN_D float cget(V3 v) {
   return K == 0 ? v.x : (K == 1 ? v.y : v.z);
 }
 
+// The test on vertices already translated by the ray origin.
 template <int KX, int KY, int KZ>
-SHN_D bool wt_test_p(V3 org, float Sx, float Sy, float Sz, float4 p0, float4 p1, float4 p2,
-                     float tmin, float tbest, float& t) {
-  const V3 A = sub(f4v(p0), org), B = sub(f4v(p1), org), C = sub(f4v(p2), org);
+SHN_D bool wt_test_t(V3 A, V3 B, V3 C, float Sx, float Sy, float Sz, float tmin, float tbest, float& t) {
   const float Akz = cget<KZ>(A), Bkz = cget<KZ>(B), Ckz = cget<KZ>(C);
   const float Ax = __fmaf_rn(-Sx, Akz, cget<KX>(A));
   const float Ay = __fmaf_rn(-Sy, Akz, cget<KY>(A));
@@ -259,6 +286,13 @@ SHN_D bool wt_test_p(V3 org, float Sx, float Sy, float Sz, float4 p0, float4 p1,
   if (!(tt > tmin && tt < tbest)) return false;
   t = tt;
   return true;
+}
+
+template <int KX, int KY, int KZ>
+SHN_D bool wt_test_p(V3 org, float Sx, float Sy, float Sz, float4 p0, float4 p1, float4 p2,
+                     float tmin, float tbest, float& t) {
+  return wt_test_t<KX, KY, KZ>(sub(f4v(p0), org), sub(f4v(p1), org), sub(f4v(p2), org), Sx, Sy, Sz, tmin,
+                               tbest, t);
 }
 
 // Whole warp tests references [b, e) against one (warp-uniform) ray.
@@ -347,9 +381,105 @@ SHN_D uint64_t warp_range(const Refs& G, uint32_t perm, V3 org, float Sx, float 
   }
 }
 
-// Per-lane test of its own (small) range with the generic watertight test.
+// Several lanes wait on the same large range (same scene, same first
+// reference, same axis permutation): each lane loads one reference of every
+// 32-reference chunk once and tests it against each of those rays in turn,
+// reading the ray's origin and shear from its parked state (a broadcast), so
+// a chunk crosses L2 once for the group instead of once per ray.  Candidates
+// of ray r go to gkey[r] (t bits << 32 | reference, ~0 = none) by atomicMin.
+// A candidate must beat the ray's bound from earlier cells strictly and may
+// tie the range's running minimum (bound = next float above it), so gkey[r]
+// ends as the argmin over (t, reference) of the range's candidates below the
+// earlier bound -- what warp_range_p returns -- in whatever order the lanes'
+// updates land.  An any-hit ray leaves after the first chunk holding a hit
+// (gend[r] = end of that chunk), as in warp_range_p.  SAME: every ray of the
+// group has the same origin (camera rays), so the vertices are translated
+// once per chunk instead of once per ray (the same operations, the same bits).
+template <int KX, int KY, int KZ, bool SAME>
+SHN_D void group_range_p(const Refs& G, const LaneG* park, unsigned long long* gkey, uint32_t* gend,
+                         uint32_t gmask, uint32_t b, uint32_t e, bool any_all) {
+  const int lane = threadIdx.x & 31;
+  uint32_t live = gmask;
+  const float4* q0 = G.rv0 + b + lane;
+  const float4* q1 = G.rv1 + b + lane;
+  const float4* q2 = G.rv2 + b + lane;
+  for (uint32_t base = b; base < e && live; base += 32, q0 += 32, q1 += 32, q2 += 32) {
+    const uint32_t it = base + lane;
+    const bool ok = it < e;
+    float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0, p2 = p0;
+    if (ok) {
+      p0 = __ldg(q0);
+      p1 = __ldg(q1);
+      p2 = __ldg(q2);
+    }
+    V3 A, B, C;
+    if (SAME) {
+      const V3 o = park[__ffs(gmask) - 1].org;
+      A = sub(f4v(p0), o);
+      B = sub(f4v(p1), o);
+      C = sub(f4v(p2), o);
+    }
+    uint32_t m = live;
+    while (m) {
+      const int r = __ffs(m) - 1;
+      m &= m - 1;
+      const float4 ra = *reinterpret_cast<const float4*>(&park[r].org);  // org, Sx
+      const float4 rb = *reinterpret_cast<const float4*>(&park[r].Sy);   // Sy, Sz, perm, tbest
+      const unsigned long long k = *reinterpret_cast<volatile const unsigned long long*>(gkey + r);
+      const float bound = k == ~0ull ? rb.w : __uint_as_float((uint32_t)(k >> 32) + 1u);
+      float t;
+      const bool hit =
+          ok && (SAME ? wt_test_t<KX, KY, KZ>(A, B, C, ra.w, rb.x, rb.y, kEps, bound, t)
+                      : wt_test_p<KX, KY, KZ>(mk(ra.x, ra.y, ra.z), ra.w, rb.x, rb.y, p0, p1, p2, kEps, bound, t));
+      if (hit) atomicMin(gkey + r, ((unsigned long long)__float_as_uint(t) << 32) | it);
+      if (any_all || park[r].anyhit) {
+        if (__any_sync(0xFFFFFFFFu, hit)) {
+          live &= ~(1u << r);
+          if (lane == 0) gend[r] = min(e, base + 32u);
+        }
+      }
+    }
+  }
+  __syncwarp();
+}
+
+template <bool SAME>
+SHN_D void group_range_s(const Refs& G, uint32_t perm, const LaneG* park, unsigned long long* gkey,
+                         uint32_t* gend, uint32_t gmask, uint32_t b, uint32_t e, bool any_all) {
+  switch (perm) {
+    case (1u | 2u << 2 | 0u << 4): group_range_p<1, 2, 0, SAME>(G, park, gkey, gend, gmask, b, e, any_all); break;
+    case (2u | 1u << 2 | 0u << 4): group_range_p<2, 1, 0, SAME>(G, park, gkey, gend, gmask, b, e, any_all); break;
+    case (2u | 0u << 2 | 1u << 4): group_range_p<2, 0, 1, SAME>(G, park, gkey, gend, gmask, b, e, any_all); break;
+    case (0u | 2u << 2 | 1u << 4): group_range_p<0, 2, 1, SAME>(G, park, gkey, gend, gmask, b, e, any_all); break;
+    case (0u | 1u << 2 | 2u << 4): group_range_p<0, 1, 2, SAME>(G, park, gkey, gend, gmask, b, e, any_all); break;
+    default:                        group_range_p<1, 0, 2, SAME>(G, park, gkey, gend, gmask, b, e, any_all); break;
+  }
+}
+
+// SAME is used by closest-hit kernels only (camera rays share the eye); the
+// any-hit kernels' rays start from per-pixel hit points.
 template <bool ANY>
-SHN_D void lane_range(const Refs& G, Lane& L, uint32_t& tests) {
+SHN_D void group_range(const Refs& G, uint32_t perm, const LaneG* park, unsigned long long* gkey,
+                       uint32_t* gend, uint32_t gmask, uint32_t b, uint32_t e, bool any_all) {
+  if (ANY) {
+    group_range_s<false>(G, perm, park, gkey, gend, gmask, b, e, any_all);
+    return;
+  }
+  // do all rays of the group share the first one's origin (bit for bit)?
+  const V3 o0 = park[__ffs(gmask) - 1].org;
+  bool same = true;
+  for (uint32_t m = gmask; m; m &= m - 1) {
+    const V3 o = park[__ffs(m) - 1].org;
+    same = same && __float_as_uint(o.x) == __float_as_uint(o0.x) && __float_as_uint(o.y) == __float_as_uint(o0.y) &&
+           __float_as_uint(o.z) == __float_as_uint(o0.z);
+  }
+  if (same) group_range_s<true>(G, perm, park, gkey, gend, gmask, b, e, any_all);
+  else group_range_s<false>(G, perm, park, gkey, gend, gmask, b, e, any_all);
+}
+
+// Per-lane test of its own (small) range with the generic watertight test.
+template <bool ANY, class LT>
+SHN_D void lane_range(const Refs& G, LT& L, uint32_t& tests) {
   const RayWT w = lane_ray(L);
   for (uint32_t it = L.b; it < L.e; ++it) {
     tests++;
@@ -367,7 +497,8 @@ SHN_D void lane_range(const Refs& G, Lane& L, uint32_t& tests) {
 
 // Final hit record of a lane: triangle id and barycentrics of the best
 // reference, recomputed with the same arithmetic.
-SHN_D void lane_result(const Refs& G, const Lane& L, Hit& h) {
+template <class LT>
+SHN_D void lane_result(const Refs& G, const LT& L, Hit& h) {
   h.t = L.tbest;
   h.tri = kMiss;
   h.u = h.v = 0.f;
@@ -386,12 +517,17 @@ SHN_D void lane_result(const Refs& G, const Lane& L, Hit& h) {
 // scene id; G holds the reference-ordered triangle arrays shared by all
 // scenes.  src(i, org, dir, tmax, scene) generates ray i; sink(i, hit, steps,
 // tests) consumes its result.  n rays are taken from *counter (pre-zeroed).
-template <int KIND, bool ANY, class Acc, class Src, class Sink>
+// GROUP: lanes waiting on the same large range test it together
+// (group_range); worth it for coherent rays (camera, AO, shadow segments).
+template <int KIND, bool ANY, bool GROUP = true, class Acc, class Src, class Sink>
 SHN_D void warp_trace_acc(const Acc& acc, uint32_t n, uint32_t* counter, Src&& src, Sink&& sink) {
-  __shared__ Lane lane_park[kCoopBlock];
+  using LaneT = typename std::conditional<GROUP, LaneG, Lane>::type;
+  __shared__ LaneT lane_park[kCoopBlock];
+  __shared__ unsigned long long grp_key[kCoopBlock];
+  __shared__ uint32_t grp_end[kCoopBlock];
   const int lane = threadIdx.x & 31;
   const uint32_t lt = (1u << lane) - 1u;
-  Lane L;
+  LaneT L;
   L.st = ST_DONE;
   bool has = false;
   uint32_t rid = 0, steps = 0, tests = 0, scene = 0;
@@ -439,22 +575,42 @@ SHN_D void warp_trace_acc(const Acc& acc, uint32_t n, uint32_t* counter, Src&& s
     uint32_t bmask = __ballot_sync(0xFFFFFFFFu, big);
     if (bmask) {
       // The lanes' traversal state waits in shared memory while the warp tests
-      // the large ranges, so the test loop has the registers to itself.
-      Lane* park = lane_park + (threadIdx.x & ~31u);
+      // the large ranges, so the test loops have the registers to themselves.
+      const uint32_t wb = threadIdx.x & ~31u;
+      LaneT* park = lane_park + wb;
+      unsigned long long* gkey = grp_key + wb;
+      uint32_t* gend = grp_end + wb;
       park[lane] = L;
+      // lanes waiting on the same range: same scene, first reference and axis permutation
+      const unsigned long long rkey =
+          big ? (((unsigned long long)scene << 38) | ((unsigned long long)L.perm << 32) | L.b) : ~0ull - lane;
+      const uint32_t same = GROUP ? __match_any_sync(0xFFFFFFFFu, rkey) : (1u << lane);
+      if (GROUP) {
+        gkey[lane] = ~0ull;
+        gend[lane] = L.e;
+      }
       __syncwarp();
+      uint32_t grouped = 0;
       while (bmask) {
         const int j = __ffs(bmask) - 1;
-        bmask &= bmask - 1;
-        const Lane& Lj = park[j];
+        const uint32_t gm = __shfl_sync(0xFFFFFFFFu, same, j) & bmask;
+        bmask &= ~gm;
+        const LaneT& Lj = park[j];
+        const uint32_t sj = __shfl_sync(0xFFFFFFFFu, scene, j);
+        const Refs R = acc.refs(sj);
+        if constexpr (GROUP) {
+          if (gm & (gm - 1)) {
+            grouped |= gm;
+            group_range<ANY>(R, Lj.perm, park, gkey, gend, gm, Lj.b, Lj.e, ANY);
+            continue;
+          }
+        }
         const V3 org = Lj.org;
         const float Sx = Lj.Sx, Sy = Lj.Sy, Sz = Lj.Sz;
         const uint32_t perm = Lj.perm;
         const float tb = Lj.tbest;
         const uint32_t b = Lj.b, e = Lj.e;
         const uint32_t aj = Lj.anyhit;
-        const uint32_t sj = __shfl_sync(0xFFFFFFFFu, scene, j);
-        const Refs R = acc.refs(sj);
         uint32_t wt = 0;
         const uint64_t key = (ANY || aj) ? warp_range<true>(R, perm, org, Sx, Sy, Sz, tb, b, e, wt)
                                          : warp_range<false>(R, perm, org, Sx, Sy, Sz, tb, b, e, wt);
@@ -467,6 +623,15 @@ SHN_D void warp_trace_acc(const Acc& acc, uint32_t n, uint32_t* counter, Src&& s
         }
         __syncwarp();
       }
+      if (GROUP && ((grouped >> lane) & 1u)) {
+        tests += gend[lane] - park[lane].b;
+        const unsigned long long k = gkey[lane];
+        if (k != ~0ull) {
+          park[lane].tbest = __uint_as_float((uint32_t)(k >> 32));
+          park[lane].best = (uint32_t)k;
+        }
+      }
+      __syncwarp();
       L = park[lane];
       __syncwarp();
     }
