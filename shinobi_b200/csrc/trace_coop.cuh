@@ -395,29 +395,43 @@ SHN_D uint64_t warp_range(const Refs& G, uint32_t perm, V3 org, float Sx, float 
 // (gend[r] = end of that chunk), as in warp_range_p.  SAME: every ray of the
 // group has the same origin (camera rays), so the vertices are translated
 // once per chunk instead of once per ray (the same operations, the same bits).
-template <int KX, int KY, int KZ, bool SAME>
+template <int KX, int KY, int KZ, bool SAME, bool ANY>
 SHN_D void group_range_p(const Refs& G, const LaneG* park, unsigned long long* gkey, uint32_t* gend,
-                         uint32_t gmask, uint32_t b, uint32_t e, bool any_all) {
+                         uint32_t gmask, uint32_t b, uint32_t e) {
+  // closest hit: two references per lane per chunk (64-reference chunks), so a
+  // ray's parameters are read once per two tests; any hit: 32-reference chunks,
+  // the granularity of warp_range_p's early exit
+  constexpr uint32_t kStep = ANY ? 32u : 64u;
   const int lane = threadIdx.x & 31;
   uint32_t live = gmask;
   const float4* q0 = G.rv0 + b + lane;
   const float4* q1 = G.rv1 + b + lane;
   const float4* q2 = G.rv2 + b + lane;
-  for (uint32_t base = b; base < e && live; base += 32, q0 += 32, q1 += 32, q2 += 32) {
-    const uint32_t it = base + lane;
-    const bool ok = it < e;
-    float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0, p2 = p0;
+  const V3 o0 = park[__ffs(gmask) - 1].org;
+  for (uint32_t base = b; base < e && live; base += kStep, q0 += kStep, q1 += kStep, q2 += kStep) {
+    const uint32_t it = base + lane, it2 = it + 32u;
+    const bool ok = it < e, ok2 = !ANY && it2 < e;
+    float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0, p2 = p0, c0 = p0, c1 = p0, c2 = p0;
     if (ok) {
       p0 = __ldg(q0);
       p1 = __ldg(q1);
       p2 = __ldg(q2);
     }
-    V3 A, B, C;
+    if (ok2) {
+      c0 = __ldg(q0 + 32);
+      c1 = __ldg(q1 + 32);
+      c2 = __ldg(q2 + 32);
+    }
+    V3 A, B, C, A2, B2, C2;
     if (SAME) {
-      const V3 o = park[__ffs(gmask) - 1].org;
-      A = sub(f4v(p0), o);
-      B = sub(f4v(p1), o);
-      C = sub(f4v(p2), o);
+      A = sub(f4v(p0), o0);
+      B = sub(f4v(p1), o0);
+      C = sub(f4v(p2), o0);
+      if (!ANY) {
+        A2 = sub(f4v(c0), o0);
+        B2 = sub(f4v(c1), o0);
+        C2 = sub(f4v(c2), o0);
+      }
     }
     uint32_t m = live;
     while (m) {
@@ -431,8 +445,20 @@ SHN_D void group_range_p(const Refs& G, const LaneG* park, unsigned long long* g
       const bool hit =
           ok && (SAME ? wt_test_t<KX, KY, KZ>(A, B, C, ra.w, rb.x, rb.y, kEps, bound, t)
                       : wt_test_p<KX, KY, KZ>(mk(ra.x, ra.y, ra.z), ra.w, rb.x, rb.y, p0, p1, p2, kEps, bound, t));
-      if (hit) atomicMin(gkey + r, ((unsigned long long)__float_as_uint(t) << 32) | it);
-      if (any_all || park[r].anyhit) {
+      unsigned long long cand = hit ? (((unsigned long long)__float_as_uint(t) << 32) | it) : ~0ull;
+      if (!ANY) {
+        float t2;
+        const bool hit2 =
+            ok2 && (SAME ? wt_test_t<KX, KY, KZ>(A2, B2, C2, ra.w, rb.x, rb.y, kEps, bound, t2)
+                         : wt_test_p<KX, KY, KZ>(mk(ra.x, ra.y, ra.z), ra.w, rb.x, rb.y, c0, c1, c2, kEps, bound,
+                                                 t2));
+        if (hit2) {
+          const unsigned long long c2k = ((unsigned long long)__float_as_uint(t2) << 32) | it2;
+          cand = c2k < cand ? c2k : cand;
+        }
+      }
+      if (cand != ~0ull) atomicMin(gkey + r, cand);
+      if (ANY) {
         if (__any_sync(0xFFFFFFFFu, hit)) {
           live &= ~(1u << r);
           if (lane == 0) gend[r] = min(e, base + 32u);
@@ -443,26 +469,28 @@ SHN_D void group_range_p(const Refs& G, const LaneG* park, unsigned long long* g
   __syncwarp();
 }
 
-template <bool SAME>
+template <bool SAME, bool ANY>
 SHN_D void group_range_s(const Refs& G, uint32_t perm, const LaneG* park, unsigned long long* gkey,
-                         uint32_t* gend, uint32_t gmask, uint32_t b, uint32_t e, bool any_all) {
+                         uint32_t* gend, uint32_t gmask, uint32_t b, uint32_t e) {
   switch (perm) {
-    case (1u | 2u << 2 | 0u << 4): group_range_p<1, 2, 0, SAME>(G, park, gkey, gend, gmask, b, e, any_all); break;
-    case (2u | 1u << 2 | 0u << 4): group_range_p<2, 1, 0, SAME>(G, park, gkey, gend, gmask, b, e, any_all); break;
-    case (2u | 0u << 2 | 1u << 4): group_range_p<2, 0, 1, SAME>(G, park, gkey, gend, gmask, b, e, any_all); break;
-    case (0u | 2u << 2 | 1u << 4): group_range_p<0, 2, 1, SAME>(G, park, gkey, gend, gmask, b, e, any_all); break;
-    case (0u | 1u << 2 | 2u << 4): group_range_p<0, 1, 2, SAME>(G, park, gkey, gend, gmask, b, e, any_all); break;
-    default:                        group_range_p<1, 0, 2, SAME>(G, park, gkey, gend, gmask, b, e, any_all); break;
+    case (1u | 2u << 2 | 0u << 4): group_range_p<1, 2, 0, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
+    case (2u | 1u << 2 | 0u << 4): group_range_p<2, 1, 0, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
+    case (2u | 0u << 2 | 1u << 4): group_range_p<2, 0, 1, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
+    case (0u | 2u << 2 | 1u << 4): group_range_p<0, 2, 1, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
+    case (0u | 1u << 2 | 2u << 4): group_range_p<0, 1, 2, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
+    default:                        group_range_p<1, 0, 2, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
   }
 }
 
-// SAME is used by closest-hit kernels only (camera rays share the eye); the
-// any-hit kernels' rays start from per-pixel hit points.
+// ANY: the kernel's rays are all any-hit (lanes with a per-ray any-hit flag in
+// a closest-hit kernel never join a group).  SAME is used by closest-hit
+// kernels only (camera rays share the eye); the any-hit kernels' rays start
+// from per-pixel hit points.
 template <bool ANY>
 SHN_D void group_range(const Refs& G, uint32_t perm, const LaneG* park, unsigned long long* gkey,
-                       uint32_t* gend, uint32_t gmask, uint32_t b, uint32_t e, bool any_all) {
+                       uint32_t* gend, uint32_t gmask, uint32_t b, uint32_t e) {
   if (ANY) {
-    group_range_s<false>(G, perm, park, gkey, gend, gmask, b, e, any_all);
+    group_range_s<false, true>(G, perm, park, gkey, gend, gmask, b, e);
     return;
   }
   // do all rays of the group share the first one's origin (bit for bit)?
@@ -473,8 +501,8 @@ SHN_D void group_range(const Refs& G, uint32_t perm, const LaneG* park, unsigned
     same = same && __float_as_uint(o.x) == __float_as_uint(o0.x) && __float_as_uint(o.y) == __float_as_uint(o0.y) &&
            __float_as_uint(o.z) == __float_as_uint(o0.z);
   }
-  if (same) group_range_s<true>(G, perm, park, gkey, gend, gmask, b, e, any_all);
-  else group_range_s<false>(G, perm, park, gkey, gend, gmask, b, e, any_all);
+  if (same) group_range_s<true, false>(G, perm, park, gkey, gend, gmask, b, e);
+  else group_range_s<false, false>(G, perm, park, gkey, gend, gmask, b, e);
 }
 
 // Per-lane test of its own (small) range with the generic watertight test.
@@ -582,8 +610,9 @@ SHN_D void warp_trace_acc(const Acc& acc, uint32_t n, uint32_t* counter, Src&& s
       uint32_t* gend = grp_end + wb;
       park[lane] = L;
       // lanes waiting on the same range: same scene, first reference and axis permutation
-      const unsigned long long rkey =
-          big ? (((unsigned long long)scene << 38) | ((unsigned long long)L.perm << 32) | L.b) : ~0ull - lane;
+      const unsigned long long rkey = (big && (ANY || !L.anyhit))
+                                          ? (((unsigned long long)scene << 38) | ((unsigned long long)L.perm << 32) | L.b)
+                                          : ~0ull - lane;
       const uint32_t same = GROUP ? __match_any_sync(0xFFFFFFFFu, rkey) : (1u << lane);
       if (GROUP) {
         gkey[lane] = ~0ull;
@@ -601,7 +630,7 @@ SHN_D void warp_trace_acc(const Acc& acc, uint32_t n, uint32_t* counter, Src&& s
         if constexpr (GROUP) {
           if (gm & (gm - 1)) {
             grouped |= gm;
-            group_range<ANY>(R, Lj.perm, park, gkey, gend, gm, Lj.b, Lj.e, ANY);
+            group_range<ANY>(R, Lj.perm, park, gkey, gend, gm, Lj.b, Lj.e);
             continue;
           }
         }
