@@ -137,14 +137,17 @@ typedef struct shn_grid_info {
 shn_status shn_grid_create(shn_ctx* ctx, shn_grid** out);
 /* Builds (or rebuilds) the grid over the scene on stream.  Synchronises the
  * stream up to twice (uniform) / four times (two-level) to size buffers from
- * device-side counts, as the reference does. */
+ * device-side counts, as the reference does.  Traces of the grid read the
+ * scene's triangles (hit records, normals), so the scene must outlive them. */
 shn_status shn_grid_build(shn_grid* g, const shn_scene* s, const shn_grid_params* p, void* stream);
 shn_status shn_grid_get_info(const shn_grid* g, shn_grid_info* out);
 /* Copies the grid to host buffers (any may be NULL): cells = 2*num_cells
  * uint32 (uniform: [begin,end) ranges; two-level: cell words in the
  * TwoLevelGridCell layout), leaves = 2*num_leaves, indices = num_refs,
  * top_pairs = num_top_refs sorted (cell<<32 | tri) keys (two-level) or
- * num_refs (uniform).  Synchronises. */
+ * num_refs (uniform), all in (cell, triangle id) order.  A two-level grid
+ * keeps the references of each leaf in spatial order on the device; the
+ * export puts them back in that order.  Synchronises. */
 shn_status shn_grid_export(const shn_grid* g, uint32_t* cells, uint32_t* leaves, uint32_t* indices,
                            uint64_t* top_pairs);
 /* Frees the grid's device memory (stream-ordered, pool); every launch that

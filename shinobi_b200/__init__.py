@@ -251,7 +251,7 @@ class Grid:
     def build(self, scene: FaceSoup, params: GridParams, stream=None) -> "Grid":
         self.ctx.check(self.ctx.lib.shn_grid_build(self.handle, scene.handle, C.byref(params),
                                                    _stream(stream)), "shn_grid_build")
-        self.scene = scene  # the grid reads the scene's triangles for AO frames
+        self.scene = scene  # traces read the scene's triangles (hit records, AO and shading normals)
         return self
 
     def info(self) -> GridInfo:

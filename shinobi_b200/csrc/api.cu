@@ -321,7 +321,8 @@ shn_status shn_grid_get_info(const shn_grid* g, shn_grid_info* o) {
   o->num_refs = g->num_refs;
   o->device_bytes = g->cap_cells + g->cap_leaves + g->cap_refs + g->cap_rtri + g->offs_tri.bytes +
                     g->offs_pair.bytes + g->scan.bytes + g->top_ranges.bytes + g->keys[0].bytes +
-                    g->keys[1].bytes + g->keys[2].bytes + g->sortws.bytes;
+                    g->keys[1].bytes + g->keys[2].bytes + g->sortws.bytes + g->mhi.bytes + g->perm_tri.bytes +
+                    g->cbox.bytes + g->sbox.bytes;
   o->build_ms = g->build_ms;
   return g->built ? SHN_OK : SHN_ERR_NOT_BUILT;
 }
@@ -336,6 +337,27 @@ shn_status shn_grid_export(const shn_grid* g, uint32_t* cells, uint32_t* leaves,
   if (e == cudaSuccess && indices && g->num_refs) e = cudaMemcpy(indices, g->indices, g->num_refs * 4, cudaMemcpyDeviceToHost);
   const uint64_t np = g->kind == SHN_GRID_TWO_LEVEL ? g->num_top_refs : g->num_refs;
   if (e == cudaSuccess && top_pairs && np) e = cudaMemcpy(top_pairs, g->top_pairs, np * 8, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && g->spatial) {
+    // a two-level grid was built on the triangles in Morton order: the
+    // references of a leaf are in that order and the pairs' low words are
+    // positions in it; both are put back in (cell, triangle id) order
+    if (indices && g->num_refs) {
+      std::vector<uint2> lv(g->num_leaves);
+      e = cudaMemcpy(lv.data(), g->leaves, g->num_leaves * 8, cudaMemcpyDeviceToHost);
+      for (size_t i = 0; e == cudaSuccess && i < lv.size(); ++i)
+        if (lv[i].y > lv[i].x) std::sort(indices + lv[i].x, indices + lv[i].y);
+    }
+    if (e == cudaSuccess && top_pairs && np) {
+      std::vector<float4> pt((size_t)g->src_nt * 3);
+      e = cudaMemcpy(pt.data(), g->perm_tri.ptr, pt.size() * sizeof(float4), cudaMemcpyDeviceToHost);
+      for (uint64_t i = 0; e == cudaSuccess && i < np; ++i) {
+        uint32_t id;
+        memcpy(&id, &pt[3 * (size_t)(uint32_t)top_pairs[i]].w, 4);
+        top_pairs[i] = (top_pairs[i] & 0xFFFFFFFF00000000ull) | id;
+      }
+      if (e == cudaSuccess) std::sort(top_pairs, top_pairs + np);
+    }
+  }
   return e == cudaSuccess ? SHN_OK : cuda_status(g->ctx, e, "grid export");
 }
 
@@ -347,7 +369,8 @@ void shn_grid_destroy(shn_grid* g) {
   dev_free(c, g->leaves, g->cap_leaves, st);
   dev_free(c, g->indices, g->cap_refs, st);
   dev_free(c, g->rtri, g->cap_rtri, st);
-  DevBuf* bufs[] = {&g->offs_tri, &g->offs_pair, &g->scan, &g->top_ranges, &g->keys[0], &g->keys[1], &g->keys[2], &g->sortws};
+  DevBuf* bufs[] = {&g->offs_tri, &g->offs_pair, &g->scan,     &g->top_ranges, &g->keys[0], &g->keys[1],
+                    &g->keys[2],   &g->sortws,    &g->mhi,      &g->perm_tri,   &g->cbox,    &g->sbox};
   for (DevBuf* b : bufs) dev_free(c, b->ptr, b->bytes, st);
   dev_free(c, g->d_err, 64, st);
   pinned_give(c, g->h_pinned);

@@ -243,6 +243,7 @@ GridView batch_view(const shn_batch* b) {
   v.rv0 = b->rtri;
   v.rv1 = b->rtri + b->P;
   v.rv2 = b->rtri + 2 * (size_t)b->P;
+  v.src = b->tri;
   return v;
 }
 
@@ -475,12 +476,13 @@ shn_status shn_batch_autotune(shn_batch* b, const float* candidates, uint32_t nu
   for (uint32_t s = 0; s < b->ns && rc == SHN_OK; ++s) {
     const uint32_t nt = b->tri_off[s + 1] - b->tri_off[s];
     if (nt == 0) continue;
-    // a scene view over the batch's packed triangles (local ids in v0.w are not needed here)
+    // a scene view over the batch's packed triangles
     shn_scene sc;
     sc.ctx = ctx;
     sc.nt = nt;
     sc.nv = 0;
     sc.tri = b->tri + 3 * (size_t)b->tri_off[s];  // the scene's records, in place
+    sc.ids = b->tri;                               // their ids count from the batch's first record
     memcpy(sc.bounds, &b->bounds[6 * s], 24);
     double best_cost = 1e300;
     for (uint32_t c = 0; c < num_candidates; ++c) {

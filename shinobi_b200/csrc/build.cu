@@ -360,13 +360,123 @@ __global__ void __launch_bounds__(kRangeBlock) k_ranges(const uint64_t* __restri
         if (next != c[q]) ranges[c[q]].y = (uint32_t)i + 1;
         // streaming (evict-first) stores: the output must not push the
         // triangles being gathered out of L2
-        if (indices) __stcs(indices + i, t[q]);
+        // the record's id: the triangle id whether or not the build ran on a
+        // reordered copy of the triangles
+        if (indices) __stcs(indices + i, rtri ? __float_as_uint(a[q].w) : t[q]);
         if (rtri) {
           __stcs(rtri + i, a[q]);
           __stcs(rtri + (size_t)n + i, b[q]);
           __stcs(rtri + 2 * (size_t)n + i, d[q]);
         }
       }
+    }
+  }
+}
+
+// ---- spatial order and block boxes (two-level grids) -------------------------
+// The build of a two-level grid runs on a copy of the triangles sorted by the
+// Morton code of their vertex sum in the scene box (20 bits per axis), so that
+// the references inside each leaf cell come out in spatial order; the cells,
+// their ranges and the set of references in each are the same as in triangle
+// order.  The 60-bit code is sorted as two stable 30-bit passes of the key
+// sort (low half first), each key carrying the triangle's position.
+SHN_HD uint32_t spread10(uint32_t v) {
+  v &= 0x3FFu;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+SHN_D uint32_t quant20(float q) { return q > 0.f ? (uint32_t)fminf(q, 1048575.f) : 0u; }
+
+__global__ void k_morton_keys(TriArr tri, uint32_t n, V3 lo3, V3 scale, uint32_t tb, uint64_t* __restrict__ keys,
+                              uint32_t* __restrict__ hi) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float4* r = tri.p + 3 * (size_t)i;
+    const V3 a = f4v(__ldg(r)), b = f4v(__ldg(r + 1)), c = f4v(__ldg(r + 2));
+    const V3 q = mul(sub(add(add(a, b), c), lo3), scale);
+    const uint32_t x = quant20(q.x), y = quant20(q.y), z = quant20(q.z);
+    const uint32_t mlo = spread10(x) | (spread10(y) << 1) | (spread10(z) << 2);
+    const uint32_t mhi = spread10(x >> 10) | (spread10(y >> 10) << 1) | (spread10(z >> 10) << 2);
+    keys[i] = ((uint64_t)mlo << tb) | i;
+    hi[i] = mhi;
+  }
+}
+
+__global__ void k_morton_second(const uint64_t* __restrict__ sorted, const uint32_t* __restrict__ hi, uint32_t n,
+                                uint32_t tb, uint64_t* __restrict__ keys) {
+  const uint64_t mask = (1ull << tb) - 1ull;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const uint32_t i = (uint32_t)(sorted[j] & mask);
+    keys[j] = ((uint64_t)__ldg(hi + i) << tb) | i;
+  }
+}
+
+__global__ void k_permute_tris(const uint64_t* __restrict__ sorted, TriArr tri, uint32_t n, uint32_t tb,
+                               float4* __restrict__ out) {
+  const uint64_t mask = (1ull << tb) - 1ull;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const uint32_t i = (uint32_t)(sorted[j] & mask);
+    const float4* r = tri.p + 3 * (size_t)i;
+    float4* o = out + 3 * (size_t)j;
+    o[0] = __ldg(r);
+    o[1] = __ldg(r + 1);
+    o[2] = __ldg(r + 2);
+  }
+}
+
+// Box (min, max) of the three vertices of references [32k, 32k + 32) of the
+// reference-ordered arrays, one warp per block; then boxes of 32 blocks.
+__global__ void k_block_boxes(const float4* __restrict__ v0, const float4* __restrict__ v1,
+                              const float4* __restrict__ v2, uint32_t n, uint32_t nblocks,
+                              float4* __restrict__ box) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t k = w0; k < nblocks; k += nw) {
+    const uint32_t i = 32u * k + lane;
+    V3 mn = mk(INFINITY, INFINITY, INFINITY), mx = mk(-INFINITY, -INFINITY, -INFINITY);
+    if (i < n) {
+      const V3 a = f4v(__ldg(v0 + i)), b = f4v(__ldg(v1 + i)), c = f4v(__ldg(v2 + i));
+      mn = vmin(vmin(a, b), c);
+      mx = vmax(vmax(a, b), c);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mn = vmin(mn, mk(__shfl_xor_sync(0xFFFFFFFFu, mn.x, o), __shfl_xor_sync(0xFFFFFFFFu, mn.y, o),
+                       __shfl_xor_sync(0xFFFFFFFFu, mn.z, o)));
+      mx = vmax(mx, mk(__shfl_xor_sync(0xFFFFFFFFu, mx.x, o), __shfl_xor_sync(0xFFFFFFFFu, mx.y, o),
+                       __shfl_xor_sync(0xFFFFFFFFu, mx.z, o)));
+    }
+    if (lane == 0) {
+      box[2 * (size_t)k] = make_float4(mn.x, mn.y, mn.z, 0.f);
+      box[2 * (size_t)k + 1] = make_float4(mx.x, mx.y, mx.z, 0.f);
+    }
+  }
+}
+
+__global__ void k_super_boxes(const float4* __restrict__ box, uint32_t nblocks, uint32_t nsuper,
+                              float4* __restrict__ sbox) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t s = w0; s < nsuper; s += nw) {
+    const uint32_t k = 32u * s + lane;
+    V3 mn = mk(INFINITY, INFINITY, INFINITY), mx = mk(-INFINITY, -INFINITY, -INFINITY);
+    if (k < nblocks) {
+      mn = f4v(__ldg(box + 2 * (size_t)k));
+      mx = f4v(__ldg(box + 2 * (size_t)k + 1));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mn = vmin(mn, mk(__shfl_xor_sync(0xFFFFFFFFu, mn.x, o), __shfl_xor_sync(0xFFFFFFFFu, mn.y, o),
+                       __shfl_xor_sync(0xFFFFFFFFu, mn.z, o)));
+      mx = vmax(mx, mk(__shfl_xor_sync(0xFFFFFFFFu, mx.x, o), __shfl_xor_sync(0xFFFFFFFFu, mx.y, o),
+                       __shfl_xor_sync(0xFFFFFFFFu, mx.z, o)));
+    }
+    if (lane == 0) {
+      sbox[2 * (size_t)s] = make_float4(mn.x, mn.y, mn.z, 0.f);
+      sbox[2 * (size_t)s + 1] = make_float4(mx.x, mx.y, mx.z, 0.f);
     }
   }
 }
@@ -627,7 +737,7 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   g->kind = p->kind;
   g->geom = make_geom(s->bounds, res);
   g->built = false;
-  g->src_tri = s->tri;
+  g->src_tri = s->ids ? s->ids : s->tri;
   g->src_nt = s->nt;
   if (!g->d_err) {
     // stream-ordered pool memory and a pinned block from the context's slab:
@@ -645,8 +755,36 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   }
   cudaMemsetAsync(g->d_err, 0, 64, st);
   cudaEventRecord(g->ev0, st);
-  const TriArr tri{s->tri};
+  TriArr tri{s->tri};
   shn_status rc;
+  g->num_blocks = g->num_super = 0;
+
+  // ---- two-level: build on the triangles in Morton order ------------------------
+  g->spatial = p->kind == SHN_GRID_TWO_LEVEL && nt > 1;
+  if (g->spatial) {
+    const uint32_t tb = 32u - (uint32_t)__builtin_clz(nt - 1);
+    for (int i = 0; i < 2; ++i)
+      if ((rc = ensure_buf(g, g->keys[i], (size_t)nt * 8, st))) return rc;
+    if ((rc = ensure_buf(g, g->mhi, (size_t)nt * 4, st))) return rc;
+    if ((rc = ensure_buf(g, g->perm_tri, (size_t)nt * 48, st))) return rc;
+    if ((rc = ensure_buf(g, g->sortws, sort_workspace_bytes(nt), st))) return rc;
+    const V3 lo = mk(s->bounds[0], s->bounds[1], s->bounds[2]);
+    const V3 hi = mk(s->bounds[3], s->bounds[4], s->bounds[5]);
+    const V3 lo3 = muls(lo, 3.f), ext3 = sub(muls(hi, 3.f), lo3);
+    const V3 scale = mk(ext3.x > 0.f ? 1048576.f / ext3.x : 0.f, ext3.y > 0.f ? 1048576.f / ext3.y : 0.f,
+                        ext3.z > 0.f ? 1048576.f / ext3.z : 0.f);
+    uint64_t* m0 = (uint64_t*)g->keys[0].ptr;
+    uint64_t* m1 = (uint64_t*)g->keys[1].ptr;
+    uint32_t* mh = (uint32_t*)g->mhi.ptr;
+    const int blocks = grid_for(nt, 256, 148 * 16);
+    k_morton_keys<<<blocks, 256, 0, st>>>(tri, nt, lo3, scale, tb, m0, mh);
+    uint64_t* s1 = onesweep_sort(m0, m1, nt, tb, 4, g->sortws.ptr, g->d_err, st);
+    uint64_t* o1 = s1 == m0 ? m1 : m0;
+    k_morton_second<<<blocks, 256, 0, st>>>(s1, mh, nt, tb, o1);
+    uint64_t* s2 = onesweep_sort(o1, s1, nt, tb, 4, g->sortws.ptr, g->d_err, st);
+    k_permute_tris<<<blocks, 256, 0, st>>>(s2, tri, nt, tb, (float4*)g->perm_tri.ptr);
+    tri = TriArr{(const float4*)g->perm_tri.ptr};
+  }
 
   // ---- counts + offsets ------------------------------------------------------
   if ((rc = ensure_buf(g, g->offs_tri, ((size_t)nt + 1) * 4, st))) return rc;
@@ -731,6 +869,18 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   if ((rc = ensure(g, (void**)&g->rtri, &g->cap_rtri, (size_t)std::max<uint32_t>(R, 1) * 48, st))) return rc;
   cudaMemsetAsync(g->leaves, 0, (size_t)Lc * 8, st);
   if (R) k_ranges<<<range_blocks(R), kRangeBlock, 0, st>>>(sortedLeaf, R, g->leaves, g->indices, tri, g->rtri);
+  if (g->spatial && R) {
+    const uint64_t nb = (R + 31) / 32, ns = (nb + 31) / 32;
+    if ((rc = ensure_buf(g, g->cbox, nb * 32, st))) return rc;
+    if ((rc = ensure_buf(g, g->sbox, ns * 32, st))) return rc;
+    const float4* rv = g->rtri;
+    k_block_boxes<<<grid_for(nb * 32, 256, 148 * 8), 256, 0, st>>>(rv, rv + R, rv + 2 * (size_t)R, R, (uint32_t)nb,
+                                                                  (float4*)g->cbox.ptr);
+    k_super_boxes<<<grid_for(ns * 32, 256, 148 * 8), 256, 0, st>>>((const float4*)g->cbox.ptr, (uint32_t)nb,
+                                                                  (uint32_t)ns, (float4*)g->sbox.ptr);
+    g->num_blocks = nb;
+    g->num_super = ns;
+  }
   g->num_leaves = Lc;
   g->num_refs = R;
   g->top_pairs = sortedTop;

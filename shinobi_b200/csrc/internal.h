@@ -51,6 +51,9 @@ struct shn_scene {
   float* vtx = nullptr;      // 3*nv
   uint32_t* idx = nullptr;   // 3*nt
   float4* tri = nullptr;     // 3*nt: per triangle a 48-byte record v0, v1, v2 (w of v0 = tri id bits)
+  // records indexed by the id in v0.w: tri itself, except for a view into a
+  // larger array whose ids count from that array's start
+  const float4* ids = nullptr;
   float bounds[6] = {0, 0, 0, 0, 0, 0};
   size_t bytes = 0;
 };
@@ -67,6 +70,13 @@ struct shn_grid {
   uint32_t* indices = nullptr;  // tri id per reference
   float4* rtri = nullptr;       // 3*num_refs: reference-ordered v0[], v1[], v2[]
   uint64_t* top_pairs = nullptr;  // two-level: sorted top pairs; uniform: sorted pairs
+  // two-level grids: the build runs on the triangles in Morton order (perm_tri,
+  // w = original id), so the pairs' low words are positions in that order;
+  // boxes of every 32 references (cbox) and every 1024 (sbox) of rtri, two
+  // float4 (min, max) each, let the traversal skip blocks a ray cannot hit
+  bool spatial = false;
+  uint64_t num_blocks = 0, num_super = 0;
+  shn::DevBuf mhi, perm_tri, cbox, sbox;
   size_t cap_cells = 0, cap_leaves = 0, cap_refs = 0, cap_rtri = 0;
   // grow-only build workspace
   shn::DevBuf offs_tri, offs_pair, scan, top_ranges, keys[3], sortws;

@@ -262,6 +262,9 @@ shn_status shn_pt_render(const shn_grid* g, const shn_scene* s, const shn_camera
     v.rv0 = g->rtri;
     v.rv1 = g->rtri + g->num_refs;
     v.rv2 = g->rtri + 2 * g->num_refs;
+    v.src = g->src_tri;
+    v.cbox = g->num_blocks ? (const float4*)g->cbox.ptr : nullptr;
+    v.sbox = g->num_blocks ? (const float4*)g->sbox.ptr : nullptr;
     return v;
   }();
 

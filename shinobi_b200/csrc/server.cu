@@ -289,6 +289,9 @@ void issue_launch(shn_server* s, ServeLaunch& la, int slot_index, std::unique_lo
     sg.g.rv0 = g->rtri;
     sg.g.rv1 = g->rtri + g->num_refs;
     sg.g.rv2 = g->rtri + 2 * g->num_refs;
+    sg.g.src = g->src_tri;
+    sg.g.cbox = g->num_blocks ? (const float4*)g->cbox.ptr : nullptr;
+    sg.g.sbox = g->num_blocks ? (const float4*)g->sbox.ptr : nullptr;
   }
   s->max_requests_per_launch = std::max<uint64_t>(s->max_requests_per_launch, la.reqs.size());
   la.busy = true;

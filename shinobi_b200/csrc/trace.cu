@@ -295,6 +295,9 @@ GridView view_of(const shn_grid* g) {
   v.rv0 = g->rtri;
   v.rv1 = g->rtri + g->num_refs;
   v.rv2 = g->rtri + 2 * g->num_refs;
+  v.src = g->src_tri;
+  v.cbox = g->num_blocks ? (const float4*)g->cbox.ptr : nullptr;
+  v.sbox = g->num_blocks ? (const float4*)g->sbox.ptr : nullptr;
   return v;
 }
 

@@ -26,6 +26,13 @@ struct GridView {
   const float4* __restrict__ rv0;
   const float4* __restrict__ rv1;
   const float4* __restrict__ rv2;
+  // the scene's triangle records (48 bytes: v0 with the id in w, v1, v2),
+  // indexed by the id that rv0[].w holds
+  const float4* __restrict__ src;
+  // boxes (min, max) of references [32k, 32k + 32) and [1024s, 1024s + 1024)
+  // of rv*, or null (no culling)
+  const float4* __restrict__ cbox;
+  const float4* __restrict__ sbox;
 };
 
 struct Hit {
@@ -97,20 +104,34 @@ SHN_D bool wt_test(const RayWT& r, float4 p0, float4 p1, float4 p2, float tmin, 
   return true;
 }
 
+// Closest hit in a range: the least (t, triangle id) below the bound from
+// earlier cells, i.e. the first minimum in triangle-id order, which is what a
+// strict-< loop over the references in (cell, triangle) order keeps.  The
+// references of a range may be stored in another order, so a candidate may
+// tie the range's running minimum (bound = next float above it) and wins on
+// the smaller id.
+SHN_D float next_up(float t) { return __uint_as_float(__float_as_uint(t) + 1u); }
+
 template <bool ANY>
 SHN_D bool test_range(const GridView& G, const RayWT& r, uint32_t b, uint32_t e, Hit& h) {
   h.steps += 1;
+  const float t0 = h.t;
+  bool found = false;
   for (uint32_t it = b; it < e; ++it) {
     h.tests += 1;
     const float4 p0 = __ldg(G.rv0 + it);
     const float4 p1 = __ldg(G.rv1 + it);
     const float4 p2 = __ldg(G.rv2 + it);
     float t, u, v;
-    if (wt_test(r, p0, p1, p2, kEps, h.t, t, u, v)) {
-      h.t = t;
-      h.tri = __float_as_uint(p0.w);
-      h.u = u;
-      h.v = v;
+    if (wt_test(r, p0, p1, p2, kEps, found ? next_up(h.t) : t0, t, u, v)) {
+      const uint32_t id = __float_as_uint(p0.w);
+      if (!found || t < h.t || id < h.tri) {
+        h.t = t;
+        h.tri = id;
+        h.u = u;
+        h.v = v;
+        found = true;
+      }
       if (ANY) return true;
     }
   }

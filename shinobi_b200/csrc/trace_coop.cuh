@@ -31,13 +31,50 @@ namespace shn {
 constexpr uint32_t kCoopThreshold = 32;
 constexpr int kCoopBlock = 128;  // threads per block of every kernel that runs the engine
 
-// Reference-ordered triangle arrays of one grid.
+// Reference-ordered triangle arrays of one grid, and the scene's records
+// indexed by triangle id (for the final hit record).
 struct Refs {
   const float4* __restrict__ rv0;
   const float4* __restrict__ rv1;
   const float4* __restrict__ rv2;
+  const float4* __restrict__ src;
+  const float4* __restrict__ cbox;  // block boxes (see GridView), or null
+  const float4* __restrict__ sbox;
 };
-SHN_D Refs refs_of(const GridView& G) { return Refs{G.rv0, G.rv1, G.rv2}; }
+SHN_D Refs refs_of(const GridView& G) { return Refs{G.rv0, G.rv1, G.rv2, G.src, G.cbox, G.sbox}; }
+
+// Ranges longer than this are tested block by block with box culling when the
+// grid has block boxes.
+constexpr uint32_t kCullMin = 64;
+
+// Reciprocal direction for box tests: infinities (zero direction components)
+// become +-1e30, so that a box face through the origin gives 0, not NaN.
+SHN_D V3 cull_rcp(V3 r) {
+  return mk(isinf(r.x) ? copysignf(1e30f, r.x) : r.x, isinf(r.y) ? copysignf(1e30f, r.y) : r.y,
+            isinf(r.z) ? copysignf(1e30f, r.z) : r.z);
+}
+
+// Whether the segment t in (0, tb] of the ray o + t d (cr = cull_rcp(1/d)) can
+// meet a triangle inside the box [mn, mx].  The slab distances carry a margin
+// of 2^-8 of their magnitude, far above the rounding of the slab arithmetic
+// and of the watertight test's t, so a block holding a triangle that the
+// watertight test hits below tb is never skipped.  Overflowing distances
+// (no finite margin) keep the box.
+SHN_D bool box_meets(V3 o, V3 cr, float4 mn, float4 mx, float tb) {
+  const float x1 = (mn.x - o.x) * cr.x, x2 = (mx.x - o.x) * cr.x;
+  const float y1 = (mn.y - o.y) * cr.y, y2 = (mx.y - o.y) * cr.y;
+  const float z1 = (mn.z - o.z) * cr.z, z2 = (mx.z - o.z) * cr.z;
+  const float tn = fmaxf(fmaxf(fminf(x1, x2), fminf(y1, y2)), fminf(z1, z2));
+  const float tf = fminf(fminf(fmaxf(x1, x2), fmaxf(y1, y2)), fmaxf(z1, z2));
+  const float m = (fabsf(tn) + fabsf(tf)) * 0x1p-8f + 1e-30f;
+  if (!(m < INFINITY)) return true;
+  return tn - m <= tf + m && tf + m >= 0.f && tn - m <= tb;
+}
+
+// Number of references of block k inside [b, e).
+SHN_D uint32_t block_refs(uint32_t k, uint32_t b, uint32_t e) {
+  return min(e, 32u * k + 32u) - max(b, 32u * k);
+}
 
 enum : uint32_t { ST_DONE = 0, ST_TOP = 1, ST_LEAF = 2, ST_LEAF_TESTED = 3, ST_TOP_NEXT = 4, ST_U_TESTED = 5 };
 
@@ -46,7 +83,7 @@ struct Lane {
   float Sx, Sy, Sz;
   uint32_t perm;          // kx | ky << 2 | kz << 4
   float tbest;
-  uint32_t best;          // reference index of the best hit, kMiss if none
+  uint32_t best;          // triangle id of the best hit, kMiss if none
   V3 cell, tMax;
   float tEntry;
   int vis, cap;
@@ -296,8 +333,10 @@ SHN_D bool wt_test_p(V3 org, float Sx, float Sy, float Sz, float4 p0, float4 p1,
 }
 
 // Whole warp tests references [b, e) against one (warp-uniform) ray.
-// Closest: returns the packed argmin key (t bits << 32 | ref) in every lane,
-// or ~0 when nothing beats tbest.  Any: returns a hit ref or ~0.
+// Closest: returns the packed argmin key (t bits << 32 | triangle id) in every
+// lane, or ~0 when nothing beats tbest.  Any: returns a hit's key or ~0.  A
+// lane's candidate must beat tbest strictly and may tie the lane's running
+// minimum (the least (t, id) wins, as in test_range).
 // L2 latency is covered by the other resident warps: the kernels that run
 // this engine are limited to 64 registers (8 blocks of 128 threads per SM),
 // which measured faster than staging the next chunk in registers or in
@@ -328,13 +367,19 @@ SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz,
         c2 = __ldg(q2 + 32);
       }
       float t;
-      if (it < e && wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, a0, a1, a2, kEps, tb, t)) {
-        tb = t;
-        key = ((uint64_t)__float_as_uint(t) << 32) | it;
+      if (it < e && wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, a0, a1, a2, kEps, key == ~0ull ? tb : next_up(tb), t)) {
+        const uint64_t c = ((uint64_t)__float_as_uint(t) << 32) | __float_as_uint(a0.w);
+        if (c < key) {
+          key = c;
+          tb = t;
+        }
       }
-      if (has2 && wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, c0, c1, c2, kEps, tb, t)) {
-        tb = t;
-        key = ((uint64_t)__float_as_uint(t) << 32) | it2;
+      if (has2 && wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, c0, c1, c2, kEps, key == ~0ull ? tb : next_up(tb), t)) {
+        const uint64_t c = ((uint64_t)__float_as_uint(t) << 32) | __float_as_uint(c0.w);
+        if (c < key) {
+          key = c;
+          tb = t;
+        }
       }
     }
   }
@@ -348,9 +393,12 @@ SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz,
       const float4 p1 = __ldg(q1);
       const float4 p2 = __ldg(q2);
       float t;
-      if (wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, p0, p1, p2, kEps, tb, t)) {
-        tb = t;
-        key = ((uint64_t)__float_as_uint(t) << 32) | it;
+      if (wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, p0, p1, p2, kEps, key == ~0ull ? tb : next_up(tb), t)) {
+        const uint64_t c = ((uint64_t)__float_as_uint(t) << 32) | __float_as_uint(p0.w);
+        if (c < key) {
+          key = c;
+          tb = t;
+        }
         hit = true;
       }
     }
@@ -368,16 +416,104 @@ SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz,
   return key;
 }
 
+// warp_range_p on a grid with block boxes: the blocks of 32 references that
+// overlap [b, e) are visited in order, 1024 at a time; a block whose box the
+// ray's segment (0, best so far] cannot meet (box_meets), or whose 1024-block
+// box it cannot meet, is skipped.  Every triangle the ray can hit below the
+// bound is in a visited block, so the result is that of warp_range_p.  Closest
+// hit takes two blocks per step (one reference of each per lane); any hit
+// stops after the first block holding a hit.  tests counts the references
+// tested.
+template <bool ANY, int KX, int KY, int KZ>
+SHN_D uint64_t warp_range_cull_p(const Refs& G, V3 org, V3 cr, float Sx, float Sy, float Sz, float tbest,
+                                 uint32_t b, uint32_t e, uint32_t& tests) {
+  const int lane = threadIdx.x & 31;
+  uint64_t key = ~0ull;
+  float tb = tbest;
+  const uint32_t kb = b >> 5, ke = (e - 1) >> 5;
+  uint32_t ntest = 0;
+  bool done = false;
+  for (uint32_t s = kb >> 5; s <= (ke >> 5) && !done; ++s) {
+    uint64_t wk = key;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const uint64_t other = __shfl_xor_sync(0xFFFFFFFFu, wk, o);
+      wk = other < wk ? other : wk;
+    }
+    const float tw = wk == ~0ull ? tbest : __uint_as_float((uint32_t)(wk >> 32));
+    if (!box_meets(org, cr, __ldg(G.sbox + 2 * (size_t)s), __ldg(G.sbox + 2 * (size_t)s + 1), tw)) continue;
+    const uint32_t k = 32u * s + lane;
+    const bool need = k >= kb && k <= ke &&
+                      box_meets(org, cr, __ldg(G.cbox + 2 * (size_t)k), __ldg(G.cbox + 2 * (size_t)k + 1), tw);
+    uint32_t m = __ballot_sync(0xFFFFFFFFu, need);
+    while (m) {
+      const uint32_t k1 = 32u * s + (uint32_t)(__ffs(m) - 1);
+      m &= m - 1;
+      uint32_t k2 = ~0u;
+      if (!ANY && m) {
+        k2 = 32u * s + (uint32_t)(__ffs(m) - 1);
+        m &= m - 1;
+      }
+      ntest += block_refs(k1, b, e) + (k2 != ~0u ? block_refs(k2, b, e) : 0u);
+      const uint32_t it = 32u * k1 + lane, it2 = 32u * k2 + lane;
+      const bool ok = it >= b && it < e;
+      const bool ok2 = !ANY && k2 != ~0u && it2 >= b && it2 < e;
+      bool hit = false;
+      float t;
+      if (ok) {
+        const float4 p0 = __ldg(G.rv0 + it), p1 = __ldg(G.rv1 + it), p2 = __ldg(G.rv2 + it);
+        if (wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, p0, p1, p2, kEps, key == ~0ull ? tb : next_up(tb), t)) {
+          const uint64_t c = ((uint64_t)__float_as_uint(t) << 32) | __float_as_uint(p0.w);
+          if (c < key) {
+            key = c;
+            tb = t;
+          }
+          hit = true;
+        }
+      }
+      if (ok2) {
+        const float4 p0 = __ldg(G.rv0 + it2), p1 = __ldg(G.rv1 + it2), p2 = __ldg(G.rv2 + it2);
+        if (wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, p0, p1, p2, kEps, key == ~0ull ? tb : next_up(tb), t)) {
+          const uint64_t c = ((uint64_t)__float_as_uint(t) << 32) | __float_as_uint(p0.w);
+          if (c < key) {
+            key = c;
+            tb = t;
+          }
+        }
+      }
+      if (ANY && __any_sync(0xFFFFFFFFu, hit)) {
+        done = true;
+        break;
+      }
+    }
+  }
+  tests += ntest;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint64_t other = __shfl_xor_sync(0xFFFFFFFFu, key, o);
+    key = other < key ? other : key;
+  }
+  return key;
+}
+
+template <bool ANY, int KX, int KY, int KZ>
+SHN_D uint64_t warp_range_q(const Refs& G, V3 org, V3 rcp, float Sx, float Sy, float Sz, float tbest,
+                            uint32_t b, uint32_t e, uint32_t& tests) {
+  if (G.cbox && e - b > kCullMin)
+    return warp_range_cull_p<ANY, KX, KY, KZ>(G, org, cull_rcp(rcp), Sx, Sy, Sz, tbest, b, e, tests);
+  return warp_range_p<ANY, KX, KY, KZ>(G, org, Sx, Sy, Sz, tbest, b, e, tests);
+}
+
 template <bool ANY>
-SHN_D uint64_t warp_range(const Refs& G, uint32_t perm, V3 org, float Sx, float Sy, float Sz,
+SHN_D uint64_t warp_range(const Refs& G, uint32_t perm, V3 org, V3 rcp, float Sx, float Sy, float Sz,
                           float tbest, uint32_t b, uint32_t e, uint32_t& tests) {
   switch (perm) {
-    case (1u | 2u << 2 | 0u << 4): return warp_range_p<ANY, 1, 2, 0>(G, org, Sx, Sy, Sz, tbest, b, e, tests);
-    case (2u | 1u << 2 | 0u << 4): return warp_range_p<ANY, 2, 1, 0>(G, org, Sx, Sy, Sz, tbest, b, e, tests);
-    case (2u | 0u << 2 | 1u << 4): return warp_range_p<ANY, 2, 0, 1>(G, org, Sx, Sy, Sz, tbest, b, e, tests);
-    case (0u | 2u << 2 | 1u << 4): return warp_range_p<ANY, 0, 2, 1>(G, org, Sx, Sy, Sz, tbest, b, e, tests);
-    case (0u | 1u << 2 | 2u << 4): return warp_range_p<ANY, 0, 1, 2>(G, org, Sx, Sy, Sz, tbest, b, e, tests);
-    default:                        return warp_range_p<ANY, 1, 0, 2>(G, org, Sx, Sy, Sz, tbest, b, e, tests);
+    case (1u | 2u << 2 | 0u << 4): return warp_range_q<ANY, 1, 2, 0>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests);
+    case (2u | 1u << 2 | 0u << 4): return warp_range_q<ANY, 2, 1, 0>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests);
+    case (2u | 0u << 2 | 1u << 4): return warp_range_q<ANY, 2, 0, 1>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests);
+    case (0u | 2u << 2 | 1u << 4): return warp_range_q<ANY, 0, 2, 1>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests);
+    case (0u | 1u << 2 | 2u << 4): return warp_range_q<ANY, 0, 1, 2>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests);
+    default:                        return warp_range_q<ANY, 1, 0, 2>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests);
   }
 }
 
@@ -445,7 +581,7 @@ SHN_D void group_range_p(const Refs& G, const LaneG* park, unsigned long long* g
       const bool hit =
           ok && (SAME ? wt_test_t<KX, KY, KZ>(A, B, C, ra.w, rb.x, rb.y, kEps, bound, t)
                       : wt_test_p<KX, KY, KZ>(mk(ra.x, ra.y, ra.z), ra.w, rb.x, rb.y, p0, p1, p2, kEps, bound, t));
-      unsigned long long cand = hit ? (((unsigned long long)__float_as_uint(t) << 32) | it) : ~0ull;
+      unsigned long long cand = hit ? (((unsigned long long)__float_as_uint(t) << 32) | __float_as_uint(p0.w)) : ~0ull;
       if (!ANY) {
         float t2;
         const bool hit2 =
@@ -453,7 +589,7 @@ SHN_D void group_range_p(const Refs& G, const LaneG* park, unsigned long long* g
                          : wt_test_p<KX, KY, KZ>(mk(ra.x, ra.y, ra.z), ra.w, rb.x, rb.y, c0, c1, c2, kEps, bound,
                                                  t2));
         if (hit2) {
-          const unsigned long long c2k = ((unsigned long long)__float_as_uint(t2) << 32) | it2;
+          const unsigned long long c2k = ((unsigned long long)__float_as_uint(t2) << 32) | __float_as_uint(c0.w);
           cand = c2k < cand ? c2k : cand;
         }
       }
@@ -469,16 +605,108 @@ SHN_D void group_range_p(const Refs& G, const LaneG* park, unsigned long long* g
   __syncwarp();
 }
 
+// group_range_p on a grid with block boxes: per 1024-reference super-block,
+// each lane tests its own ray against the super-block's box; then each lane
+// takes one block of the super-block and tests its box against every ray
+// still in, giving per block the set of rays that must test it; a block is
+// loaded once for those rays.  Skipped blocks hold no triangle a ray can hit
+// below its bound, so the keys are those of group_range_p.  gend[r] = b +
+// number of references ray r tested.
+template <int KX, int KY, int KZ, bool SAME, bool ANY>
+SHN_D void group_cull_p(const Refs& G, const LaneG* park, unsigned long long* gkey, uint32_t* gend,
+                        uint32_t gmask, uint32_t b, uint32_t e) {
+  const int lane = threadIdx.x & 31;
+  uint32_t live = gmask;
+  const uint32_t kb = b >> 5, ke = (e - 1) >> 5;
+  const V3 o0 = park[__ffs(gmask) - 1].org;
+  const bool mine = (gmask >> lane) & 1u;
+  const V3 myo = park[lane].org;
+  const V3 mycr = cull_rcp(park[lane].rcp);
+  const float mytb0 = park[lane].tbest;
+  uint32_t mycount = 0;
+  for (uint32_t s = kb >> 5; s <= (ke >> 5) && live; ++s) {
+    bool in = false;
+    if (mine && ((live >> lane) & 1u)) {
+      const unsigned long long k = *reinterpret_cast<volatile const unsigned long long*>(gkey + lane);
+      const float tb = k == ~0ull ? mytb0 : __uint_as_float((uint32_t)(k >> 32));
+      in = box_meets(myo, mycr, __ldg(G.sbox + 2 * (size_t)s), __ldg(G.sbox + 2 * (size_t)s + 1), tb);
+    }
+    const uint32_t rs = __ballot_sync(0xFFFFFFFFu, in);
+    if (!rs) continue;
+    const uint32_t kl = 32u * s + lane;
+    const bool kval = kl >= kb && kl <= ke;
+    float4 bmn = make_float4(0.f, 0.f, 0.f, 0.f), bmx = bmn;
+    if (kval) {
+      bmn = __ldg(G.cbox + 2 * (size_t)kl);
+      bmx = __ldg(G.cbox + 2 * (size_t)kl + 1);
+    }
+    uint32_t need = 0;  // rays that must test block kl
+    for (uint32_t m = rs; m; m &= m - 1) {
+      const int r = __ffs(m) - 1;
+      const unsigned long long k = *reinterpret_cast<volatile const unsigned long long*>(gkey + r);
+      const float tb = k == ~0ull ? park[r].tbest : __uint_as_float((uint32_t)(k >> 32));
+      if (kval && box_meets(park[r].org, cull_rcp(park[r].rcp), bmn, bmx, tb)) need |= 1u << r;
+    }
+    uint32_t U = __ballot_sync(0xFFFFFFFFu, need != 0u);
+    while (U && live) {
+      const int bl = __ffs(U) - 1;
+      U &= U - 1;
+      const uint32_t rays = __shfl_sync(0xFFFFFFFFu, need, bl) & live;
+      if (!rays) continue;
+      const uint32_t kk = 32u * s + (uint32_t)bl;
+      if ((rays >> lane) & 1u) mycount += block_refs(kk, b, e);
+      const uint32_t it = 32u * kk + lane;
+      const bool ok = it >= b && it < e;
+      float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0, p2 = p0;
+      if (ok) {
+        p0 = __ldg(G.rv0 + it);
+        p1 = __ldg(G.rv1 + it);
+        p2 = __ldg(G.rv2 + it);
+      }
+      V3 A, B, C;
+      if (SAME) {
+        A = sub(f4v(p0), o0);
+        B = sub(f4v(p1), o0);
+        C = sub(f4v(p2), o0);
+      }
+      for (uint32_t m = rays; m; m &= m - 1) {
+        const int r = __ffs(m) - 1;
+        const float4 ra = *reinterpret_cast<const float4*>(&park[r].org);  // org, Sx
+        const float4 rb = *reinterpret_cast<const float4*>(&park[r].Sy);   // Sy, Sz, perm, tbest
+        const unsigned long long k = *reinterpret_cast<volatile const unsigned long long*>(gkey + r);
+        const float bound = k == ~0ull ? rb.w : __uint_as_float((uint32_t)(k >> 32) + 1u);
+        float t;
+        const bool hit =
+            ok && (SAME ? wt_test_t<KX, KY, KZ>(A, B, C, ra.w, rb.x, rb.y, kEps, bound, t)
+                        : wt_test_p<KX, KY, KZ>(mk(ra.x, ra.y, ra.z), ra.w, rb.x, rb.y, p0, p1, p2, kEps, bound, t));
+        if (hit) atomicMin(gkey + r, ((unsigned long long)__float_as_uint(t) << 32) | __float_as_uint(p0.w));
+        if (ANY) {
+          if (__any_sync(0xFFFFFFFFu, hit)) live &= ~(1u << r);
+        }
+      }
+    }
+  }
+  if (mine) gend[lane] = b + mycount;
+  __syncwarp();
+}
+
+template <int KX, int KY, int KZ, bool SAME, bool ANY>
+SHN_D void group_range_q(const Refs& G, const LaneG* park, unsigned long long* gkey, uint32_t* gend,
+                         uint32_t gmask, uint32_t b, uint32_t e) {
+  if (G.cbox && e - b > kCullMin) group_cull_p<KX, KY, KZ, SAME, ANY>(G, park, gkey, gend, gmask, b, e);
+  else group_range_p<KX, KY, KZ, SAME, ANY>(G, park, gkey, gend, gmask, b, e);
+}
+
 template <bool SAME, bool ANY>
 SHN_D void group_range_s(const Refs& G, uint32_t perm, const LaneG* park, unsigned long long* gkey,
                          uint32_t* gend, uint32_t gmask, uint32_t b, uint32_t e) {
   switch (perm) {
-    case (1u | 2u << 2 | 0u << 4): group_range_p<1, 2, 0, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
-    case (2u | 1u << 2 | 0u << 4): group_range_p<2, 1, 0, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
-    case (2u | 0u << 2 | 1u << 4): group_range_p<2, 0, 1, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
-    case (0u | 2u << 2 | 1u << 4): group_range_p<0, 2, 1, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
-    case (0u | 1u << 2 | 2u << 4): group_range_p<0, 1, 2, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
-    default:                        group_range_p<1, 0, 2, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
+    case (1u | 2u << 2 | 0u << 4): group_range_q<1, 2, 0, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
+    case (2u | 1u << 2 | 0u << 4): group_range_q<2, 1, 0, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
+    case (2u | 0u << 2 | 1u << 4): group_range_q<2, 0, 1, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
+    case (0u | 2u << 2 | 1u << 4): group_range_q<0, 2, 1, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
+    case (0u | 1u << 2 | 2u << 4): group_range_q<0, 1, 2, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
+    default:                        group_range_q<1, 0, 2, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
   }
 }
 
@@ -509,34 +737,41 @@ SHN_D void group_range(const Refs& G, uint32_t perm, const LaneG* park, unsigned
 template <bool ANY, class LT>
 SHN_D void lane_range(const Refs& G, LT& L, uint32_t& tests) {
   const RayWT w = lane_ray(L);
+  const float t0 = L.tbest;
+  bool found = false;
   for (uint32_t it = L.b; it < L.e; ++it) {
     tests++;
     const float4 p0 = __ldg(G.rv0 + it);
     const float4 p1 = __ldg(G.rv1 + it);
     const float4 p2 = __ldg(G.rv2 + it);
     float t, u, v;
-    if (wt_test(w, p0, p1, p2, kEps, L.tbest, t, u, v)) {
-      L.tbest = t;
-      L.best = it;
+    if (wt_test(w, p0, p1, p2, kEps, found ? next_up(L.tbest) : t0, t, u, v)) {
+      const uint32_t id = __float_as_uint(p0.w);
+      if (!found || t < L.tbest || id < L.best) {
+        L.tbest = t;
+        L.best = id;
+        found = true;
+      }
       if (ANY || L.anyhit) return;
     }
   }
 }
 
 // Final hit record of a lane: triangle id and barycentrics of the best
-// reference, recomputed with the same arithmetic.
+// triangle, recomputed with the same arithmetic from the scene's record.
 template <class LT>
 SHN_D void lane_result(const Refs& G, const LT& L, Hit& h) {
   h.t = L.tbest;
   h.tri = kMiss;
   h.u = h.v = 0.f;
   if (L.best == kMiss) return;
-  const float4 p0 = __ldg(G.rv0 + L.best);
-  const float4 p1 = __ldg(G.rv1 + L.best);
-  const float4 p2 = __ldg(G.rv2 + L.best);
+  const float4* rec = G.src + 3 * (size_t)L.best;
+  const float4 p0 = __ldg(rec);
+  const float4 p1 = __ldg(rec + 1);
+  const float4 p2 = __ldg(rec + 2);
   float t, u, v;
   wt_test(lane_ray(L), p0, p1, p2, kEps, INFINITY, t, u, v);
-  h.tri = __float_as_uint(p0.w);
+  h.tri = L.best;
   h.u = u;
   h.v = v;
 }
@@ -641,8 +876,9 @@ SHN_D void warp_trace_acc(const Acc& acc, uint32_t n, uint32_t* counter, Src&& s
         const uint32_t b = Lj.b, e = Lj.e;
         const uint32_t aj = Lj.anyhit;
         uint32_t wt = 0;
-        const uint64_t key = (ANY || aj) ? warp_range<true>(R, perm, org, Sx, Sy, Sz, tb, b, e, wt)
-                                         : warp_range<false>(R, perm, org, Sx, Sy, Sz, tb, b, e, wt);
+        const V3 rcp = Lj.rcp;
+        const uint64_t key = (ANY || aj) ? warp_range<true>(R, perm, org, rcp, Sx, Sy, Sz, tb, b, e, wt)
+                                         : warp_range<false>(R, perm, org, rcp, Sx, Sy, Sz, tb, b, e, wt);
         if (lane == j) {
           tests += wt;
           if (key != ~0ull) {
