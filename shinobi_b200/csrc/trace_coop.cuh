@@ -289,6 +289,13 @@ SHN_D bool lane_advance(const Geom& g, const uint2* __restrict__ cells, const ui
 }
 
 // ---- watertight test with a compile-time axis permutation ---------------------
+// Component K of v; K == 3: component k, chosen at run time (one copy of the
+// code for every axis permutation, for kernels whose rays take all six).
+template <int K>
+SHN_D float pget(V3 v, uint32_t k) {
+  return K == 0 ? v.x : (K == 1 ? v.y : (K == 2 ? v.z : sel((int)k, v)));
+}
+
 template <int K>
 SHN_D float cget(V3 v) {
   return K == 0 ? v.x : (K == 1 ? v.y : v.z);
@@ -296,14 +303,16 @@ SHN_D float cget(V3 v) {
 
 // The test on vertices already translated by the ray origin.
 template <int KX, int KY, int KZ>
-SHN_D bool wt_test_t(V3 A, V3 B, V3 C, float Sx, float Sy, float Sz, float tmin, float tbest, float& t) {
-  const float Akz = cget<KZ>(A), Bkz = cget<KZ>(B), Ckz = cget<KZ>(C);
-  const float Ax = __fmaf_rn(-Sx, Akz, cget<KX>(A));
-  const float Ay = __fmaf_rn(-Sy, Akz, cget<KY>(A));
-  const float Bx = __fmaf_rn(-Sx, Bkz, cget<KX>(B));
-  const float By = __fmaf_rn(-Sy, Bkz, cget<KY>(B));
-  const float Cx = __fmaf_rn(-Sx, Ckz, cget<KX>(C));
-  const float Cy = __fmaf_rn(-Sy, Ckz, cget<KY>(C));
+SHN_D bool wt_test_t(V3 A, V3 B, V3 C, float Sx, float Sy, float Sz, float tmin, float tbest, float& t,
+                     uint32_t perm) {
+  const uint32_t kx = perm & 3u, ky = (perm >> 2) & 3u, kz = (perm >> 4) & 3u;
+  const float Akz = pget<KZ>(A, kz), Bkz = pget<KZ>(B, kz), Ckz = pget<KZ>(C, kz);
+  const float Ax = __fmaf_rn(-Sx, Akz, pget<KX>(A, kx));
+  const float Ay = __fmaf_rn(-Sy, Akz, pget<KY>(A, ky));
+  const float Bx = __fmaf_rn(-Sx, Bkz, pget<KX>(B, kx));
+  const float By = __fmaf_rn(-Sy, Bkz, pget<KY>(B, ky));
+  const float Cx = __fmaf_rn(-Sx, Ckz, pget<KX>(C, kx));
+  const float Cy = __fmaf_rn(-Sy, Ckz, pget<KY>(C, ky));
   float U = __fmaf_rn(Cx, By, -(Cy * Bx));
   float V = __fmaf_rn(Ax, Cy, -(Ay * Cx));
   float W = __fmaf_rn(Bx, Ay, -(By * Ax));
@@ -327,9 +336,9 @@ SHN_D bool wt_test_t(V3 A, V3 B, V3 C, float Sx, float Sy, float Sz, float tmin,
 
 template <int KX, int KY, int KZ>
 SHN_D bool wt_test_p(V3 org, float Sx, float Sy, float Sz, float4 p0, float4 p1, float4 p2,
-                     float tmin, float tbest, float& t) {
+                     float tmin, float tbest, float& t, uint32_t perm) {
   return wt_test_t<KX, KY, KZ>(sub(f4v(p0), org), sub(f4v(p1), org), sub(f4v(p2), org), Sx, Sy, Sz, tmin,
-                               tbest, t);
+                               tbest, t, perm);
 }
 
 // Whole warp tests references [b, e) against one (warp-uniform) ray.
@@ -343,7 +352,7 @@ SHN_D bool wt_test_p(V3 org, float Sx, float Sy, float Sz, float4 p0, float4 p1,
 // shared memory (cp.async) at lower occupancy.
 template <bool ANY, int KX, int KY, int KZ>
 SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz, float tbest,
-                            uint32_t b, uint32_t e, uint32_t& tests) {
+                            uint32_t b, uint32_t e, uint32_t& tests, uint32_t perm) {
   const int lane = threadIdx.x & 31;
   uint64_t key = ~0ull;
   float tb = tbest;
@@ -367,14 +376,14 @@ SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz,
         c2 = __ldg(q2 + 32);
       }
       float t;
-      if (it < e && wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, a0, a1, a2, kEps, key == ~0ull ? tb : next_up(tb), t)) {
+      if (it < e && wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, a0, a1, a2, kEps, key == ~0ull ? tb : next_up(tb), t, perm)) {
         const uint64_t c = ((uint64_t)__float_as_uint(t) << 32) | __float_as_uint(a0.w);
         if (c < key) {
           key = c;
           tb = t;
         }
       }
-      if (has2 && wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, c0, c1, c2, kEps, key == ~0ull ? tb : next_up(tb), t)) {
+      if (has2 && wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, c0, c1, c2, kEps, key == ~0ull ? tb : next_up(tb), t, perm)) {
         const uint64_t c = ((uint64_t)__float_as_uint(t) << 32) | __float_as_uint(c0.w);
         if (c < key) {
           key = c;
@@ -393,7 +402,7 @@ SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz,
       const float4 p1 = __ldg(q1);
       const float4 p2 = __ldg(q2);
       float t;
-      if (wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, p0, p1, p2, kEps, key == ~0ull ? tb : next_up(tb), t)) {
+      if (wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, p0, p1, p2, kEps, key == ~0ull ? tb : next_up(tb), t, perm)) {
         const uint64_t c = ((uint64_t)__float_as_uint(t) << 32) | __float_as_uint(p0.w);
         if (c < key) {
           key = c;
@@ -426,7 +435,7 @@ SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz,
 // tested.
 template <bool ANY, int KX, int KY, int KZ>
 SHN_D uint64_t warp_range_cull_p(const Refs& G, V3 org, V3 cr, float Sx, float Sy, float Sz, float tbest,
-                                 uint32_t b, uint32_t e, uint32_t& tests) {
+                                 uint32_t b, uint32_t e, uint32_t& tests, uint32_t perm) {
   const int lane = threadIdx.x & 31;
   uint64_t key = ~0ull;
   float tb = tbest;
@@ -462,7 +471,7 @@ SHN_D uint64_t warp_range_cull_p(const Refs& G, V3 org, V3 cr, float Sx, float S
       float t;
       if (ok) {
         const float4 p0 = __ldg(G.rv0 + it), p1 = __ldg(G.rv1 + it), p2 = __ldg(G.rv2 + it);
-        if (wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, p0, p1, p2, kEps, key == ~0ull ? tb : next_up(tb), t)) {
+        if (wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, p0, p1, p2, kEps, key == ~0ull ? tb : next_up(tb), t, perm)) {
           const uint64_t c = ((uint64_t)__float_as_uint(t) << 32) | __float_as_uint(p0.w);
           if (c < key) {
             key = c;
@@ -473,7 +482,7 @@ SHN_D uint64_t warp_range_cull_p(const Refs& G, V3 org, V3 cr, float Sx, float S
       }
       if (ok2) {
         const float4 p0 = __ldg(G.rv0 + it2), p1 = __ldg(G.rv1 + it2), p2 = __ldg(G.rv2 + it2);
-        if (wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, p0, p1, p2, kEps, key == ~0ull ? tb : next_up(tb), t)) {
+        if (wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, p0, p1, p2, kEps, key == ~0ull ? tb : next_up(tb), t, perm)) {
           const uint64_t c = ((uint64_t)__float_as_uint(t) << 32) | __float_as_uint(p0.w);
           if (c < key) {
             key = c;
@@ -498,22 +507,24 @@ SHN_D uint64_t warp_range_cull_p(const Refs& G, V3 org, V3 cr, float Sx, float S
 
 template <bool ANY, int KX, int KY, int KZ>
 SHN_D uint64_t warp_range_q(const Refs& G, V3 org, V3 rcp, float Sx, float Sy, float Sz, float tbest,
-                            uint32_t b, uint32_t e, uint32_t& tests) {
+                            uint32_t b, uint32_t e, uint32_t& tests, uint32_t perm) {
   if (G.cbox && e - b > kCullMin)
-    return warp_range_cull_p<ANY, KX, KY, KZ>(G, org, cull_rcp(rcp), Sx, Sy, Sz, tbest, b, e, tests);
-  return warp_range_p<ANY, KX, KY, KZ>(G, org, Sx, Sy, Sz, tbest, b, e, tests);
+    return warp_range_cull_p<ANY, KX, KY, KZ>(G, org, cull_rcp(rcp), Sx, Sy, Sz, tbest, b, e, tests, perm);
+  return warp_range_p<ANY, KX, KY, KZ>(G, org, Sx, Sy, Sz, tbest, b, e, tests, perm);
 }
 
 template <bool ANY>
 SHN_D uint64_t warp_range(const Refs& G, uint32_t perm, V3 org, V3 rcp, float Sx, float Sy, float Sz,
                           float tbest, uint32_t b, uint32_t e, uint32_t& tests) {
+  // any-hit kernels: one copy with the permutation chosen at run time
+  if (ANY) return warp_range_q<ANY, 3, 3, 3>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
   switch (perm) {
-    case (1u | 2u << 2 | 0u << 4): return warp_range_q<ANY, 1, 2, 0>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests);
-    case (2u | 1u << 2 | 0u << 4): return warp_range_q<ANY, 2, 1, 0>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests);
-    case (2u | 0u << 2 | 1u << 4): return warp_range_q<ANY, 2, 0, 1>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests);
-    case (0u | 2u << 2 | 1u << 4): return warp_range_q<ANY, 0, 2, 1>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests);
-    case (0u | 1u << 2 | 2u << 4): return warp_range_q<ANY, 0, 1, 2>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests);
-    default:                        return warp_range_q<ANY, 1, 0, 2>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests);
+    case (1u | 2u << 2 | 0u << 4): return warp_range_q<ANY, 1, 2, 0>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
+    case (2u | 1u << 2 | 0u << 4): return warp_range_q<ANY, 2, 1, 0>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
+    case (2u | 0u << 2 | 1u << 4): return warp_range_q<ANY, 2, 0, 1>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
+    case (0u | 2u << 2 | 1u << 4): return warp_range_q<ANY, 0, 2, 1>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
+    case (0u | 1u << 2 | 2u << 4): return warp_range_q<ANY, 0, 1, 2>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
+    default:                        return warp_range_q<ANY, 1, 0, 2>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
   }
 }
 
@@ -533,7 +544,7 @@ SHN_D uint64_t warp_range(const Refs& G, uint32_t perm, V3 org, V3 rcp, float Sx
 // once per chunk instead of once per ray (the same operations, the same bits).
 template <int KX, int KY, int KZ, bool SAME, bool ANY>
 SHN_D void group_range_p(const Refs& G, const LaneG* park, unsigned long long* gkey, uint32_t* gend,
-                         uint32_t gmask, uint32_t b, uint32_t e) {
+                         uint32_t gmask, uint32_t b, uint32_t e, uint32_t perm) {
   // closest hit: two references per lane per chunk (64-reference chunks), so a
   // ray's parameters are read once per two tests; any hit: 32-reference chunks,
   // the granularity of warp_range_p's early exit
@@ -579,15 +590,15 @@ SHN_D void group_range_p(const Refs& G, const LaneG* park, unsigned long long* g
       const float bound = k == ~0ull ? rb.w : __uint_as_float((uint32_t)(k >> 32) + 1u);
       float t;
       const bool hit =
-          ok && (SAME ? wt_test_t<KX, KY, KZ>(A, B, C, ra.w, rb.x, rb.y, kEps, bound, t)
-                      : wt_test_p<KX, KY, KZ>(mk(ra.x, ra.y, ra.z), ra.w, rb.x, rb.y, p0, p1, p2, kEps, bound, t));
+          ok && (SAME ? wt_test_t<KX, KY, KZ>(A, B, C, ra.w, rb.x, rb.y, kEps, bound, t, perm)
+                      : wt_test_p<KX, KY, KZ>(mk(ra.x, ra.y, ra.z), ra.w, rb.x, rb.y, p0, p1, p2, kEps, bound, t, perm));
       unsigned long long cand = hit ? (((unsigned long long)__float_as_uint(t) << 32) | __float_as_uint(p0.w)) : ~0ull;
       if (!ANY) {
         float t2;
         const bool hit2 =
-            ok2 && (SAME ? wt_test_t<KX, KY, KZ>(A2, B2, C2, ra.w, rb.x, rb.y, kEps, bound, t2)
+            ok2 && (SAME ? wt_test_t<KX, KY, KZ>(A2, B2, C2, ra.w, rb.x, rb.y, kEps, bound, t2, perm)
                          : wt_test_p<KX, KY, KZ>(mk(ra.x, ra.y, ra.z), ra.w, rb.x, rb.y, c0, c1, c2, kEps, bound,
-                                                 t2));
+                                                 t2, perm));
         if (hit2) {
           const unsigned long long c2k = ((unsigned long long)__float_as_uint(t2) << 32) | __float_as_uint(c0.w);
           cand = c2k < cand ? c2k : cand;
@@ -614,7 +625,7 @@ SHN_D void group_range_p(const Refs& G, const LaneG* park, unsigned long long* g
 // number of references ray r tested.
 template <int KX, int KY, int KZ, bool SAME, bool ANY>
 SHN_D void group_cull_p(const Refs& G, const LaneG* park, unsigned long long* gkey, uint32_t* gend,
-                        uint32_t gmask, uint32_t b, uint32_t e) {
+                        uint32_t gmask, uint32_t b, uint32_t e, uint32_t perm) {
   const int lane = threadIdx.x & 31;
   uint32_t live = gmask;
   const uint32_t kb = b >> 5, ke = (e - 1) >> 5;
@@ -677,8 +688,8 @@ SHN_D void group_cull_p(const Refs& G, const LaneG* park, unsigned long long* gk
         const float bound = k == ~0ull ? rb.w : __uint_as_float((uint32_t)(k >> 32) + 1u);
         float t;
         const bool hit =
-            ok && (SAME ? wt_test_t<KX, KY, KZ>(A, B, C, ra.w, rb.x, rb.y, kEps, bound, t)
-                        : wt_test_p<KX, KY, KZ>(mk(ra.x, ra.y, ra.z), ra.w, rb.x, rb.y, p0, p1, p2, kEps, bound, t));
+            ok && (SAME ? wt_test_t<KX, KY, KZ>(A, B, C, ra.w, rb.x, rb.y, kEps, bound, t, perm)
+                        : wt_test_p<KX, KY, KZ>(mk(ra.x, ra.y, ra.z), ra.w, rb.x, rb.y, p0, p1, p2, kEps, bound, t, perm));
         if (hit) atomicMin(gkey + r, ((unsigned long long)__float_as_uint(t) << 32) | __float_as_uint(p0.w));
         if (ANY) {
           if (__any_sync(0xFFFFFFFFu, hit)) live &= ~(1u << r);
@@ -692,21 +703,25 @@ SHN_D void group_cull_p(const Refs& G, const LaneG* park, unsigned long long* gk
 
 template <int KX, int KY, int KZ, bool SAME, bool ANY>
 SHN_D void group_range_q(const Refs& G, const LaneG* park, unsigned long long* gkey, uint32_t* gend,
-                         uint32_t gmask, uint32_t b, uint32_t e) {
-  if (G.cbox && e - b > kCullMin) group_cull_p<KX, KY, KZ, SAME, ANY>(G, park, gkey, gend, gmask, b, e);
-  else group_range_p<KX, KY, KZ, SAME, ANY>(G, park, gkey, gend, gmask, b, e);
+                         uint32_t gmask, uint32_t b, uint32_t e, uint32_t perm) {
+  if (G.cbox && e - b > kCullMin) group_cull_p<KX, KY, KZ, SAME, ANY>(G, park, gkey, gend, gmask, b, e, perm);
+  else group_range_p<KX, KY, KZ, SAME, ANY>(G, park, gkey, gend, gmask, b, e, perm);
 }
 
 template <bool SAME, bool ANY>
 SHN_D void group_range_s(const Refs& G, uint32_t perm, const LaneG* park, unsigned long long* gkey,
                          uint32_t* gend, uint32_t gmask, uint32_t b, uint32_t e) {
+  if (ANY) {
+    group_range_q<3, 3, 3, SAME, ANY>(G, park, gkey, gend, gmask, b, e, perm);
+    return;
+  }
   switch (perm) {
-    case (1u | 2u << 2 | 0u << 4): group_range_q<1, 2, 0, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
-    case (2u | 1u << 2 | 0u << 4): group_range_q<2, 1, 0, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
-    case (2u | 0u << 2 | 1u << 4): group_range_q<2, 0, 1, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
-    case (0u | 2u << 2 | 1u << 4): group_range_q<0, 2, 1, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
-    case (0u | 1u << 2 | 2u << 4): group_range_q<0, 1, 2, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
-    default:                        group_range_q<1, 0, 2, SAME, ANY>(G, park, gkey, gend, gmask, b, e); break;
+    case (1u | 2u << 2 | 0u << 4): group_range_q<1, 2, 0, SAME, ANY>(G, park, gkey, gend, gmask, b, e, perm); break;
+    case (2u | 1u << 2 | 0u << 4): group_range_q<2, 1, 0, SAME, ANY>(G, park, gkey, gend, gmask, b, e, perm); break;
+    case (2u | 0u << 2 | 1u << 4): group_range_q<2, 0, 1, SAME, ANY>(G, park, gkey, gend, gmask, b, e, perm); break;
+    case (0u | 2u << 2 | 1u << 4): group_range_q<0, 2, 1, SAME, ANY>(G, park, gkey, gend, gmask, b, e, perm); break;
+    case (0u | 1u << 2 | 2u << 4): group_range_q<0, 1, 2, SAME, ANY>(G, park, gkey, gend, gmask, b, e, perm); break;
+    default:                        group_range_q<1, 0, 2, SAME, ANY>(G, park, gkey, gend, gmask, b, e, perm); break;
   }
 }
 
