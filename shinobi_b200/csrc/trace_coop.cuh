@@ -198,6 +198,17 @@ SHN_D bool lane_advance(const Geom& g, const uint2* __restrict__ cells, const ui
           if (L.e > L.b) return true;
           break;
         }
+        if ((cw.y & kNotEmpty) && (cw.y & 0xFFFFFFu) == 0x010101u) {
+          // a top cell with one leaf: its leaf DDA visits that leaf and then
+          // always leaves the cell, so the range goes straight to the top step
+          const uint2 range = __ldg(leaves + cw.x);
+          steps++;
+          L.b = range.x;
+          L.e = range.y;
+          L.st = ST_TOP_NEXT;
+          if (L.e > L.b) return true;
+          break;
+        }
         if (cw.y & kNotEmpty) {
           const V3 rcp = L.rcp, org = L.org;
           const float te = L.tEntry;
