@@ -238,15 +238,36 @@ SHN_D bool lane_advance(const Geom& g, const uint2* __restrict__ cells, const ui
         break;
       }
       case ST_LEAF: {
-        L.vis2++;
-        const V3 sc = L.sc, cres = L.cres;
-        const uint32_t li = L.lb + (uint32_t)(sc.x + cres.x * sc.y + cres.x * cres.y * sc.z);
-        const uint2 range = __ldg(leaves + li);
-        steps++;
-        L.b = range.x;
-        L.e = range.y;
-        L.st = ST_LEAF_TESTED;
-        if (L.e > L.b) return true;
+        // runs of empty leaf cells are walked here, each with the step of
+        // ST_LEAF_TESTED (nothing was tested, so its any-hit exit cannot fire)
+        const float tb = L.tbest;
+        const int cap2 = (int)L.cres.x + (int)L.cres.y + (int)L.cres.z + 3;
+        while (true) {
+          L.vis2++;
+          const uint32_t li = L.lb + (uint32_t)(L.sc.x + L.cres.x * L.sc.y + L.cres.x * L.cres.y * L.sc.z);
+          const uint2 range = __ldg(leaves + li);
+          steps++;
+          if (range.y > range.x) {
+            L.b = range.x;
+            L.e = range.y;
+            L.st = ST_LEAF_TESTED;
+            return true;
+          }
+          if (!(tb > L.sMax.x || tb > L.sMax.y || tb > L.sMax.z)) {
+            L.st = ST_TOP_NEXT;
+            break;
+          }
+          const int d = min_dim(L.sMax);
+          const float rd = sel(d, L.rcp);
+          bump(L.sc, d, rd > 0.f ? 1.f : -1.f);
+          bump(L.sMax, d, sel(d, L.scs) * fabsf(rd));
+          const float cd = sel(d, L.sc);
+          const bool v2 = !(fabsf(cd - sel(d, L.cres)) < 0.1f || fabsf(cd + 1.f) < 0.1f);
+          if (!(v2 && L.vis2 < cap2)) {
+            L.st = ST_TOP_NEXT;
+            break;
+          }
+        }
         break;
       }
       case ST_LEAF_TESTED: {
