@@ -38,7 +38,6 @@ struct shn_batch {
   void* sort_ws = nullptr;
   uint2* cells = nullptr;
   uint32_t* indices = nullptr;
-  float4* rtri = nullptr;
   uint32_t* d_err = nullptr;           // [0] error bits, [1..] scratch words
   uint32_t* h_pinned = nullptr;
   uint64_t total_cells = 0;
@@ -71,6 +70,7 @@ struct BatchAcc {
 };
 
 struct BatchAccW {
+  static constexpr bool kIndirect = true;  // no reference-ordered copy: triangles through indices[]
   BatchAcc a;
   Refs r;
   SHN_D const Geom& geom(uint32_t s) const { return a.geom(s); }
@@ -157,7 +157,6 @@ void release_plan(shn_batch* b, cudaStream_t st) {
   b->keys[0] = b->keys[1] = nullptr;
   b->cells = nullptr;
   b->indices = nullptr;
-  b->rtri = nullptr;
   b->d_scenes = nullptr;
   b->d_ray_off = nullptr;
   b->ray_off_cap = 0;
@@ -221,7 +220,6 @@ shn_status plan(shn_batch* b, cudaStream_t st) {
   if (e == cudaSuccess) e = own(b, &b->sort_ws, sort_workspace_bytes(b->P), st);
   if (e == cudaSuccess) e = own(b, (void**)&b->cells, co * 8, st);
   if (e == cudaSuccess) e = own(b, (void**)&b->indices, (size_t)b->P * 4, st);
-  if (e == cudaSuccess) e = own(b, (void**)&b->rtri, (size_t)b->P * 48, st);
   if (e != cudaSuccess) return alloc_err(b, e, "batch buffers");
   b->planned = true;
   return SHN_OK;
@@ -234,16 +232,18 @@ void enqueue_build(shn_batch* b, cudaStream_t st) {
   launch_batch_emit(b->tri, b->T, b->d_tri_off, b->d_scenes, b->ns, b->offs, b->keys[0], b->P, b->d_err, st);
   b->sorted = onesweep_sort(b->keys[0], b->keys[1], b->P, 32, b->passes, b->sort_ws, b->d_err, st);
   cudaMemsetAsync(b->cells, 0, b->total_cells * 8, st);
-  launch_ranges(b->sorted, b->P, b->cells, b->indices, b->tri, b->T, b->rtri, st);
+  // no reference-ordered triangle copy: the batch's cells hold a few
+  // references each and the trace reads a reference's triangle through its
+  // id (indices[]), which measured cheaper than gathering and writing 96 bytes
+  // per reference in the build
+  launch_ranges(b->sorted, b->P, b->cells, b->indices, b->tri, b->T, nullptr, st);
 }
 
 GridView batch_view(const shn_batch* b) {
   GridView v{};
   v.kind = 0;
-  v.rv0 = b->rtri;
-  v.rv1 = b->rtri + b->P;
-  v.rv2 = b->rtri + 2 * (size_t)b->P;
   v.src = b->tri;
+  v.ridx = b->indices;
   return v;
 }
 

@@ -265,6 +265,7 @@ shn_status shn_pt_render(const shn_grid* g, const shn_scene* s, const shn_camera
     v.src = g->src_tri;
     v.cbox = g->num_blocks ? (const float4*)g->cbox.ptr : nullptr;
     v.sbox = g->num_blocks ? (const float4*)g->sbox.ptr : nullptr;
+    v.ridx = nullptr;
     return v;
   }();
 

@@ -38,6 +38,7 @@ struct ServeSeg {
 };
 
 struct ServeAcc {
+  static constexpr bool kIndirect = false;
   const ServeSeg* __restrict__ segs;
   SHN_D const Geom& geom(uint32_t s) const { return segs[s].g.g; }
   SHN_D const uint2* cells(uint32_t s) const { return segs[s].g.cells; }
@@ -292,6 +293,7 @@ void issue_launch(shn_server* s, ServeLaunch& la, int slot_index, std::unique_lo
     sg.g.src = g->src_tri;
     sg.g.cbox = g->num_blocks ? (const float4*)g->cbox.ptr : nullptr;
     sg.g.sbox = g->num_blocks ? (const float4*)g->sbox.ptr : nullptr;
+    sg.g.ridx = nullptr;
   }
   s->max_requests_per_launch = std::max<uint64_t>(s->max_requests_per_launch, la.reqs.size());
   la.busy = true;

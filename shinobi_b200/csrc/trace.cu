@@ -298,6 +298,7 @@ GridView view_of(const shn_grid* g) {
   v.src = g->src_tri;
   v.cbox = g->num_blocks ? (const float4*)g->cbox.ptr : nullptr;
   v.sbox = g->num_blocks ? (const float4*)g->sbox.ptr : nullptr;
+  v.ridx = nullptr;
   return v;
 }
 

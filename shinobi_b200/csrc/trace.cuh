@@ -33,6 +33,8 @@ struct GridView {
   // of rv*, or null (no culling)
   const float4* __restrict__ cbox;
   const float4* __restrict__ sbox;
+  // when not null: no reference-ordered copy; reference i is src[3 * ridx[i]]
+  const uint32_t* __restrict__ ridx;
 };
 
 struct Hit {

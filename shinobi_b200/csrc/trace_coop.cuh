@@ -40,8 +40,25 @@ struct Refs {
   const float4* __restrict__ src;
   const float4* __restrict__ cbox;  // block boxes (see GridView), or null
   const float4* __restrict__ sbox;
+  const uint32_t* __restrict__ ridx;  // not null: reference i is src[3 * ridx[i]] (no rv*)
 };
-SHN_D Refs refs_of(const GridView& G) { return Refs{G.rv0, G.rv1, G.rv2, G.src, G.cbox, G.sbox}; }
+SHN_D Refs refs_of(const GridView& G) { return Refs{G.rv0, G.rv1, G.rv2, G.src, G.cbox, G.sbox, G.ridx}; }
+
+// Triangle of reference i: from the reference-ordered arrays, or (IND: grids
+// that keep no reference-ordered copy) through the reference's triangle id.
+template <bool IND>
+SHN_D void ref_load(const Refs& G, uint32_t i, float4& p0, float4& p1, float4& p2) {
+  if (IND) {
+    const float4* r = G.src + 3 * (size_t)__ldg(G.ridx + i);
+    p0 = __ldg(r);
+    p1 = __ldg(r + 1);
+    p2 = __ldg(r + 2);
+  } else {
+    p0 = __ldg(G.rv0 + i);
+    p1 = __ldg(G.rv1 + i);
+    p2 = __ldg(G.rv2 + i);
+  }
+}
 
 // Ranges longer than this are tested block by block with box culling when the
 // grid has block boxes.
@@ -382,7 +399,7 @@ SHN_D bool wt_test_p(V3 org, float Sx, float Sy, float Sz, float4 p0, float4 p1,
 // this engine are limited to 64 registers (8 blocks of 128 threads per SM),
 // which measured faster than staging the next chunk in registers or in
 // shared memory (cp.async) at lower occupancy.
-template <bool ANY, int KX, int KY, int KZ>
+template <bool ANY, int KX, int KY, int KZ, bool IND>
 SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz, float tbest,
                             uint32_t b, uint32_t e, uint32_t& tests, uint32_t perm) {
   const int lane = threadIdx.x & 31;
@@ -399,13 +416,24 @@ SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz,
     // warp's argmin over (t, reference) is that of the sequential loop
     for (; base + 32 < e; base += 64, q0 += 64, q1 += 64, q2 += 64) {
       const uint32_t it = base + lane, it2 = it + 32;
-      const float4 a0 = __ldg(q0), a1 = __ldg(q1), a2 = __ldg(q2);
+      float4 a0, a1, a2;
+      if (IND) {
+        ref_load<IND>(G, it, a0, a1, a2);
+      } else {
+        a0 = __ldg(q0);
+        a1 = __ldg(q1);
+        a2 = __ldg(q2);
+      }
       const bool has2 = it2 < e;
       float4 c0 = a0, c1 = a1, c2 = a2;
       if (has2) {
-        c0 = __ldg(q0 + 32);
-        c1 = __ldg(q1 + 32);
-        c2 = __ldg(q2 + 32);
+        if (IND) {
+          ref_load<IND>(G, it2, c0, c1, c2);
+        } else {
+          c0 = __ldg(q0 + 32);
+          c1 = __ldg(q1 + 32);
+          c2 = __ldg(q2 + 32);
+        }
       }
       float t;
       if (it < e && wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, a0, a1, a2, kEps, key == ~0ull ? tb : next_up(tb), t, perm)) {
@@ -430,9 +458,14 @@ SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz,
     const uint32_t it = base + lane;
     bool hit = false;
     if (it < e) {
-      const float4 p0 = __ldg(q0);
-      const float4 p1 = __ldg(q1);
-      const float4 p2 = __ldg(q2);
+      float4 p0, p1, p2;
+      if (IND) {
+        ref_load<IND>(G, it, p0, p1, p2);
+      } else {
+        p0 = __ldg(q0);
+        p1 = __ldg(q1);
+        p2 = __ldg(q2);
+      }
       float t;
       if (wt_test_p<KX, KY, KZ>(org, Sx, Sy, Sz, p0, p1, p2, kEps, key == ~0ull ? tb : next_up(tb), t, perm)) {
         const uint64_t c = ((uint64_t)__float_as_uint(t) << 32) | __float_as_uint(p0.w);
@@ -537,26 +570,26 @@ SHN_D uint64_t warp_range_cull_p(const Refs& G, V3 org, V3 cr, float Sx, float S
   return key;
 }
 
-template <bool ANY, int KX, int KY, int KZ>
+template <bool ANY, int KX, int KY, int KZ, bool IND>
 SHN_D uint64_t warp_range_q(const Refs& G, V3 org, V3 rcp, float Sx, float Sy, float Sz, float tbest,
                             uint32_t b, uint32_t e, uint32_t& tests, uint32_t perm) {
-  if (G.cbox && e - b > kCullMin)
+  if (!IND && G.cbox && e - b > kCullMin)
     return warp_range_cull_p<ANY, KX, KY, KZ>(G, org, cull_rcp(rcp), Sx, Sy, Sz, tbest, b, e, tests, perm);
-  return warp_range_p<ANY, KX, KY, KZ>(G, org, Sx, Sy, Sz, tbest, b, e, tests, perm);
+  return warp_range_p<ANY, KX, KY, KZ, IND>(G, org, Sx, Sy, Sz, tbest, b, e, tests, perm);
 }
 
-template <bool ANY>
+template <bool ANY, bool IND>
 SHN_D uint64_t warp_range(const Refs& G, uint32_t perm, V3 org, V3 rcp, float Sx, float Sy, float Sz,
                           float tbest, uint32_t b, uint32_t e, uint32_t& tests) {
   // any-hit kernels: one copy with the permutation chosen at run time
-  if (ANY) return warp_range_q<ANY, 3, 3, 3>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
+  if (ANY) return warp_range_q<ANY, 3, 3, 3, IND>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
   switch (perm) {
-    case (1u | 2u << 2 | 0u << 4): return warp_range_q<ANY, 1, 2, 0>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
-    case (2u | 1u << 2 | 0u << 4): return warp_range_q<ANY, 2, 1, 0>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
-    case (2u | 0u << 2 | 1u << 4): return warp_range_q<ANY, 2, 0, 1>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
-    case (0u | 2u << 2 | 1u << 4): return warp_range_q<ANY, 0, 2, 1>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
-    case (0u | 1u << 2 | 2u << 4): return warp_range_q<ANY, 0, 1, 2>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
-    default:                        return warp_range_q<ANY, 1, 0, 2>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
+    case (1u | 2u << 2 | 0u << 4): return warp_range_q<ANY, 1, 2, 0, IND>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
+    case (2u | 1u << 2 | 0u << 4): return warp_range_q<ANY, 2, 1, 0, IND>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
+    case (2u | 0u << 2 | 1u << 4): return warp_range_q<ANY, 2, 0, 1, IND>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
+    case (0u | 2u << 2 | 1u << 4): return warp_range_q<ANY, 0, 2, 1, IND>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
+    case (0u | 1u << 2 | 2u << 4): return warp_range_q<ANY, 0, 1, 2, IND>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
+    default:                        return warp_range_q<ANY, 1, 0, 2, IND>(G, org, rcp, Sx, Sy, Sz, tbest, b, e, tests, perm);
   }
 }
 
@@ -781,16 +814,15 @@ SHN_D void group_range(const Refs& G, uint32_t perm, const LaneG* park, unsigned
 }
 
 // Per-lane test of its own (small) range with the generic watertight test.
-template <bool ANY, class LT>
+template <bool ANY, bool IND, class LT>
 SHN_D void lane_range(const Refs& G, LT& L, uint32_t& tests) {
   const RayWT w = lane_ray(L);
   const float t0 = L.tbest;
   bool found = false;
   for (uint32_t it = L.b; it < L.e; ++it) {
     tests++;
-    const float4 p0 = __ldg(G.rv0 + it);
-    const float4 p1 = __ldg(G.rv1 + it);
-    const float4 p2 = __ldg(G.rv2 + it);
+    float4 p0, p1, p2;
+    ref_load<IND>(G, it, p0, p1, p2);
     float t, u, v;
     if (wt_test(w, p0, p1, p2, kEps, found ? next_up(L.tbest) : t0, t, u, v)) {
       const uint32_t id = __float_as_uint(p0.w);
@@ -832,6 +864,9 @@ SHN_D void lane_result(const Refs& G, const LT& L, Hit& h) {
 template <int KIND, bool ANY, bool GROUP = true, class Acc, class Src, class Sink>
 SHN_D void warp_trace_acc(const Acc& acc, uint32_t n, uint32_t* counter, Src&& src, Sink&& sink) {
   using LaneT = typename std::conditional<GROUP, LaneG, Lane>::type;
+  // grids without a reference-ordered triangle copy (batched scenes)
+  constexpr bool IND = Acc::kIndirect;
+  static_assert(!(GROUP && IND), "grouped range tests read the reference-ordered copy");
   __shared__ LaneT lane_park[kCoopBlock];
   __shared__ unsigned long long grp_key[kCoopBlock];
   __shared__ uint32_t grp_end[kCoopBlock];
@@ -881,7 +916,7 @@ SHN_D void warp_trace_acc(const Acc& acc, uint32_t n, uint32_t* counter, Src&& s
       continue;
     }
     const bool big = pending && (L.e - L.b > kCoopThreshold);
-    if (pending && !big) lane_range<ANY>(acc.refs(scene), L, tests);
+    if (pending && !big) lane_range<ANY, IND>(acc.refs(scene), L, tests);
     uint32_t bmask = __ballot_sync(0xFFFFFFFFu, big);
     if (bmask) {
       // The lanes' traversal state waits in shared memory while the warp tests
@@ -924,8 +959,8 @@ SHN_D void warp_trace_acc(const Acc& acc, uint32_t n, uint32_t* counter, Src&& s
         const uint32_t aj = Lj.anyhit;
         uint32_t wt = 0;
         const V3 rcp = Lj.rcp;
-        const uint64_t key = (ANY || aj) ? warp_range<true>(R, perm, org, rcp, Sx, Sy, Sz, tb, b, e, wt)
-                                         : warp_range<false>(R, perm, org, rcp, Sx, Sy, Sz, tb, b, e, wt);
+        const uint64_t key = (ANY || aj) ? warp_range<true, IND>(R, perm, org, rcp, Sx, Sy, Sz, tb, b, e, wt)
+                                         : warp_range<false, IND>(R, perm, org, rcp, Sx, Sy, Sz, tb, b, e, wt);
         if (lane == j) {
           tests += wt;
           if (key != ~0ull) {
@@ -952,6 +987,7 @@ SHN_D void warp_trace_acc(const Acc& acc, uint32_t n, uint32_t* counter, Src&& s
 
 // Grid access of a lane: the single-grid kernels use one GridView for every lane.
 struct OneGrid {
+  static constexpr bool kIndirect = false;
   const GridView* G;
   SHN_D const Geom& geom(uint32_t) const { return G->g; }
   SHN_D const uint2* cells(uint32_t) const { return G->cells; }
