@@ -489,7 +489,7 @@ def launches_per_step(P, R, C0, L):
              + 1 + 2 + 1 + sort_launches(R, L) + 1)  # leaf cells scan, leaf count + scan, emit, sort, ranges
     # Morton order of the triangles (keys, two 4-pass sorts, second keys, permute)
     # and the boxes per 32 and per 1024 references
-    spatial = 1 + 2 * (2 + 4) + 1 + 1 + (2 if R else 0)
+    spatial = 1 + 2 * (2 + 4) + 1 + 1 + (2 if R else 0) + 3   # + the three leaf-distance passes
     return build + spatial + 1 + 3                     # primary; compact + trace + finalize (AO or shading)
 
 

@@ -322,7 +322,7 @@ shn_status shn_grid_get_info(const shn_grid* g, shn_grid_info* o) {
   o->device_bytes = g->cap_cells + g->cap_leaves + g->cap_refs + g->cap_rtri + g->offs_tri.bytes +
                     g->offs_pair.bytes + g->scan.bytes + g->top_ranges.bytes + g->keys[0].bytes +
                     g->keys[1].bytes + g->keys[2].bytes + g->sortws.bytes + g->mhi.bytes + g->perm_tri.bytes +
-                    g->cbox.bytes + g->sbox.bytes;
+                    g->cbox.bytes + g->sbox.bytes + g->ldist.bytes;
   o->build_ms = g->build_ms;
   return g->built ? SHN_OK : SHN_ERR_NOT_BUILT;
 }
@@ -337,6 +337,12 @@ shn_status shn_grid_export(const shn_grid* g, uint32_t* cells, uint32_t* leaves,
   if (e == cudaSuccess && indices && g->num_refs) e = cudaMemcpy(indices, g->indices, g->num_refs * 4, cudaMemcpyDeviceToHost);
   const uint64_t np = g->kind == SHN_GRID_TWO_LEVEL ? g->num_top_refs : g->num_refs;
   if (e == cudaSuccess && top_pairs && np) e = cudaMemcpy(top_pairs, g->top_pairs, np * 8, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && leaves && g->spatial) {
+    // empty leaves carry their distance to the nearest non-empty leaf on the
+    // device; exported, an empty leaf is [0, 0)
+    for (uint64_t i = 0; i < g->num_leaves; ++i)
+      if (leaves[2 * i] == leaves[2 * i + 1]) leaves[2 * i] = leaves[2 * i + 1] = 0;
+  }
   if (e == cudaSuccess && g->spatial) {
     // a two-level grid was built on the triangles in Morton order: the
     // references of a leaf are in that order and the pairs' low words are
@@ -370,7 +376,8 @@ void shn_grid_destroy(shn_grid* g) {
   dev_free(c, g->indices, g->cap_refs, st);
   dev_free(c, g->rtri, g->cap_rtri, st);
   DevBuf* bufs[] = {&g->offs_tri, &g->offs_pair, &g->scan,     &g->top_ranges, &g->keys[0], &g->keys[1],
-                    &g->keys[2],   &g->sortws,    &g->mhi,      &g->perm_tri,   &g->cbox,    &g->sbox};
+                    &g->keys[2],   &g->sortws,    &g->mhi,      &g->perm_tri,   &g->cbox,    &g->sbox,
+                    &g->ldist};
   for (DevBuf* b : bufs) dev_free(c, b->ptr, b->bytes, st);
   dev_free(c, g->d_err, 64, st);
   pinned_give(c, g->h_pinned);

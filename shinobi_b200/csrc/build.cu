@@ -481,6 +481,72 @@ __global__ void k_super_boxes(const float4* __restrict__ box, uint32_t nblocks, 
   }
 }
 
+// ---- distance to the nearest non-empty leaf (two-level grids) ---------------------
+// For every leaf of a top cell with a leaf grid of more than one cell: D = the
+// L-infinity distance (in leaf cells, capped at kLeafDistCap + 1) to the
+// nearest non-empty leaf of the same grid, computed as three separable min-max
+// passes (x, then y, then z).  An empty leaf stores [D, D): its range stays
+// empty, and a DDA that fetched it may take its next D - 1 steps without
+// fetching, since every cell within those steps lies closer than D.
+constexpr uint32_t kLeafDistCap = 15;
+
+// top cell owning leaf li: the last cell whose leaf offset is <= li (offsets
+// are the exclusive scan of the leaf counts, so empty cells never match last)
+SHN_D uint32_t leaf_owner(const uint2* __restrict__ cells, uint32_t C, uint32_t li) {
+  uint32_t lo = 0, hi = C;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(&cells[mid].x) <= li) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// pass: axis 0 reads occupancy from the leaves, axes 1 and 2 the previous pass
+// (the first pass finds each leaf's top cell and keeps it in owner[])
+template <int AXIS>
+__global__ void k_leaf_dist(const uint2* __restrict__ cells, uint32_t C, uint2* __restrict__ leaves, uint32_t L,
+                            uint32_t* __restrict__ owner, const uint8_t* __restrict__ din,
+                            uint8_t* __restrict__ dout) {
+  for (uint32_t li = blockIdx.x * blockDim.x + threadIdx.x; li < L; li += gridDim.x * blockDim.x) {
+    uint32_t c;
+    if (AXIS == 0) {
+      c = leaf_owner(cells, C, li);
+      owner[li] = c;
+    } else {
+      c = __ldg(owner + li);
+    }
+    const uint2 cw = __ldg(cells + c);
+    const uint32_t rx = cw.y & 0xFFu, ry = (cw.y >> 8) & 0xFFu, rz = (cw.y >> 16) & 0xFFu;
+    if (!(cw.y & kNotEmpty) || rx * ry * rz <= 1u) continue;
+    const uint32_t k = li - cw.x;
+    const uint32_t x = k % rx, y = (k / rx) % ry, z = k / (rx * ry);
+    const uint32_t pos = AXIS == 0 ? x : (AXIS == 1 ? y : z);
+    const uint32_t len = AXIS == 0 ? rx : (AXIS == 1 ? ry : rz);
+    const uint32_t stride = AXIS == 0 ? 1u : (AXIS == 1 ? rx : rx * ry);
+    uint32_t best = kLeafDistCap + 1;
+    const uint32_t lo = pos >= kLeafDistCap ? pos - kLeafDistCap : 0u;
+    const uint32_t hi = min(len - 1u, pos + kLeafDistCap);
+    for (uint32_t q = lo; q <= hi; ++q) {
+      const uint32_t j = li - pos * stride + q * stride;
+      const uint32_t dq = q > pos ? q - pos : pos - q;
+      uint32_t v;
+      if (AXIS == 0) {
+        const uint2 r = leaves[j];
+        v = r.y > r.x ? dq : kLeafDistCap + 1;
+      } else {
+        v = max(dq, (uint32_t)__ldg(din + j));
+      }
+      best = min(best, v);
+    }
+    if (AXIS < 2) {
+      dout[li] = (uint8_t)best;
+    } else {
+      const uint2 r = leaves[li];
+      if (r.y <= r.x) leaves[li] = make_uint2(best, best);
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kScanBlock) k_leaf_cells_scan(const uint2* __restrict__ top_ranges,
                                                                uint32_t C, Geom g, float lambda,
                                                                uint32_t threshold, LookbackState st,
@@ -869,6 +935,16 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   if ((rc = ensure(g, (void**)&g->rtri, &g->cap_rtri, (size_t)std::max<uint32_t>(R, 1) * 48, st))) return rc;
   cudaMemsetAsync(g->leaves, 0, (size_t)Lc * 8, st);
   if (R) k_ranges<<<range_blocks(R), kRangeBlock, 0, st>>>(sortedLeaf, R, g->leaves, g->indices, tri, g->rtri);
+  if (g->spatial && Lc) {
+    if ((rc = ensure_buf(g, g->ldist, 6 * (size_t)Lc, st))) return rc;
+    uint32_t* own = (uint32_t*)g->ldist.ptr;
+    uint8_t* d1 = (uint8_t*)(own + Lc);
+    uint8_t* d2 = d1 + Lc;
+    const int blocks = grid_for(Lc, 256, 148 * 8);
+    k_leaf_dist<0><<<blocks, 256, 0, st>>>(g->cells, (uint32_t)C, g->leaves, Lc, own, nullptr, d1);
+    k_leaf_dist<1><<<blocks, 256, 0, st>>>(g->cells, (uint32_t)C, g->leaves, Lc, own, d1, d2);
+    k_leaf_dist<2><<<blocks, 256, 0, st>>>(g->cells, (uint32_t)C, g->leaves, Lc, own, d2, nullptr);
+  }
   if (g->spatial && R) {
     const uint64_t nb = (R + 31) / 32, ns = (nb + 31) / 32;
     if ((rc = ensure_buf(g, g->cbox, nb * 32, st))) return rc;

@@ -76,7 +76,7 @@ struct shn_grid {
   // float4 (min, max) each, let the traversal skip blocks a ray cannot hit
   bool spatial = false;
   uint64_t num_blocks = 0, num_super = 0;
-  shn::DevBuf mhi, perm_tri, cbox, sbox;
+  shn::DevBuf mhi, perm_tri, cbox, sbox, ldist;
   size_t cap_cells = 0, cap_leaves = 0, cap_refs = 0, cap_rtri = 0;
   // grow-only build workspace
   shn::DevBuf offs_tri, offs_pair, scan, top_ranges, keys[3], sortws;

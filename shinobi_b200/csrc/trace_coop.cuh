@@ -257,18 +257,27 @@ SHN_D bool lane_advance(const Geom& g, const uint2* __restrict__ cells, const ui
       case ST_LEAF: {
         // runs of empty leaf cells are walked here, each with the step of
         // ST_LEAF_TESTED (nothing was tested, so its any-hit exit cannot fire)
+        // An empty leaf of a two-level grid built here holds [D, D), D its
+        // distance to the nearest non-empty leaf: the next D - 1 cells of the
+        // walk are empty too and are stepped through without fetching.
         const float tb = L.tbest;
         const int cap2 = (int)L.cres.x + (int)L.cres.y + (int)L.cres.z + 3;
+        uint32_t skip = 0;
         while (true) {
           L.vis2++;
-          const uint32_t li = L.lb + (uint32_t)(L.sc.x + L.cres.x * L.sc.y + L.cres.x * L.cres.y * L.sc.z);
-          const uint2 range = __ldg(leaves + li);
           steps++;
-          if (range.y > range.x) {
-            L.b = range.x;
-            L.e = range.y;
-            L.st = ST_LEAF_TESTED;
-            return true;
+          if (skip == 0) {
+            const uint32_t li = L.lb + (uint32_t)(L.sc.x + L.cres.x * L.sc.y + L.cres.x * L.cres.y * L.sc.z);
+            const uint2 range = __ldg(leaves + li);
+            if (range.y > range.x) {
+              L.b = range.x;
+              L.e = range.y;
+              L.st = ST_LEAF_TESTED;
+              return true;
+            }
+            skip = range.x > 0u ? range.x - 1u : 0u;
+          } else {
+            --skip;
           }
           if (!(tb > L.sMax.x || tb > L.sMax.y || tb > L.sMax.z)) {
             L.st = ST_TOP_NEXT;
