@@ -94,7 +94,10 @@ uint32_t shn_abi_version(void);
  * input). */
 shn_status shn_scene_create(shn_ctx* ctx, const float* vtx_xyz, uint32_t nv, const uint32_t* idx,
                             uint32_t nt, uint32_t mem, void* stream, shn_scene** out);
-/* Replace vertex positions (same counts); recomputes bounds. */
+/* Replace vertex positions (same counts); recomputes bounds.  Host vertices
+ * are staged on the device and checked there for inf/NaN before they replace
+ * the scene's (SHN_ERR_INVALID leaves the scene unchanged); synchronises the
+ * stream once for that check and once for the bounds. */
 shn_status shn_scene_update_vertices(shn_scene* s, const float* vtx_xyz, uint32_t nv, uint32_t mem,
                                      void* stream);
 shn_status shn_scene_bounds(const shn_scene* s, float out_min_max[6]);

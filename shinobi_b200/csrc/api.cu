@@ -80,6 +80,14 @@ shn_status validate_host(shn_ctx* ctx, const float* vtx, uint32_t nv, const uint
   return SHN_OK;
 }
 
+// Sets *flag when any of the n words is an inf/NaN float (exponent all ones).
+__global__ void k_nonfinite(const uint32_t* __restrict__ bits, size_t n, uint32_t* flag) {
+  uint32_t bad = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    bad |= (uint32_t)((__ldg(bits + i) & 0x7F800000u) == 0x7F800000u);
+  if (__any_sync(0xFFFFFFFFu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
+}
+
 shn_status refresh_bounds(shn_scene* s, cudaStream_t st) {
   float* d6 = nullptr;
   cudaError_t e = dev_alloc(s->ctx, (void**)&d6, 64, st);
@@ -236,13 +244,44 @@ shn_status shn_scene_create(shn_ctx* ctx, const float* vtx, uint32_t nv, const u
 shn_status shn_scene_update_vertices(shn_scene* s, const float* vtx, uint32_t nv, uint32_t mem,
                                      void* stream) {
   if (!s || !vtx || nv != s->nv || mem > SHN_MEM_DEVICE) return SHN_ERR_INVALID;
-  if (mem == SHN_MEM_HOST) {
-    shn_status v = validate_host(s->ctx, vtx, nv, nullptr, 0);
-    if (v) return v;
-  }
   cudaStream_t st = (cudaStream_t)stream;
-  shn_status rc = copy_in(s->ctx, s->vtx, vtx, 12 * (size_t)nv, mem, st);
-  if (rc) return rc;
+  shn_status rc;
+  if (mem == SHN_MEM_HOST) {
+    // host vertices are checked on the device: copied to a staging buffer,
+    // scanned for inf/NaN, and only then copied over the scene's vertices,
+    // so a rejected update leaves the scene as it was
+    const size_t vb = 12 * (size_t)nv;
+    char* stage = nullptr;
+    cudaError_t e = dev_alloc(s->ctx, (void**)&stage, vb + 256, st);
+    if (e != cudaSuccess) return alloc_status(s->ctx, e, "vertex staging");
+    uint32_t* flag = (uint32_t*)(stage + ((vb + 255) & ~(size_t)255));
+    uint32_t* h = pinned_take(s->ctx);
+    if (!h) {
+      dev_free(s->ctx, stage, vb + 256, st);
+      return set_error(s->ctx, SHN_ERR_OOM, "pinned");
+    }
+    cudaMemsetAsync(flag, 0, 4, st);
+    rc = copy_in(s->ctx, stage, vtx, vb, mem, st);
+    if (!rc && nv) {
+      const size_t n = 3 * (size_t)nv;
+      const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 8);
+      k_nonfinite<<<blocks, 256, 0, st>>>((const uint32_t*)stage, n, flag);
+    }
+    cudaMemcpyAsync(h, flag, 4, cudaMemcpyDeviceToHost, st);
+    if (!rc) {
+      e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) rc = cuda_status(s->ctx, e, "vertex check");
+    }
+    const uint32_t bad = rc ? 0u : h[0];
+    pinned_give(s->ctx, h);
+    if (!rc && bad) rc = set_error(s->ctx, SHN_ERR_INVALID, "non-finite vertex coordinate");
+    if (!rc) rc = copy_in(s->ctx, s->vtx, stage, vb, SHN_MEM_DEVICE, st);
+    dev_free(s->ctx, stage, vb + 256, st);
+    if (rc) return rc;
+  } else {
+    rc = copy_in(s->ctx, s->vtx, vtx, 12 * (size_t)nv, mem, st);
+    if (rc) return rc;
+  }
   launch_pack_triangles(s->vtx, s->idx, s->nt, s->tri, st);
   return refresh_bounds(s, st);
 }

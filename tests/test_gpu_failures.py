@@ -6,6 +6,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import oracle
 from shinobi_b200 import scenes
 
 pytestmark = pytest.mark.gpu
@@ -40,6 +41,29 @@ def test_invalid_scene_inputs_are_refused(gpu):
     with pytest.raises(shn.ShinobiError) as e:
         shn.FaceSoup(v, bad_i)
     assert e.value.status == shn._abi.SHN_ERR_INVALID
+
+
+def test_rejected_vertex_update_leaves_the_scene_unchanged(gpu):
+    """Host vertices are checked on the device before they replace the
+    scene's: an update holding inf/NaN is refused and the scene still builds
+    the same grid as before."""
+    import shinobi_b200 as shn
+    sc = scenes.uniform_soup(2000, seed=4)
+    soup = shn.FaceSoup(sc.vertices, sc.indices)
+    p = shn.grid_params(shn.SHN_GRID_UNIFORM, lambda_=5.0)
+    before = shn.Grid().build(soup, p).export()
+    for bad in (np.nan, np.inf):
+        v = sc.vertices.copy()
+        v[17, 2] = bad
+        with pytest.raises(shn.ShinobiError) as e:
+            soup.update_vertices(v)
+        assert e.value.status == shn._abi.SHN_ERR_INVALID
+    after = shn.Grid().build(soup, p).export()
+    for k in ("cells", "indices", "top_pairs"):
+        assert np.array_equal(before[k], after[k]), k
+    moved = sc.vertices * np.float32(1.5)
+    soup.update_vertices(moved)                 # a valid update still goes through
+    assert np.allclose(soup.bounds[3:], oracle.bounds(moved, sc.indices)[3:])
 
 
 def test_trace_before_build_is_refused(gpu):
