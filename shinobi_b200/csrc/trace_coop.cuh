@@ -18,9 +18,11 @@
 // top of the loop (persistent threads with per-lane replenishment).
 //
 // The per-ray sequence of cell visits, tests and continuation decisions is
-// exactly that of trace_uniform / trace_two_level (trace.cuh); the closest
-// hit is the argmin of (t, reference index) over the tested references, the
-// same winner the sequential strict-< loop keeps, so results are identical.
+// exactly that of trace_uniform / trace_two_level (trace.cuh) (block culling
+// and the empty-leaf skips only leave out work that cannot change the result);
+// the closest hit of a range is the least (t, triangle id) of its candidates,
+// the winner the reference's strict-< loop keeps over references in (cell,
+// triangle) order, so results are identical.
 #pragma once
 #include <type_traits>
 
@@ -421,8 +423,8 @@ SHN_D uint64_t warp_range_p(const Refs& G, V3 org, float Sx, float Sy, float Sz,
   uint32_t base = b;
   if (!ANY) {
     // closest hit: two references per lane per step (independent tests in
-    // flight); the lane-local minimum is updated in reference order, so the
-    // warp's argmin over (t, reference) is that of the sequential loop
+    // flight); each lane keeps its least (t, triangle id), and the warp's
+    // least key is the range's
     for (; base + 32 < e; base += 64, q0 += 64, q1 += 64, q2 += 64) {
       const uint32_t it = base + lane, it2 = it + 32;
       float4 a0, a1, a2;
@@ -607,10 +609,10 @@ SHN_D uint64_t warp_range(const Refs& G, uint32_t perm, V3 org, V3 rcp, float Sx
 // 32-reference chunk once and tests it against each of those rays in turn,
 // reading the ray's origin and shear from its parked state (a broadcast), so
 // a chunk crosses L2 once for the group instead of once per ray.  Candidates
-// of ray r go to gkey[r] (t bits << 32 | reference, ~0 = none) by atomicMin.
+// of ray r go to gkey[r] (t bits << 32 | triangle id, ~0 = none) by atomicMin.
 // A candidate must beat the ray's bound from earlier cells strictly and may
 // tie the range's running minimum (bound = next float above it), so gkey[r]
-// ends as the argmin over (t, reference) of the range's candidates below the
+// ends as the least (t, triangle id) of the range's candidates below the
 // earlier bound -- what warp_range_p returns -- in whatever order the lanes'
 // updates land.  An any-hit ray leaves after the first chunk holding a hit
 // (gend[r] = end of that chunk), as in warp_range_p.  SAME: every ray of the
