@@ -152,7 +152,9 @@ shn_status shn_grid_get_info(const shn_grid* g, shn_grid_info* out);
  * keeps the references of each leaf in spatial order on the device, and its
  * empty leaves hold [D, D) with D the distance to the nearest non-empty leaf;
  * the export puts the references back in (cell, triangle id) order and
- * returns empty leaves as [0, 0).  Synchronises. */
+ * returns empty leaves as [0, 0).  Uniform grids of 2^22 cells or more keep
+ * the same distances in their empty cells, exported as [0, 0).
+ * Synchronises. */
 shn_status shn_grid_export(const shn_grid* g, uint32_t* cells, uint32_t* leaves, uint32_t* indices,
                            uint64_t* top_pairs);
 /* Frees the grid's device memory (stream-ordered, pool); every launch that

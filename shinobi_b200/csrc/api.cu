@@ -376,6 +376,12 @@ shn_status shn_grid_export(const shn_grid* g, uint32_t* cells, uint32_t* leaves,
   if (e == cudaSuccess && indices && g->num_refs) e = cudaMemcpy(indices, g->indices, g->num_refs * 4, cudaMemcpyDeviceToHost);
   const uint64_t np = g->kind == SHN_GRID_TWO_LEVEL ? g->num_top_refs : g->num_refs;
   if (e == cudaSuccess && top_pairs && np) e = cudaMemcpy(top_pairs, g->top_pairs, np * 8, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && cells && g->cell_dist) {
+    // empty cells of a large uniform grid carry their distance to the nearest
+    // non-empty cell on the device; exported, an empty cell is [0, 0)
+    for (uint64_t i = 0; i < g->num_cells; ++i)
+      if (cells[2 * i] == cells[2 * i + 1]) cells[2 * i] = cells[2 * i + 1] = 0;
+  }
   if (e == cudaSuccess && leaves && g->spatial) {
     // empty leaves carry their distance to the nearest non-empty leaf on the
     // device; exported, an empty leaf is [0, 0)

@@ -547,6 +547,43 @@ __global__ void k_leaf_dist(const uint2* __restrict__ cells, uint32_t C, uint2* 
   }
 }
 
+// The same distances for the cells of a large uniform grid (one grid, no
+// owner search); an empty cell stores [D, D).
+constexpr uint64_t kCellDistMin = 1ull << 22;  // uniform grids with at least this many cells
+
+template <int AXIS>
+__global__ void k_cell_dist(uint2* __restrict__ cells, uint32_t rx, uint32_t ry, uint32_t rz,
+                            const uint8_t* __restrict__ din, uint8_t* __restrict__ dout) {
+  const uint64_t n = (uint64_t)rx * ry * rz;
+  for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < n; c += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t x = (uint32_t)(c % rx), y = (uint32_t)((c / rx) % ry), z = (uint32_t)(c / ((uint64_t)rx * ry));
+    const uint32_t pos = AXIS == 0 ? x : (AXIS == 1 ? y : z);
+    const uint32_t len = AXIS == 0 ? rx : (AXIS == 1 ? ry : rz);
+    const uint64_t stride = AXIS == 0 ? 1ull : (AXIS == 1 ? (uint64_t)rx : (uint64_t)rx * ry);
+    uint32_t best = kLeafDistCap + 1;
+    const uint32_t lo = pos >= kLeafDistCap ? pos - kLeafDistCap : 0u;
+    const uint32_t hi = min(len - 1u, pos + kLeafDistCap);
+    for (uint32_t q = lo; q <= hi; ++q) {
+      const uint64_t j = c - (uint64_t)pos * stride + (uint64_t)q * stride;
+      const uint32_t dq = q > pos ? q - pos : pos - q;
+      uint32_t v;
+      if (AXIS == 0) {
+        const uint2 r = cells[j];
+        v = r.y > r.x ? dq : kLeafDistCap + 1;
+      } else {
+        v = max(dq, (uint32_t)__ldg(din + j));
+      }
+      best = min(best, v);
+    }
+    if (AXIS < 2) {
+      dout[c] = (uint8_t)best;
+    } else {
+      const uint2 r = cells[c];
+      if (r.y <= r.x) cells[c] = make_uint2(best, best);
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kScanBlock) k_leaf_cells_scan(const uint2* __restrict__ top_ranges,
                                                                uint32_t C, Geom g, float lambda,
                                                                uint32_t threshold, LookbackState st,
@@ -824,6 +861,7 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   TriArr tri{s->tri};
   shn_status rc;
   g->num_blocks = g->num_super = 0;
+  g->cell_dist = false;
 
   // ---- two-level: build on the triangles in Morton order ------------------------
   g->spatial = p->kind == SHN_GRID_TWO_LEVEL && nt > 1;
@@ -885,6 +923,16 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
     if ((rc = ensure(g, (void**)&g->rtri, &g->cap_rtri, (size_t)std::max<uint32_t>(P, 1) * 48, st))) return rc;
     cudaMemsetAsync(g->cells, 0, C * 8, st);
     if (P) k_ranges<<<range_blocks(P), kRangeBlock, 0, st>>>(sortedTop, P, g->cells, g->indices, tri, g->rtri);
+    g->cell_dist = C >= kCellDistMin;
+    if (g->cell_dist) {
+      if ((rc = ensure_buf(g, g->ldist, 2 * (size_t)C, st))) return rc;
+      uint8_t* d1 = (uint8_t*)g->ldist.ptr;
+      uint8_t* d2 = d1 + C;
+      const int blocks = grid_for(C, 256, 148 * 8);
+      k_cell_dist<0><<<blocks, 256, 0, st>>>(g->cells, res[0], res[1], res[2], nullptr, d1);
+      k_cell_dist<1><<<blocks, 256, 0, st>>>(g->cells, res[0], res[1], res[2], d1, d2);
+      k_cell_dist<2><<<blocks, 256, 0, st>>>(g->cells, res[0], res[1], res[2], d2, nullptr);
+    }
     g->num_refs = P;
     g->num_leaves = 0;
     g->top_pairs = sortedTop;

@@ -75,6 +75,9 @@ struct shn_grid {
   // boxes of every 32 references (cbox) and every 1024 (sbox) of rtri, two
   // float4 (min, max) each, let the traversal skip blocks a ray cannot hit
   bool spatial = false;
+  // large uniform grids: empty cells hold [D, D), D their distance to the
+  // nearest non-empty cell (see k_cell_dist)
+  bool cell_dist = false;
   uint64_t num_blocks = 0, num_super = 0;
   shn::DevBuf mhi, perm_tri, cbox, sbox, ldist;
   size_t cap_cells = 0, cap_leaves = 0, cap_refs = 0, cap_rtri = 0;

@@ -168,12 +168,22 @@ SHN_D void trace_uniform(const GridView& G, V3 org, V3 dir, Hit& h) {
   bool valid = (cell.x != (rcp.x > 0.f ? g.resf.x : -1.f)) && (cell.y != (rcp.y > 0.f ? g.resf.y : -1.f)) &&
                (cell.z != (rcp.z > 0.f ? g.resf.z : -1.f));
   const int cap = g.res[0] + g.res[1] + g.res[2] + 3;
+  // An empty cell of a large uniform grid holds [D, D), D its distance to the
+  // nearest non-empty cell: the next D - 1 cells are empty and are stepped
+  // through without fetching (counted as visits all the same).
+  uint32_t skip = 0;
   for (int step = 0; valid && step < cap; ++step) {
-    const uint32_t cx = (uint32_t)clampf(cell.x, 0.f, g.resf.x - 1.f);
-    const uint32_t cy = (uint32_t)clampf(cell.y, 0.f, g.resf.y - 1.f);
-    const uint32_t cz = (uint32_t)clampf(cell.z, 0.f, g.resf.z - 1.f);
-    const uint2 range = __ldg(G.cells + (cx + cy * (uint32_t)g.res[0] + cz * (uint32_t)g.res[0] * (uint32_t)g.res[1]));
-    if (test_range<ANY>(G, w, range.x, range.y, h)) return;
+    if (skip == 0) {
+      const uint32_t cx = (uint32_t)clampf(cell.x, 0.f, g.resf.x - 1.f);
+      const uint32_t cy = (uint32_t)clampf(cell.y, 0.f, g.resf.y - 1.f);
+      const uint32_t cz = (uint32_t)clampf(cell.z, 0.f, g.resf.z - 1.f);
+      const uint2 range = __ldg(G.cells + (cx + cy * (uint32_t)g.res[0] + cz * (uint32_t)g.res[0] * (uint32_t)g.res[1]));
+      if (test_range<ANY>(G, w, range.x, range.y, h)) return;
+      if (range.y <= range.x && range.x > 0u) skip = range.x - 1u;
+    } else {
+      --skip;
+      h.steps += 1;
+    }
     valid = h.t > tMax.x || h.t > tMax.y || h.t > tMax.z;
     if (!valid) break;
     const int d = min_dim(tMax);
