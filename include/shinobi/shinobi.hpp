@@ -142,11 +142,12 @@ class FaceSoup {
     const size_t nv = aKeyFrame1.getNumVertices();
     if (aKeyFrame2.getNumVertices() != nv || 3 * nv != mVtx.size())
       throw Error(SHN_ERR_INVALID, "FaceSoup::uploadVertices: vertex counts differ");
+    const float omc = 1.f - aCoeff;
     for (size_t i = 0; i < nv; ++i) {
       const vec3f a = aKeyFrame1.getVertex(i), b = aKeyFrame2.getVertex(i);
-      mVtx[3 * i + 0] = a.x + aCoeff * (b.x - a.x);
-      mVtx[3 * i + 1] = a.y + aCoeff * (b.y - a.y);
-      mVtx[3 * i + 2] = a.z + aCoeff * (b.z - a.z);
+      mVtx[3 * i + 0] = a.x * omc + b.x * aCoeff;  // the reference's order of operations
+      mVtx[3 * i + 1] = a.y * omc + b.y * aCoeff;
+      mVtx[3 * i + 2] = a.z * omc + b.z * aCoeff;
     }
     check(shn_scene_update_vertices(mScene, mVtx.data(), (uint32_t)nv, SHN_MEM_HOST, aStream),
           "FaceSoup::uploadVertices", mCtx->get());

@@ -100,6 +100,16 @@ shn_status shn_scene_create(shn_ctx* ctx, const float* vtx_xyz, uint32_t nv, con
  * stream once for that check and once for the bounds. */
 shn_status shn_scene_update_vertices(shn_scene* s, const float* vtx_xyz, uint32_t nv, uint32_t mem,
                                      void* stream);
+/* Keyframe interpolation on the device (FaceSoup::uploadVertices as used by
+ * DynamicRTEngine, src/Control/Structure/FaceSoup.h:249-339,
+ * src/Engine/DynamicRTEngine.h:73-158): vertex coordinate i becomes
+ * kf1[i] * (1 - coeff) + kf2[i] * coeff (FP32, in that order) for the first
+ * n1 vertices and kf2[i] for the rest, as the reference does when the first
+ * keyframe is shorter.  d_kf1 (3*n1 floats) and d_kf2 (3*nv floats, nv the
+ * scene's count) are device arrays; recomputes bounds (one stream
+ * synchronisation).  Inputs are not checked for inf/NaN beyond the bounds. */
+shn_status shn_scene_interpolate_vertices(shn_scene* s, const float* d_kf1, uint32_t n1, const float* d_kf2,
+                                          float coeff, void* stream);
 shn_status shn_scene_bounds(const shn_scene* s, float out_min_max[6]);
 uint32_t shn_scene_num_triangles(const shn_scene* s);
 void shn_scene_destroy(shn_scene* s);

@@ -128,6 +128,16 @@ class FaceSoup:
                                                _stream(stream))
         self.ctx.check(st, "shn_scene_update_vertices")
 
+    def interpolate_vertices(self, kf1, kf2, coeff: float, stream=None):
+        """Vertices = kf1 * (1 - coeff) + kf2 * coeff on the device (FaceSoup::uploadVertices of
+        the reference's dynamic engine); kf1 (n1, 3) may be shorter than kf2 (nv, 3): the rest
+        take kf2.  Both are device tensors."""
+        kf1 = kf1.contiguous()
+        kf2 = kf2.contiguous()
+        self.ctx.check(self.ctx.lib.shn_scene_interpolate_vertices(
+            self.handle, _ptr(kf1), kf1.shape[0], _ptr(kf2), float(coeff), _stream(stream)),
+            "shn_scene_interpolate_vertices")
+
     @property
     def bounds(self) -> np.ndarray:
         out = (C.c_float * 6)()

@@ -105,6 +105,7 @@ SIGNATURES = {
     "shn_scene_create": ([vp, vp, u32, vp, u32, u32, vp, C.POINTER(vp)], i32),
     "shn_scene_update_vertices": ([vp, vp, u32, u32, vp], i32),
     "shn_scene_bounds": ([vp, C.POINTER(f32)], i32),
+    "shn_scene_interpolate_vertices": ([vp, vp, u32, vp, f32, vp], i32),
     "shn_scene_num_triangles": ([vp], u32),
     "shn_scene_destroy": ([vp], None),
     "shn_grid_params_default": ([u32, C.POINTER(GridParams)], None),

@@ -88,6 +88,13 @@ __global__ void k_nonfinite(const uint32_t* __restrict__ bits, size_t n, uint32_
   if (__any_sync(0xFFFFFFFFu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
 }
 
+// kf1 * (1 - c) + kf2 * c for the first m coordinates, kf2 for the rest.
+__global__ void k_lerp_vertices(const float* __restrict__ kf1, const float* __restrict__ kf2, size_t m, size_t n,
+                                float omc, float c, float* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = i < m ? __ldg(kf1 + i) * omc + __ldg(kf2 + i) * c : __ldg(kf2 + i);
+}
+
 shn_status refresh_bounds(shn_scene* s, cudaStream_t st) {
   float* d6 = nullptr;
   cudaError_t e = dev_alloc(s->ctx, (void**)&d6, 64, st);
@@ -281,6 +288,21 @@ shn_status shn_scene_update_vertices(shn_scene* s, const float* vtx, uint32_t nv
   } else {
     rc = copy_in(s->ctx, s->vtx, vtx, 12 * (size_t)nv, mem, st);
     if (rc) return rc;
+  }
+  launch_pack_triangles(s->vtx, s->idx, s->nt, s->tri, st);
+  return refresh_bounds(s, st);
+}
+
+shn_status shn_scene_interpolate_vertices(shn_scene* s, const float* kf1, uint32_t n1, const float* kf2,
+                                          float coeff, void* stream) {
+  if (!s || !kf2 || (n1 && !kf1) || n1 > s->nv) return SHN_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t n = 3 * (size_t)s->nv;
+  if (n) {
+    const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 8);
+    k_lerp_vertices<<<blocks, 256, 0, st>>>(kf1, kf2, 3 * (size_t)n1, n, 1.f - coeff, coeff, s->vtx);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(s->ctx, e, "interpolate vertices");
   }
   launch_pack_triangles(s->vtx, s->idx, s->nt, s->tri, st);
   return refresh_bounds(s, st);
