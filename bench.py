@@ -194,14 +194,21 @@ def cpu_baseline(sc, cam, stride: int, use_reference_build: bool, direct: bool =
     sel = np.arange(0, org.shape[0], stride)
     t1 = time.perf_counter()
     tri, t, _, _, st_p = oracle.trace_closest(g, org[sel], d[sel])
+    # the sample's secondary rays are keyed by their pixels' ids in the full
+    # frame, so the sample's results are those of the frame at those pixels
     if direct:
-        # timing only: the sample's rays are numbered by their position in the sample
-        ro, rd, _ = oracle.direct_rays(org[sel], d[sel], tri, t, DI_SPP, DI_SEED, 0, DI_LIGHT)
+        ro, rd, _ = oracle.direct_rays(org[sel], d[sel], tri, t, DI_SPP, DI_SEED, 0, DI_LIGHT, pix=sel)
         occ, st_s = oracle.trace_any(g, ro, rd, np.full(ro.shape[0], 0.9999, np.float32))
-        oracle.shade_direct(sc.vertices, sc.indices, org[sel], d[sel], tri, t, DI_SPP, DI_SEED, 0, DI_LIGHT, occ)
+        shaded, _ = oracle.shade_direct(sc.vertices, sc.indices, org[sel], d[sel], tri, t, DI_SPP, DI_SEED, 0,
+                                        DI_LIGHT, occ, pix=sel)
     else:
-        ro, rd, _ = oracle.ao_rays(sc.vertices, sc.indices, org[sel], d[sel], tri, t, AO_SPP, AO_SEED, AO_OFFSET)
-        _, st_s = oracle.trace_any(g, ro, rd, np.full(ro.shape[0], AO_LEN, np.float32))
+        ro, rd, rpix = oracle.ao_rays(sc.vertices, sc.indices, org[sel], d[sel], tri, t, AO_SPP, AO_SEED,
+                                      AO_OFFSET, pix=sel)
+        occ, st_s = oracle.trace_any(g, ro, rd, np.full(ro.shape[0], AO_LEN, np.float32))
+        cnt = np.zeros(sel.size, np.int64)
+        np.add.at(cnt, rpix, occ.astype(np.int64))
+        shaded = np.where(tri == 0xFFFFFFFF, np.float32(1.0),
+                          np.float32(1.0) - cnt.astype(np.float32) / np.float32(AO_SPP)).astype(np.float32)
     t_trace = time.perf_counter() - t1
     sample_rays = sel.size + ro.shape[0]
     # full-frame estimate: every pixel traced, AO rays in proportion to the sample's hit rate
@@ -219,7 +226,28 @@ def cpu_baseline(sc, cam, stride: int, use_reference_build: bool, direct: bool =
         # and triangle tests), scaled to the full frame by the sample ratio
         "oracle_work": {"scale": org.shape[0] / sel.size,
                         "primary": [int(st_p[0]), int(st_p[1])], "secondary": [int(st_s[0]), int(st_s[1])]},
+        # the oracle's results on the sampled pixels (for the parity check of the timed frame)
+        "oracle_sample": {"pixels": sel, "tri": tri, "t": t, "shaded": shaded},
     }
+
+
+def frame_parity(sample, hits, shaded_dev, direct: bool):
+    """The timed frame's results on the CPU baseline's sampled pixels against
+    the oracle's (bit-exact: hit triangle, t and the AO value / shaded RGB)."""
+    pix = sample["pixels"]
+    tri = hits.tri.cpu().numpy().view(np.uint32)[pix]
+    t = hits.t.cpu().numpy()[pix]
+    if direct:
+        got = shaded_dev.cpu().numpy().reshape(-1, 3)[pix]
+    else:
+        got = shaded_dev.cpu().numpy()[pix]
+    bad_hit = int(np.count_nonzero((tri != sample["tri"]) | (t.view(np.uint32) != sample["t"].view(np.uint32))))
+    ref = sample["shaded"]
+    bad_sh = int(np.count_nonzero((got.view(np.uint32) != ref.view(np.uint32)).reshape(pix.size, -1).any(axis=1)))
+    return {"pixels": int(pix.size), "mismatches": bad_hit + bad_sh, "hit_mismatches": bad_hit,
+            ("shading_mismatches" if direct else "ao_mismatches"): bad_sh,
+            "what": "the timed frame's primary hits (tri, t) and " + ("shaded RGB" if direct else "AO values")
+                    + " on the CPU baseline's sampled pixels against the oracle, bit for bit"}
 
 
 def run_reference(args):
@@ -238,6 +266,7 @@ def run_reference(args):
     last = None
     for _ in range(args.steps):
         last = cpu_baseline(sc, cam, stride, True, direct=direct)
+        last.pop("oracle_sample")
         vals.append(last["value"])
         secs += last["sample_seconds"]
     v = float(np.mean(vals))
@@ -245,7 +274,7 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Philox4x32-10 scene)",
-            "config": workload_config({"cpu_sample": last["sample"]}, direct=direct),
+            "config": workload_config(direct=direct),
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": last["cores"], "kind": "reference",
                              "sample": last["sample"]},
             "build_ms_per_mtri": last["build_ms_per_mtri"],
@@ -406,8 +435,14 @@ def run_shinobi(args):
     ctx.lib.shn_grid_set_stats(g.handle, None)
     fp32 = fp32_peak_tflops(torch)
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the GPU results of the last step (the same scene, camera and seeds every step)
+        step()
+        torch.cuda.synchronize()
+        g.sync_status()
         cpu = cpu_baseline(sc, cam, args.cpu_sample_stride, False, direct=direct)
+        parity = frame_parity(cpu.pop("oracle_sample"), hits, ao, direct)
     # dominant kernel: the longer of the two trace kernels
     if ao_ms >= prim_ms:
         kname = "k_trace_direct<two-level>" if direct else "k_trace_ao<two-level>"
@@ -418,16 +453,19 @@ def run_shinobi(args):
     # the reference algorithm makes
     work = 10.0 * ksteps + 40.0 * ktests  # FP32 ops per launch (cell visit 10, triangle test 40)
     executed = work / (kms * 1e-3) / 1e12
-    achieved, work_note = executed, (f"{ksteps} cell visits x 10 + {ktests} triangle tests x 40 FP32 ops per "
-                                     "launch, counted on the device (executed work)")
+    algorithmic = None
     if cpu is not None:
+        # the reference algorithm's work (no block culling): what the kernel
+        # would execute without skipping blocks, as a rate -- above the FP32
+        # peak, so reported beside the roofline, not as its fraction
         ow = cpu.pop("oracle_work")
         which = "primary" if kname.startswith("k_trace_camera") else "secondary"
         a_steps, a_tests = (ow[which][0] * ow["scale"], ow[which][1] * ow["scale"])
-        achieved = (10.0 * a_steps + 40.0 * a_tests) / (kms * 1e-3) / 1e12
-        work_note = (f"{a_steps:.4g} cell visits x 10 + {a_tests:.4g} triangle tests x 40 FP32 ops per launch: "
-                     f"the reference algorithm's work, counted by the oracle on every "
-                     f"{args.cpu_sample_stride}th pixel and scaled to the frame")
+        arate = (10.0 * a_steps + 40.0 * a_tests) / (kms * 1e-3) / 1e12
+        algorithmic = {"tflops": arate, "vs_peak": arate / fp32,
+                       "work": (f"{a_steps:.4g} cell visits x 10 + {a_tests:.4g} triangle tests x 40 FP32 ops per "
+                                f"launch: the reference algorithm's work, counted by the oracle on every "
+                                f"{args.cpu_sample_stride}th pixel and scaled to the frame")}
     traffic = profile_traffic().get(kname)
     inf = g.info()
     peaks, peak_kind = measured_peaks()
@@ -448,19 +486,18 @@ def run_shinobi(args):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Philox4x32-10 scene, resident in HBM)",
-        "config": workload_config({"rays_per_step": rays_per_step, "parallelism": f"replicas x{world}"},
-                                  direct=direct),
+        "config": workload_config(direct=direct),
+        "rays_per_step": rays_per_step, "parallelism": f"replicas x{world}",
         "build_ms_per_mtri": build_ms / (N_TRIS / 1e6),
         "phase_ms": {"build": build_ms, "primary": prim_ms, ("direct" if direct else "ao"): ao_ms},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {
-            "bound": "fp32", "kernel": kname, "achieved": achieved, "peak": fp32, "unit": "TFLOP/s",
-            "frac": achieved / fp32, "traffic": traffic,
-            "work": work_note,
-            "executed": {"achieved": executed, "frac": executed / fp32,
-                         "work": f"{ksteps} cell visits x 10 + {ktests} triangle tests x 40 FP32 ops per launch "
-                                 "as executed (device counters)"},
+            "bound": "fp32", "kernel": kname, "achieved": executed, "peak": fp32, "unit": "TFLOP/s",
+            "frac": executed / fp32, "traffic": traffic,
+            "work": (f"{ksteps} cell visits x 10 + {ktests} triangle tests x 40 FP32 ops per launch as executed "
+                     "(device counters of the kernel's counting variant)"),
             "peak_source": "cuBLAS SGEMM (TF32 off) 8192^3 measured in this run; no FP32 figure in MEASURED_PEAKS.json",
+            "algorithmic_rate": algorithmic,
         },
         "roofline_build": {
             "bound": "hbm", "achieved": build_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
@@ -473,6 +510,7 @@ def run_shinobi(args):
     line["gpu_launches"] = args.steps * launches_per_step(P, R, C0, L)
     if cpu is not None:
         line["cpu_baseline"] = cpu
+        line["parity"] = parity
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -6,6 +6,14 @@
  *
  * Conventions
  *  - every call returns shn_status; shn_ctx_last_error() gives a message;
+ *  - bounded device-side waits (look-back scans, bulk copies) that give up
+ *    set an error bit instead of hanging.  Calls that synchronise (builds,
+ *    exports) report it themselves; asynchronous calls (traces, AO, direct
+ *    illumination, the path tracer, scans, compaction, sorts, batch replays)
+ *    leave it in a device word that shn_grid_sync_status /
+ *    shn_ctx_sync_status / shn_batch_sync_status /
+ *    shn_exclusive_scan_u32_noalloc_status report (SHN_ERR_TIMEOUT) and
+ *    clear; the reference aborted through cutil's check macros instead;
  *  - pointers named d_* are device pointers owned by the caller; objects
  *    created by shn_*_create are owned by the library and released by the
  *    matching shn_*_destroy;
@@ -170,6 +178,13 @@ shn_status shn_grid_export(const shn_grid* g, uint32_t* cells, uint32_t* leaves,
 /* Frees the grid's device memory (stream-ordered, pool); every launch that
  * reads the grid must have completed. */
 void shn_grid_destroy(shn_grid* g);
+/* Synchronises stream, then reports and clears the grid's device error word:
+ * SHN_ERR_TIMEOUT if a bounded wait gave up in any trace, AO,
+ * direct-illumination or path-tracer call on the grid since the last check
+ * (their results are then not valid), else SHN_OK.  The word also clears at
+ * the start of each build, which reports its own waits.  No counterpart in
+ * the reference (its cutil macros aborted the process). */
+shn_status shn_grid_sync_status(const shn_grid* g, void* stream);
 
 /* ---- traversal -------------------------------------------------------------- */
 typedef struct shn_rays {
@@ -304,6 +319,11 @@ shn_status shn_batch_info(const shn_batch* b, uint64_t* num_pairs, uint64_t* tot
 shn_status shn_batch_export_scene(const shn_batch* b, uint32_t scene, int32_t res[3], float bounds[6],
                                   uint32_t* cells, uint32_t* indices, uint64_t* num_refs);
 void shn_batch_destroy(shn_batch* b);
+/* Synchronises stream, then reports and clears the batch's device error word
+ * (set by the build, trace or graph replay of the batch since the last check;
+ * each build clears it first): SHN_ERR_TIMEOUT for a bounded wait that gave
+ * up, SHN_ERR_INVALID when a replay found more pairs than planned. */
+shn_status shn_batch_sync_status(shn_batch* b, void* stream);
 
 /* ---- ray-query server ------------------------------------------------------------
  * Resident uniform grids in scene slots, requests admitted by the context's
@@ -411,13 +431,44 @@ shn_status shn_exclusive_scan_u32(shn_ctx* ctx, const uint32_t* d_in, uint32_t* 
  * of about 64 KiB held by every GPU that loads the library, not in a pool.
  * n <= 2^24 (SHN_SCAN_NOALLOC_MAX_N), larger n returns SHN_ERR_INVALID.  All
  * calls on a device share that array: calls whose work overlaps on the GPU
- * race, so order them on one stream.  The first call on each device looks up
- * the array's device address (cudaGetSymbolAddress, with that device
- * current); make it before any stream capture.  No counterpart in the
- * reference. */
+ * race, so order them on one stream.  Each call clears the words it uses
+ * (8 * (ceil(n / 2048) + 1) bytes, one cudaMemsetAsync on the stream).  A
+ * look-back wait that gives up is reported by
+ * shn_exclusive_scan_u32_noalloc_status.  The first call on each device looks
+ * up the array's device address (cudaGetSymbolAddress, with that device
+ * current) and caches it for the life of the process; make it before any
+ * stream capture, and do not call after a cudaDeviceReset, which invalidates
+ * the cached address.  No counterpart in the reference. */
 #define SHN_SCAN_NOALLOC_MAX_N (1u << 24)
 shn_status shn_exclusive_scan_u32_noalloc(const uint32_t* d_in, uint32_t* d_out, uint32_t n,
                                           void* stream);
+/* Synchronises stream, then reports and clears the error word of the
+ * allocation-free scan: SHN_ERR_TIMEOUT if a look-back wait gave up in any
+ * shn_exclusive_scan_u32_noalloc call on the current device since the last
+ * check (those calls' outputs are not valid), else SHN_OK.  Allocates
+ * nothing (it reads the same fixed array).  No counterpart in the reference. */
+shn_status shn_exclusive_scan_u32_noalloc_status(void* stream);
+/* Synchronises stream, then reports and clears the error word of the
+ * context-level primitives (shn_exclusive_scan_u32, shn_compact_u32,
+ * shn_sort_keys_u64): SHN_ERR_TIMEOUT if a bounded wait gave up in any of
+ * them since the last check.  No counterpart in the reference. */
+shn_status shn_ctx_sync_status(shn_ctx* ctx, void* stream);
+/* Failure-detection self test of the look-back scans that run inside other
+ * calls.  Arms the next look-back scan of the chosen kind to launch without
+ * its first tile, which then never publishes, so every other tile's bounded
+ * wait runs out (about a second) and records SHN_ERR_TIMEOUT for the status
+ * call above; the output of that one call is not valid, and no access leaves
+ * its buffers.  The arm is used by the first call with at least two tiles
+ * (more than 2048 elements / pixels):
+ *   SHN_FORCE_CTX_SCAN         shn_exclusive_scan_u32 or shn_compact_u32 on ctx;
+ *   SHN_FORCE_GRID_COMPACTION  the hit compaction of shn_trace_ao or
+ *                              shn_shade_direct on g;
+ *   SHN_FORCE_NOALLOC_SCAN     shn_exclusive_scan_u32_noalloc (any device).
+ * No counterpart in the reference. */
+#define SHN_FORCE_CTX_SCAN 1u
+#define SHN_FORCE_GRID_COMPACTION 2u
+#define SHN_FORCE_NOALLOC_SCAN 3u
+shn_status shn_debug_force_lookback_timeout(uint32_t target, shn_ctx* ctx, shn_grid* g);
 /* Failure-detection self test: runs the look-back scan kernel with tile 0
  * never published, so tile 1's bounded wait must run out (about a second)
  * and report it.  Returns SHN_ERR_TIMEOUT when the wait ran out and the

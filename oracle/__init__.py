@@ -75,12 +75,14 @@ def lib():
         L.orc_philox.argtypes = [vp, u32, u32, u32, vp]
         L.orc_camera.argtypes = [vp, vp, vp, f32, u32, u32, vp]
         L.orc_primary_rays.argtypes = [vp, u32, u32, u32, vp, vp, vp]
-        L.orc_ao_rays.argtypes = [vp, vp] + [vp] * 8 + [u32, u32, u32, f32] + [vp] * 7
+        L.orc_ao_rays.argtypes = [vp, vp] + [vp] * 8 + [u32, u32, u32, f32] + [vp] * 8
         L.orc_ao_rays.restype = u32
-        L.orc_direct_rays.argtypes = [vp] * 8 + [u32, u32, u32, u32, vp] + [vp] * 7
+        L.orc_direct_rays.argtypes = [vp] * 8 + [u32, u32, u32, u32, vp] + [vp] * 8
         L.orc_direct_rays.restype = u32
-        L.orc_shade_direct.argtypes = [vp] * 10 + [u32, u32, u32, u32] + [vp] * 3 + [u32] + [vp] * 5
+        L.orc_shade_direct.argtypes = [vp] * 10 + [u32, u32, u32, u32] + [vp] * 3 + [u32] + [vp] * 6
         L.orc_pt_render.argtypes = [vp, vp, vp, u32, u32, u32, u32, u32, f32, vp, vp, vp, vp, vp, f32, u32, vp]
+        L.orc_pt_render_pixels.argtypes = [vp, vp, vp, u32, u32, u32, u32, u32, f32, vp, vp, vp, vp, vp, f32,
+                                           u32, vp, u32, vp]
         L.orc_compact.argtypes = [vp, u32, vp]
         L.orc_compact.restype = u32
         _lib = L
@@ -287,15 +289,18 @@ def primary_rays(cam, image_id: int = 0):
     return org, np.stack([dx, dy, dz], axis=1)
 
 
-def ao_rays(vtx, idx, org, dirs, tri, t, spp: int, seed: int, offset: float):
-    """AO rays from primary hits; returns (org, dir, pixel) for hit pixels only."""
+def ao_rays(vtx, idx, org, dirs, tri, t, spp: int, seed: int, offset: float, pix=None):
+    """AO rays from primary hits; returns (org, dir, pixel) for hit pixels only.
+    pix: the frame's pixel id of each input ray (a sample of a frame), which keys
+    the random numbers; default 0..n-1.  The returned pixel is the input index."""
     vtx, idx, org, dirs, tri, t = _f32(vtx), _u32(idx), _f32(org), _f32(dirs), _u32(tri), _f32(t)
+    pix = _u32(pix) if pix is not None else None
     n = org.shape[0]
     m_max = int(np.count_nonzero(tri != MISS)) * spp
     outs = [np.zeros(m_max, np.float32) for _ in range(6)] + [np.zeros(m_max, np.uint32)]
     cols = [np.ascontiguousarray(org[:, k]) for k in range(3)] + [np.ascontiguousarray(dirs[:, k]) for k in range(3)]
     m = lib().orc_ao_rays(_p(vtx), _p(idx), *[_p(c) for c in cols], _p(tri), _p(t), n, spp, seed,
-                          offset, *[_p(o) for o in outs])
+                          offset, *[_p(o) for o in outs], _p(pix))
     assert m == m_max
     ro = np.stack(outs[0:3], axis=1)
     rd = np.stack(outs[3:6], axis=1)
@@ -306,21 +311,24 @@ def _light15(light) -> np.ndarray:
     return np.concatenate([_f32(light[k]) for k in ("position", "edge1", "edge2", "normal", "intensity")])
 
 
-def direct_rays(org, dirs, tri, t, spp: int, seed: int, image_id: int, light):
-    """Shadow segments of the hit pixels; returns (org, dir, pixel) in pixel-major order."""
+def direct_rays(org, dirs, tri, t, spp: int, seed: int, image_id: int, light, pix=None):
+    """Shadow segments of the hit pixels; returns (org, dir, pixel) in pixel-major order.
+    pix: frame pixel ids of the inputs (keys the random numbers), default 0..n-1."""
     org, dirs, tri, t = _f32(org), _f32(dirs), _u32(tri), _f32(t)
+    pix = _u32(pix) if pix is not None else None
     n = org.shape[0]
     m_max = int(np.count_nonzero(tri != MISS)) * spp
     outs = [np.zeros(m_max, np.float32) for _ in range(6)] + [np.zeros(m_max, np.uint32)]
     cols = [np.ascontiguousarray(org[:, k]) for k in range(3)] + [np.ascontiguousarray(dirs[:, k]) for k in range(3)]
     m = lib().orc_direct_rays(*[_p(c) for c in cols], _p(tri), _p(t), n, spp, seed, image_id,
-                              _p(_light15(light)), *[_p(o) for o in outs])
+                              _p(_light15(light)), *[_p(o) for o in outs], _p(pix))
     assert m == m_max
     return np.stack(outs[0:3], axis=1), np.stack(outs[3:6], axis=1), outs[6]
 
 
 def shade_direct(vtx, idx, org, dirs, tri, t, spp, seed, image_id, light, occ, tri_material=None,
-                 diffuse=None, default_diffuse=(0.7, 0.7, 0.7), background=(0.15, 0.2, 0.3), final=None):
+                 diffuse=None, default_diffuse=(0.7, 0.7, 0.7), background=(0.15, 0.2, 0.3), final=None,
+                 pix=None):
     """(frame (n,3), final (n,3) or None) with the semantics of shn_shade_direct;
     occ = blocked flags of direct_rays' segments, in its order."""
     vtx, idx, org, dirs, tri, t = _f32(vtx), _u32(idx), _f32(org), _f32(dirs), _u32(tri), _f32(t)
@@ -335,7 +343,8 @@ def shade_direct(vtx, idx, org, dirs, tri, t, spp, seed, image_id, light, occ, t
     lib().orc_shade_direct(_p(vtx), _p(idx), *[_p(c) for c in cols], _p(tri), _p(t), n, spp, seed, image_id,
                            _p(_light15(light)), _p(tm) if tm is not None else None,
                            _p(df) if df is not None else None, nmat, _p(_f32(default_diffuse)),
-                           _p(_f32(background)), _p(occ), _p(frame), _p(fin) if fin is not None else None)
+                           _p(_f32(background)), _p(occ), _p(frame), _p(fin) if fin is not None else None,
+                           _p(_u32(pix)) if pix is not None else None)
     return frame.reshape(n, 3), (fin.reshape(n, 3) if fin is not None else None)
 
 
@@ -348,6 +357,19 @@ def pt_render(g: Grid, cam, spp, max_depth, rr_depth, albedo, light_pos, light_e
                         rr_depth, albedo, _p(_f32(light_pos)), _p(_f32(light_e1)), _p(_f32(light_e2)),
                         _p(_f32(light_radiance)), _p(_f32(background)), offset, seed, _p(img))
     return img.reshape(cam.res_y, cam.res_x, 3)
+
+
+def pt_render_pixels(g: Grid, cam, pix, spp, max_depth, rr_depth, albedo, light_pos, light_e1, light_e2,
+                     light_radiance, background, offset, seed) -> np.ndarray:
+    """pt_render's values at the frame pixels pix only: (len(pix), 3)."""
+    c = camera(cam)
+    pix = _u32(pix)
+    out = np.zeros(pix.size * 3, np.float32)
+    lib().orc_pt_render_pixels(g.handle, _p(c), _p(_f32(cam.eye)), cam.res_x, cam.res_y, spp, max_depth,
+                               rr_depth, albedo, _p(_f32(light_pos)), _p(_f32(light_e1)), _p(_f32(light_e2)),
+                               _p(_f32(light_radiance)), _p(_f32(background)), offset, seed, _p(pix), pix.size,
+                               _p(out))
+    return out.reshape(-1, 3)
 
 
 def compact(flags) -> np.ndarray:

@@ -878,10 +878,11 @@ uint32_t orc_ao_rays(const float* vtx, const uint32_t* idx, const float* ox, con
                      const float* oz, const float* dx, const float* dy, const float* dz,
                      const uint32_t* tri, const float* t, uint32_t n, uint32_t spp, uint32_t seed,
                      float offset, float* rox, float* roy, float* roz, float* rdx, float* rdy,
-                     float* rdz, uint32_t* rpix) {
+                     float* rdz, uint32_t* rpix, const uint32_t* pix) {
   uint32_t m = 0;
   for (uint32_t p = 0; p < n; ++p) {
     if (tri[p] == kMiss) continue;
+    const uint32_t pid = pix ? pix[p] : p;  // the pixel's id in the full frame
     const Tri tr = load_tri(vtx, idx, tri[p]);
     const V3 d = mk(dx[p], dy[p], dz[p]);
     const V3 e1 = sub(tr.v[1], tr.v[0]);
@@ -892,7 +893,7 @@ uint32_t orc_ao_rays(const float* vtx, const uint32_t* idx, const float* ox, con
     const V3 hp = add(mk(ox[p], oy[p], oz[p]), muls(d, t[p]));
     const V3 o = add(hp, muls(nn, offset));
     for (uint32_t s = 0; s < spp; ++s) {
-      uint32_t c[4] = {p, s, 0u, 0x414Fu};
+      uint32_t c[4] = {pid, s, 0u, 0x414Fu};
       philox(c, seed, 0u);
       const float u1 = u01(c[0]), u2 = u01(c[1]);
       float sn, cs;
@@ -937,13 +938,14 @@ uint32_t orc_direct_rays(const float* ox, const float* oy, const float* oz, cons
                          const float* dy, const float* dz, const uint32_t* tri, const float* t,
                          uint32_t n, uint32_t spp, uint32_t seed, uint32_t image_id,
                          const float* light15, float* rox, float* roy, float* roz, float* rdx,
-                         float* rdy, float* rdz, uint32_t* rpix) {
+                         float* rdy, float* rdz, uint32_t* rpix, const uint32_t* pix) {
   uint32_t m = 0;
   for (uint32_t p = 0; p < n; ++p) {
     if (tri[p] == kMiss) continue;
+    const uint32_t pid = pix ? pix[p] : p;
     for (uint32_t s = 0; s < spp; ++s) {
       V3 o, L;
-      di_segment(mk(ox[p], oy[p], oz[p]), mk(dx[p], dy[p], dz[p]), t[p], light15, p, s, image_id, seed, o, L);
+      di_segment(mk(ox[p], oy[p], oz[p]), mk(dx[p], dy[p], dz[p]), t[p], light15, pid, s, image_id, seed, o, L);
       rox[m] = o.x; roy[m] = o.y; roz[m] = o.z;
       rdx[m] = L.x; rdy[m] = L.y; rdz[m] = L.z;
       rpix[m] = p;
@@ -965,7 +967,7 @@ void orc_shade_direct(const float* vtx, const uint32_t* idx, const float* ox, co
                       const uint32_t* tri, const float* t, uint32_t n, uint32_t spp, uint32_t seed,
                       uint32_t image_id, const float* light15, const uint32_t* tri_mat,
                       const float* diffuse, uint32_t nmat, const float* ddef, const float* bg,
-                      const uint8_t* occ, float* frame, float* fin) {
+                      const uint8_t* occ, float* frame, float* fin, const uint32_t* pix) {
   const V3 E1 = mk(light15[3], light15[4], light15[5]), E2 = mk(light15[6], light15[7], light15[8]);
   const V3 LN = mk(light15[9], light15[10], light15[11]), LI = mk(light15[12], light15[13], light15[14]);
   const V3 lc = cross(E1, E2);
@@ -987,10 +989,11 @@ void orc_shade_direct(const float* vtx, const uint32_t* idx, const float* ox, co
         diff = mk(diffuse[4 * m], diffuse[4 * m + 1], diffuse[4 * m + 2]);
       }
       const V3 kk = mul(muls(LI, larea), diff);
+      const uint32_t pid = pix ? pix[p] : p;
       for (uint32_t s = 0; s < spp; ++s, ++k) {
         if (occ[k]) continue;
         V3 o, L;
-        di_segment(mk(ox[p], oy[p], oz[p]), mk(dx[p], dy[p], dz[p]), t[p], light15, p, s, image_id, seed, o, L);
+        di_segment(mk(ox[p], oy[p], oz[p]), mk(dx[p], dy[p], dz[p]), t[p], light15, pid, s, image_id, seed, o, L);
         const V3 ln = normalize(L);
         const float att = 1.0f / dot(L, L);
         const float a = fmaxf(0.f, -dot(LN, ln));
@@ -1021,11 +1024,14 @@ void orc_shade_direct(const float* vtx, const uint32_t* idx, const float* ox, co
 // RandomPixelSampler (src/Primitive/PixelSampler.h:56-70), Philox4x32-10
 // counters (pixel, sample, depth, tag) with key (seed, 0).  The image is the
 // per-pixel mean of the per-path radiance summed in sample order.
-void orc_pt_render(const orc_grid* G, const float cam9[9], const float eye[3], uint32_t resx,
-                   uint32_t resy, uint32_t spp, uint32_t max_depth, uint32_t rr_depth, float albedo,
-                   const float lpos[3], const float le1[3], const float le2[3], const float lrad[3],
-                   const float bg[3], float offset, uint32_t seed, float* image) {
-  const uint32_t npix = resx * resy;
+// pix (may be null): render only pixels pix[0..npix_sel) of the frame into
+// image[3k..3k+3) (a sample of a frame); null renders every pixel.
+void orc_pt_render_pixels(const orc_grid* G, const float cam9[9], const float eye[3], uint32_t resx,
+                          uint32_t resy, uint32_t spp, uint32_t max_depth, uint32_t rr_depth, float albedo,
+                          const float lpos[3], const float le1[3], const float le2[3], const float lrad[3],
+                          const float bg[3], float offset, uint32_t seed, const uint32_t* pix,
+                          uint32_t npix_sel, float* image) {
+  const uint32_t npix = pix ? npix_sel : resx * resy;
   const V3 LP = mk(lpos[0], lpos[1], lpos[2]), E1 = mk(le1[0], le1[1], le1[2]),
            E2 = mk(le2[0], le2[1], le2[2]), LR = mk(lrad[0], lrad[1], lrad[2]), BG = mk(bg[0], bg[1], bg[2]);
   const V3 ln = cross(E1, E2);
@@ -1036,7 +1042,7 @@ void orc_pt_render(const orc_grid* G, const float cam9[9], const float eye[3], u
   const float rxf = (float)resx;
 #pragma omp parallel for schedule(dynamic, 64)
   for (int64_t pi = 0; pi < (int64_t)npix; ++pi) {
-    const uint32_t p = (uint32_t)pi;
+    const uint32_t p = pix ? pix[pi] : (uint32_t)pi;
     float ir = 0.f, ig = 0.f, ib = 0.f;
     for (uint32_t s = 0; s < spp; ++s) {
       uint32_t c[4] = {p, s, 0u, 0x4A49u};
@@ -1104,10 +1110,18 @@ void orc_pt_render(const orc_grid* G, const float cam9[9], const float eye[3], u
       ig += L.y;
       ib += L.z;
     }
-    image[3 * (size_t)p] = ir / (float)spp;
-    image[3 * (size_t)p + 1] = ig / (float)spp;
-    image[3 * (size_t)p + 2] = ib / (float)spp;
+    image[3 * (size_t)pi] = ir / (float)spp;
+    image[3 * (size_t)pi + 1] = ig / (float)spp;
+    image[3 * (size_t)pi + 2] = ib / (float)spp;
   }
+}
+
+void orc_pt_render(const orc_grid* G, const float cam9[9], const float eye[3], uint32_t resx,
+                   uint32_t resy, uint32_t spp, uint32_t max_depth, uint32_t rr_depth, float albedo,
+                   const float lpos[3], const float le1[3], const float le2[3], const float lrad[3],
+                   const float bg[3], float offset, uint32_t seed, float* image) {
+  orc_pt_render_pixels(G, cam9, eye, resx, resy, spp, max_depth, rr_depth, albedo, lpos, le1, le2, lrad, bg,
+                       offset, seed, nullptr, 0, image);
 }
 
 // Stable stream compaction: indices of non-zero flags in order.

@@ -52,22 +52,27 @@ uint32_t orc_ao_rays(const float* vtx, const uint32_t* idx, const float* ox, con
                      const float* oz, const float* dx, const float* dy, const float* dz,
                      const uint32_t* tri, const float* t, uint32_t n, uint32_t spp, uint32_t seed,
                      float offset, float* rox, float* roy, float* roz, float* rdx, float* rdy,
-                     float* rdz, uint32_t* rpix);
+                     float* rdz, uint32_t* rpix, const uint32_t* pix);
 uint32_t orc_direct_rays(const float* ox, const float* oy, const float* oz, const float* dx,
                          const float* dy, const float* dz, const uint32_t* tri, const float* t,
                          uint32_t n, uint32_t spp, uint32_t seed, uint32_t image_id,
                          const float* light15, float* rox, float* roy, float* roz, float* rdx,
-                         float* rdy, float* rdz, uint32_t* rpix);
+                         float* rdy, float* rdz, uint32_t* rpix, const uint32_t* pix);
 void orc_shade_direct(const float* vtx, const uint32_t* idx, const float* ox, const float* oy,
                       const float* oz, const float* dx, const float* dy, const float* dz,
                       const uint32_t* tri, const float* t, uint32_t n, uint32_t spp, uint32_t seed,
                       uint32_t image_id, const float* light15, const uint32_t* tri_mat,
                       const float* diffuse, uint32_t nmat, const float* ddef, const float* bg,
-                      const uint8_t* occ, float* frame, float* fin);
+                      const uint8_t* occ, float* frame, float* fin, const uint32_t* pix);
 void orc_pt_render(const orc_grid* g, const float cam9[9], const float eye[3], uint32_t resx,
                    uint32_t resy, uint32_t spp, uint32_t max_depth, uint32_t rr_depth, float albedo,
                    const float lpos[3], const float le1[3], const float le2[3], const float lrad[3],
                    const float bg[3], float offset, uint32_t seed, float* image);
+void orc_pt_render_pixels(const orc_grid* G, const float cam9[9], const float eye[3], uint32_t resx,
+                          uint32_t resy, uint32_t spp, uint32_t max_depth, uint32_t rr_depth, float albedo,
+                          const float lpos[3], const float le1[3], const float le2[3], const float lrad[3],
+                          const float bg[3], float offset, uint32_t seed, const uint32_t* pix,
+                          uint32_t npix_sel, float* image);
 uint32_t orc_compact(const uint32_t* flags, uint32_t n, uint32_t* out);
 
 #endif

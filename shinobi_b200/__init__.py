@@ -67,6 +67,12 @@ class Context:
             msg = self.lib.shn_ctx_last_error(self.handle)
             raise ShinobiError(st, f"{what}: {msg.decode() if msg else ''}")
 
+    def sync_status(self, stream=None):
+        """Synchronise the stream and raise ShinobiError (SHN_ERR_TIMEOUT) if a
+        bounded device wait gave up in a scan, compaction or sort on this
+        context since the last check."""
+        self.check(self.lib.shn_ctx_sync_status(self.handle, _stream(stream)), "shn_ctx_sync_status")
+
     def memory(self):
         used, budget = C.c_uint64(), C.c_uint64()
         self.check(self.lib.shn_ctx_memory(self.handle, C.byref(used), C.byref(budget)), "memory")
@@ -264,6 +270,12 @@ class Grid:
         self.scene = scene  # traces read the scene's triangles (hit records, AO and shading normals)
         return self
 
+    def sync_status(self, stream=None):
+        """Synchronise the stream and raise ShinobiError (SHN_ERR_TIMEOUT) if a
+        bounded device wait gave up in a trace, AO, direct-illumination or
+        path-tracer call on this grid since the last check."""
+        self.ctx.check(self.ctx.lib.shn_grid_sync_status(self.handle, _stream(stream)), "shn_grid_sync_status")
+
     def info(self) -> GridInfo:
         inf = GridInfo()
         self.ctx.check(self.ctx.lib.shn_grid_get_info(self.handle, C.byref(inf)), "shn_grid_get_info")
@@ -441,6 +453,11 @@ class Batch:
 
     def replay(self, stream=None):
         self.ctx.check(self.ctx.lib.shn_batch_replay(self.handle, _stream(stream)), "shn_batch_replay")
+
+    def sync_status(self, stream=None):
+        """Synchronise and raise ShinobiError if a bounded wait gave up (or a replay
+        overflowed its planned pairs) in this batch since the last check."""
+        self.ctx.check(self.ctx.lib.shn_batch_sync_status(self.handle, _stream(stream)), "shn_batch_sync_status")
 
     def export_scene(self, s: int, max_cells: int, max_refs: int):
         res = (C.c_int32 * 3)()

@@ -21,6 +21,7 @@ SHN_OK, SHN_ERR_INVALID, SHN_ERR_CUDA, SHN_ERR_OOM, SHN_ERR_TIMEOUT = 0, 1, 2, 3
 SHN_ERR_BUDGET, SHN_ERR_NOT_BUILT, SHN_ERR_BUSY, SHN_ERR_CANCELLED = 5, 6, 7, 8
 
 SHN_MISS = 0xFFFFFFFF
+SHN_FORCE_CTX_SCAN, SHN_FORCE_GRID_COMPACTION, SHN_FORCE_NOALLOC_SCAN = 1, 2, 3
 SHN_MEM_HOST = 0
 SHN_MEM_DEVICE = 1
 SHN_GRID_UNIFORM = 0
@@ -147,6 +148,11 @@ SIGNATURES = {
     "shn_exclusive_scan_u32_noalloc": ([vp, vp, u32, vp], i32),
     "shn_compact_u32": ([vp, vp, u32, vp, vp, vp], i32),
     "shn_selftest_lookback_timeout": ([vp, vp], i32),
+    "shn_exclusive_scan_u32_noalloc_status": ([vp], i32),
+    "shn_ctx_sync_status": ([vp, vp], i32),
+    "shn_grid_sync_status": ([vp, vp], i32),
+    "shn_batch_sync_status": ([vp, vp], i32),
+    "shn_debug_force_lookback_timeout": ([u32, vp, vp], i32),
     "shn_server_get_records": ([vp, u32, vp, vp], i32),
     "shn_sort_keys_u64": ([vp, vp, vp, u32, u32, u32, vp], i32),
 }

@@ -49,7 +49,7 @@ def build(force: bool = False, verbose: bool = False, jobs: int = 0) -> str:
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         objs.append(obj)
-        cmd = [NVCC, *ARCH, *FLAGS, "-dc" if False else "-c", src, "-o", obj]
+        cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))

@@ -464,7 +464,8 @@ shn_status shn_exclusive_scan_u32(shn_ctx* ctx, const uint32_t* in, uint32_t* ou
   const size_t wb = scan_workspace_bytes(n);
   cudaError_t e = dev_alloc(ctx, &ws, wb, st);
   if (e != cudaSuccess) return alloc_status(ctx, e, "scan workspace");
-  launch_exclusive_scan(in, out, n, ws, ctx->d_err, st);
+  const uint32_t armed = ctx->force_lookback.exchange(0);
+  if (!launch_exclusive_scan(in, out, n, ws, ctx->d_err, st, armed != 0) && armed) ctx->force_lookback.store(armed);
   dev_free(ctx, ws, wb, st);
   e = cudaGetLastError();
   return e == cudaSuccess ? SHN_OK : cuda_status(ctx, e, "exclusive_scan");
@@ -479,7 +480,9 @@ shn_status shn_compact_u32(shn_ctx* ctx, const uint32_t* flags, uint32_t n, uint
   const size_t wb = scan_workspace_bytes(n);
   cudaError_t e = dev_alloc(ctx, &ws, wb, st);
   if (e != cudaSuccess) return alloc_status(ctx, e, "compact workspace");
-  launch_compact(flags, n, out_idx, d_count, ws, ctx->d_err, st);
+  const uint32_t armed = ctx->force_lookback.exchange(0);
+  if (!launch_compact(flags, n, out_idx, d_count, ws, ctx->d_err, st, armed != 0) && armed)
+    ctx->force_lookback.store(armed);
   dev_free(ctx, ws, wb, st);
   e = cudaGetLastError();
   return e == cudaSuccess ? SHN_OK : cuda_status(ctx, e, "compact");
@@ -502,6 +505,67 @@ shn_status shn_sort_keys_u64(shn_ctx* ctx, uint64_t* keys, uint64_t* tmp, uint32
   dev_free(ctx, ws, wb, st);
   e = cudaGetLastError();
   return e == cudaSuccess ? SHN_OK : cuda_status(ctx, e, "sort");
+}
+
+// ---- device-side status -------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+// Synchronises the stream, then reads and clears the error word.
+shn_status read_and_clear(shn_ctx* ctx, uint32_t* d_word, cudaStream_t st, const char* what) {
+  uint32_t* h = pinned_take(ctx);
+  if (!h) return set_error(ctx, SHN_ERR_OOM, "pinned");
+  h[0] = 0;
+  cudaError_t e = cudaMemcpyAsync(h, d_word, 4, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  const uint32_t bits = h[0];
+  pinned_give(ctx, h);
+  if (e != cudaSuccess) return cuda_status(ctx, e, what);
+  if (!bits) return SHN_OK;
+  e = cudaMemsetAsync(d_word, 0, 4, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_status(ctx, e, what);
+  std::string m = std::string(what) + ": a bounded device wait gave up (";
+  if (bits & kErrLookbackTimeout) m += "look-back";
+  if (bits & kErrTmaTimeout) m += (bits & kErrLookbackTimeout) ? ", bulk copy" : "bulk copy";
+  if (bits & kErrCapacity) m += (bits & (kErrLookbackTimeout | kErrTmaTimeout)) ? ", capacity" : "capacity";
+  m += "); the results of the calls since the last check are not valid";
+  return set_error(ctx, (bits & (kErrLookbackTimeout | kErrTmaTimeout)) ? SHN_ERR_TIMEOUT : SHN_ERR_INVALID, m);
+}
+
+}  // namespace
+
+extern "C" {
+
+shn_status shn_ctx_sync_status(shn_ctx* ctx, void* stream) {
+  if (!ctx) return SHN_ERR_INVALID;
+  return read_and_clear(ctx, ctx->d_err, (cudaStream_t)stream, "context primitives");
+}
+
+shn_status shn_grid_sync_status(const shn_grid* g, void* stream) {
+  if (!g) return SHN_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!g->d_err) {  // never built: nothing of this grid ran on the device
+    const cudaError_t e = cudaStreamSynchronize(st);
+    return e == cudaSuccess ? SHN_OK : cuda_status(g->ctx, e, "grid status");
+  }
+  return read_and_clear(g->ctx, g->d_err, st, "grid");
+}
+
+shn_status shn_debug_force_lookback_timeout(uint32_t target, shn_ctx* ctx, shn_grid* g) {
+  if (target == SHN_FORCE_CTX_SCAN) {
+    if (!ctx) return SHN_ERR_INVALID;
+    ctx->force_lookback.store(1);
+    return SHN_OK;
+  }
+  if (target == SHN_FORCE_GRID_COMPACTION) {
+    if (!g) return SHN_ERR_INVALID;
+    g->force_lookback.store(1);
+    return SHN_OK;
+  }
+  if (target == SHN_FORCE_NOALLOC_SCAN) return noalloc_force_lookback_timeout();
+  return SHN_ERR_INVALID;
 }
 
 }  // extern "C"

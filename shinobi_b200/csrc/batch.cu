@@ -448,6 +448,22 @@ shn_status shn_batch_replay(shn_batch* b, void* stream) {
   return e == cudaSuccess ? SHN_OK : cuda_status(b->ctx, e, "batch graph launch");
 }
 
+shn_status shn_batch_sync_status(shn_batch* b, void* stream) {
+  if (!b) return SHN_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(b->h_pinned + 2, b->d_err, 4, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_status(b->ctx, e, "batch status");
+  const uint32_t bits = b->h_pinned[2];
+  if (!bits) return SHN_OK;
+  e = cudaMemsetAsync(b->d_err, 0, 4, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_status(b->ctx, e, "batch status");
+  if (bits & (kErrLookbackTimeout | kErrTmaTimeout))
+    return set_error(b->ctx, SHN_ERR_TIMEOUT, "a bounded device wait gave up in a batch build, trace or replay");
+  return set_error(b->ctx, SHN_ERR_INVALID, "pair capacity exceeded in a batch replay; build again to re-plan");
+}
+
 shn_status shn_batch_autotune(shn_batch* b, const float* candidates, uint32_t num_candidates,
                               const uint32_t* expected_rays, uint32_t sample_rays, uint32_t seed,
                               float* chosen, void* stream) {

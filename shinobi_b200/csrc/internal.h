@@ -33,6 +33,9 @@ struct shn_ctx {
   std::mutex mu;
   std::string last_error;
   uint32_t* d_err = nullptr;    // device error word of context-level primitives
+  // failure-detection self test: the next context-level look-back scan
+  // withholds its first tile (shn_debug_force_lookback_timeout)
+  std::atomic<uint32_t> force_lookback{0};
   // One reference for the handle returned by shn_ctx_create and one per live
   // scene / grid / batch / server: the context (and its memory pool) is torn
   // down when the last of them is released, whatever the destruction order.
@@ -83,8 +86,14 @@ struct shn_grid {
   size_t cap_cells = 0, cap_leaves = 0, cap_refs = 0, cap_rtri = 0;
   // grow-only build workspace
   shn::DevBuf offs_tri, offs_pair, scan, top_ranges, keys[3], sortws;
+  // word 0: error bits of bounded waits that gave up, set by this grid's build
+  // and by every trace call on it; cleared by shn_grid_sync_status (which
+  // reports them) and at the start of each build.  Words 1.. are build scratch.
   uint32_t* d_err = nullptr;
   uint32_t* h_pinned = nullptr; // pinned host words for size read-backs
+  // failure-detection self test: the next hit compaction of an AO or
+  // direct-illumination call withholds its first tile
+  mutable std::atomic<uint32_t> force_lookback{0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float build_ms = 0.f;
   size_t bytes = 0;
@@ -148,10 +157,19 @@ struct CamView;
 CamView make_camera(const shn_camera* c);
 
 // scan.cu (context-level primitives)
-void launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, void* ws, uint32_t* err,
-                           cudaStream_t st);
+// withhold_first: failure-detection self test -- the launch leaves out tile 0
+// (which then never publishes), so the other tiles' look-back waits run out;
+// only honoured when there are at least two tiles (returns whether it was).
+bool launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, void* ws, uint32_t* err,
+                           cudaStream_t st, bool withhold_first = false);
 size_t scan_workspace_bytes(uint32_t n);
-void launch_compact(const uint32_t* flags, uint32_t n, uint32_t* out_idx, uint32_t* d_count,
-                    void* ws, uint32_t* err, cudaStream_t st);
+bool launch_compact(const uint32_t* flags, uint32_t n, uint32_t* out_idx, uint32_t* d_count,
+                    void* ws, uint32_t* err, cudaStream_t st, bool withhold_first = false);
+// Look-back launch shape with tile 0 optionally withheld: sets the ticket
+// word to 1 when withholding and returns the number of blocks to launch.
+uint32_t lookback_blocks(uint32_t tiles, uint32_t* ticket, bool withhold_first, cudaStream_t st);
+
+// scan_noalloc.cu: arms the failure-detection self test of the allocation-free scan
+shn_status noalloc_force_lookback_timeout();
 
 }  // namespace shn

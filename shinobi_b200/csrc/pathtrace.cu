@@ -91,6 +91,10 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_bounce(GridView G, PtView P, Pa
     V3 beta = mk(r.r0.w, r.r1.w, r.r2.w);
     V3 L = mk(r.r2.x, r.r2.y, r.r2.z);
     const uint32_t p = __float_as_uint(r.r3.x), s = __float_as_uint(r.r3.y);
+    if (p >= P.npix || s >= P.spp) {  // record left unwritten by a look-back that gave up
+      alive[i] = 0u;
+      continue;
+    }
     Hit h{FLT_MAX, kMiss, 0.f, 0.f};
     trace_ray<KIND, false>(G, org, dir, h);
     bool live = false;

@@ -46,24 +46,37 @@ static LookbackState prep(void* ws, uint32_t n, uint32_t* err, cudaStream_t st) 
   return LookbackState{status, (uint32_t*)(status + tiles + 1), err};
 }
 
-void launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, void* ws, uint32_t* err,
-                           cudaStream_t st) {
-  if (n == 0) {
-    cudaMemsetAsync(out, 0, 4, st);
-    return;
-  }
-  LookbackState ls = prep(ws, n, err, st);
-  k_exclusive_scan<<<(n + kTile - 1) / kTile, kBlock, 0, st>>>(in, out, n, ls);
+uint32_t lookback_blocks(uint32_t tiles, uint32_t* ticket, bool withhold_first, cudaStream_t st) {
+  if (!withhold_first || tiles < 2) return tiles;
+  static const uint32_t one = 1u;  // tickets start at 1: tile 0 is never taken
+  cudaMemcpyAsync(ticket, &one, 4, cudaMemcpyHostToDevice, st);
+  return tiles - 1;
 }
 
-void launch_compact(const uint32_t* flags, uint32_t n, uint32_t* out_idx, uint32_t* d_count,
-                    void* ws, uint32_t* err, cudaStream_t st) {
+bool launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, void* ws, uint32_t* err,
+                           cudaStream_t st, bool withhold_first) {
   if (n == 0) {
-    cudaMemsetAsync(d_count, 0, 4, st);
-    return;
+    cudaMemsetAsync(out, 0, 4, st);
+    return false;
   }
   LookbackState ls = prep(ws, n, err, st);
-  k_compact<<<(n + kTile - 1) / kTile, kBlock, 0, st>>>(flags, out_idx, n, d_count, ls);
+  const uint32_t tiles = (n + kTile - 1) / kTile;
+  const uint32_t blocks = lookback_blocks(tiles, ls.ticket, withhold_first, st);
+  k_exclusive_scan<<<blocks, kBlock, 0, st>>>(in, out, n, ls);
+  return blocks != tiles;
+}
+
+bool launch_compact(const uint32_t* flags, uint32_t n, uint32_t* out_idx, uint32_t* d_count,
+                    void* ws, uint32_t* err, cudaStream_t st, bool withhold_first) {
+  if (n == 0) {
+    cudaMemsetAsync(d_count, 0, 4, st);
+    return false;
+  }
+  LookbackState ls = prep(ws, n, err, st);
+  const uint32_t tiles = (n + kTile - 1) / kTile;
+  const uint32_t blocks = lookback_blocks(tiles, ls.ticket, withhold_first, st);
+  k_compact<<<blocks, kBlock, 0, st>>>(flags, out_idx, n, d_count, ls);
+  return blocks != tiles;
 }
 
 }  // namespace shn

@@ -24,6 +24,10 @@ constexpr int kSortTile = kSortBlock * kSortItems;  // 4096 keys, 32 KB
 constexpr int kSortWarps = kSortBlock / 32;
 constexpr uint32_t kDigFlagAgg = 1u << 30;
 constexpr uint32_t kDigFlagPrefix = 2u << 30;
+// A tile that gave up (its staged keys never arrived, or its own look-back
+// ran out) publishes this for its digits: later tiles stop looking back,
+// record the error and publish it in turn.
+constexpr uint32_t kDigFlagPoison = 3u << 30;
 constexpr uint32_t kDigValueMask = (1u << 30) - 1u;
 constexpr int kLookback = 8;
 
@@ -61,6 +65,16 @@ __global__ void __launch_bounds__(256) k_sort_hist_scan(uint32_t* hist) {
 }
 
 SHN_D uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+SHN_D uint32_t mbar_try_wait(uint32_t bar) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(bar)
+      : "memory");
+  return done;
+}
 
 __global__ void __launch_bounds__(kSortBlock, 3) k_onesweep(const uint64_t* __restrict__ in,
                                                          uint64_t* __restrict__ out, uint32_t n,
@@ -108,19 +122,30 @@ __global__ void __launch_bounds__(kSortBlock, 3) k_onesweep(const uint64_t* __re
   // keys not covered by the bulk copy are staged with plain loads
   for (uint32_t i = bulk_keys + threadIdx.x; i < count; i += kSortBlock) s_keys[i] = in[base + i];
   __syncthreads();
+  // Bounded wait for the staged tile, taken by the whole block: if any
+  // thread's wait runs out, every thread leaves together.  The tile then
+  // publishes a poisoned status for all 256 digits, so later tiles stop
+  // looking back at once instead of spending their own wait budget on it.
+  int timed_out = 0;
   {
     uint32_t done = 0, spins = 0;
     while (!done) {
-      asm volatile(
-          "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
-          : "=r"(done)
-          : "r"(bar)
-          : "memory");
+      done = mbar_try_wait(bar);
       if (!done && ++spins > kSpinLimit) {
-        atomicOr(err, kErrTmaTimeout);
-        return;
+        timed_out = 1;
+        break;
       }
     }
+  }
+  if (__syncthreads_or(timed_out)) {
+    if (threadIdx.x == 0) atomicOr(err, kErrTmaTimeout);
+    st_release(status + (uint64_t)tile * 256 + threadIdx.x, kDigFlagPoison);
+    // the copy may still be in flight into this block's shared memory: wait
+    // for it once more (bounded) before the block exits
+    uint32_t spins = 0;
+    while (!mbar_try_wait(bar) && ++spins <= kSpinLimit) __nanosleep(64);
+    __syncthreads();
+    return;
   }
 
   // ---- stable rank within each warp's 512-key slice ------------------------
@@ -173,6 +198,7 @@ __global__ void __launch_bounds__(kSortBlock, 3) k_onesweep(const uint64_t* __re
 
   // ---- look-back across tiles for this digit ----------------------------------
   uint32_t excl = 0;
+  bool poisoned = false;
   if (tile != 0) {
     // kLookback predecessors per round trip: the status word carries flag
     // and value together, so relaxed loads suffice and all of a round's
@@ -193,19 +219,24 @@ __global__ void __launch_bounds__(kSortBlock, 3) k_onesweep(const uint64_t* __re
           uint32_t spins = 0;
           while (((v = ld_relaxed(p)) >> 30) == 0u) {
             if (++spins > kSpinLimit) {
-              atomicOr(err, kErrLookbackTimeout);
-              v = kDigFlagPrefix;
+              v = kDigFlagPoison;
               break;
             }
             __nanosleep(20);
           }
+        }
+        if ((v >> 30) == 3u) {  // a predecessor gave up, or this wait ran out
+          atomicOr(err, kErrLookbackTimeout);
+          poisoned = true;
+          done = true;
+          break;
         }
         excl += v & kDigValueMask;
         if ((v >> 30) == 2u) done = true;
       }
       j -= kLookback;
     }
-    st_release(my, kDigFlagPrefix | (excl + tcount));
+    st_release(my, poisoned ? kDigFlagPoison : (kDigFlagPrefix | (excl + tcount)));
   }
   s_gbase[dgt] = digit_base[dgt] + excl - bstart;  // global index = s_gbase[d] + local index
   __syncthreads();

@@ -112,6 +112,7 @@ struct AoParams {
   float len, offset;
   const float4* stri;  // scene triangles, 48-byte records (v0, v1, v2)
   uint32_t snt;
+  uint32_t npix;
 };
 
 template <int KIND, bool STATS>
@@ -129,7 +130,16 @@ __global__ void __launch_bounds__(kTraceBlock, 9) k_trace_ao(GridView G, AoParam
       [&](uint32_t r, V3& o, V3& dir, float& tmax) {
         const uint32_t k = r / A.spp, s = r - k * A.spp;
         const uint32_t p = hit_idx[k];
-        const uint32_t tri = ptri[p];
+        // a compaction whose look-back gave up (error bit set) can leave a
+        // slot unwritten: such a ray becomes an empty segment, no access leaves
+        // the pixel and triangle arrays
+        const uint32_t tri = p < A.npix ? ptri[p] : kMiss;
+        if (tri >= A.snt) {
+          o = A.cam.eye;
+          dir = mk(0.f, 0.f, 1.f);
+          tmax = 0.f;
+          return;
+        }
         const float t = pt[p];
         const V3 d = primary_dir(A.cam, p, A.image_id);
         const float4* rec = A.stri + 3 * (size_t)tri;
@@ -169,7 +179,12 @@ __global__ void k_ao_finalize(const uint32_t* __restrict__ ptri, const uint32_t*
     ao[p] = 1.0f;
     return;
   }
-  const uint32_t b = pos[p] * spp;
+  const uint32_t q = pos[p];
+  if (q >= *d_m) {  // only after a look-back that gave up (error bit set)
+    ao[p] = 1.0f;
+    return;
+  }
+  const uint32_t b = q * spp;
   uint32_t c = 0;
   for (uint32_t s = 0; s < spp; ++s) c += occ[b + s];
   ao[p] = 1.0f - (float)c / (float)spp;
@@ -182,7 +197,7 @@ struct DiParams {
   CamView cam;
   V3 lpos, le1, le2, lnrm, lint, ddef, bg;
   float larea;
-  uint32_t spp, seed, image_id, nmat;
+  uint32_t spp, seed, image_id, nmat, npix;
   const float4* stri;        // scene triangles, 48-byte records (v0, v1, v2)
   const uint32_t* tri_mat;   // per scene triangle, or null
   const float4* diffuse;     // per material, or null
@@ -215,6 +230,12 @@ __global__ void __launch_bounds__(kTraceBlock, 9) k_trace_direct(GridView G, DiP
       [&](uint32_t r, V3& o, V3& dir, float& tmax) {
         const uint32_t k = r / P.spp, s = r - k * P.spp;
         const uint32_t p = hit_idx[k];
+        if (p >= P.npix) {  // slot left unwritten by a look-back that gave up
+          o = P.cam.eye;
+          dir = mk(0.f, 0.f, 1.f);
+          tmax = 0.f;
+          return;
+        }
         di_segment(P, p, s, pt[p], o, dir);
         tmax = 0.9999f;
       },
@@ -253,9 +274,11 @@ __global__ void __launch_bounds__(256) k_shade_direct(DiParams P, const uint32_t
       diff = f4v(__ldg(P.diffuse + m));
     }
     const V3 k = mul(muls(P.lint, P.larea), diff);
-    const uint8_t* oc = occ + (size_t)pos[p] * P.spp;
+    const uint32_t q = pos[p];
+    const bool valid = q < *d_m;  // false only after a look-back that gave up
+    const uint8_t* oc = occ + (size_t)q * P.spp;
     for (uint32_t s = 0; s < P.spp; ++s) {
-      if (oc[s]) continue;
+      if (!valid || oc[s]) continue;
       V3 o, L;
       di_segment(P, p, s, t, o, L);
       const V3 ln = normalize(L);
@@ -479,7 +502,10 @@ shn_status shn_trace_ao(const shn_grid* g, const shn_camera* cam, const shn_hits
   cudaMemsetAsync(status, 0, (tiles + 2) * 8, st);
   LookbackState ls{status, (uint32_t*)(status + tiles + 1), g->d_err};
   uint32_t* d_m = counter + 1;
-  k_compact_hits<<<(unsigned)tiles, 256, 0, st>>>(primary->tri, n, hit_idx, pos, d_m, ls);
+  const uint32_t armed = g->force_lookback.exchange(0);
+  const uint32_t cblocks = lookback_blocks((uint32_t)tiles, ls.ticket, armed != 0, st);
+  if (armed && cblocks == tiles) g->force_lookback.store(armed);
+  k_compact_hits<<<cblocks, 256, 0, st>>>(primary->tri, n, hit_idx, pos, d_m, ls);
   const GridView G = view_of(g);
   AoParams A;
   A.cam = make_camera(cam);
@@ -490,6 +516,7 @@ shn_status shn_trace_ao(const shn_grid* g, const shn_camera* cam, const shn_hits
   A.offset = offset;
   A.stri = g->src_tri;
   A.snt = g->src_nt;
+  A.npix = n;
 #define SHN_LAUNCH_AO(K, S)                                                                       \
   {                                                                                               \
     static int blocks = persistent_blocks(k_trace_ao<K, S>, g->ctx->num_sms);                     \
@@ -551,7 +578,10 @@ shn_status shn_shade_direct(const shn_grid* g, const shn_camera* cam, const shn_
   cudaMemsetAsync(status, 0, (tiles + 2) * 8, st);
   LookbackState ls{status, (uint32_t*)(status + tiles + 1), g->d_err};
   uint32_t* d_m = counter + 1;
-  k_compact_hits<<<(unsigned)tiles, 256, 0, st>>>(primary->tri, n, hit_idx, pos, d_m, ls);
+  const uint32_t armed = g->force_lookback.exchange(0);
+  const uint32_t cblocks = lookback_blocks((uint32_t)tiles, ls.ticket, armed != 0, st);
+  if (armed && cblocks == tiles) g->force_lookback.store(armed);
+  k_compact_hits<<<cblocks, 256, 0, st>>>(primary->tri, n, hit_idx, pos, d_m, ls);
   const GridView G = view_of(g);
   const shn_area_light& l = prm->light;
   DiParams P;
@@ -569,6 +599,7 @@ shn_status shn_shade_direct(const shn_grid* g, const shn_camera* cam, const shn_
   P.seed = prm->seed;
   P.image_id = prm->image_id;
   P.nmat = prm->num_materials;
+  P.npix = n;
   P.stri = g->src_tri;
   P.tri_mat = prm->tri_material;
   P.diffuse = (const float4*)prm->diffuse;

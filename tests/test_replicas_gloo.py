@@ -56,10 +56,13 @@ def test_max_over_ranks_and_value_gloo():
 def _dead_rank_worker(rank, world, port, out):
     sys.path.insert(0, ROOT)
     import bench
-    dist = _init(rank, world, port)
     if rank == 1:
+        _init(rank, world, port)
         os._exit(0)                           # leaves between steps, never joins the collective
     try:
+        # the dead rank may already be gone while this rank still sets up its
+        # connections: an error there ends the collective just the same
+        dist = _init(rank, world, port)
         bench.max_over_ranks(1.0, dist, device="cpu")
         out.put((rank, "completed"))
     except Exception as e:                    # noqa: BLE001

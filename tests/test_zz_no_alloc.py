@@ -32,6 +32,11 @@ def _scan_both(shn, torch, x):
     return ref.cpu().numpy().view(np.uint32), out.cpu().numpy().view(np.uint32)
 
 
+def _status(shn, torch):
+    lib = shn._abi.load()
+    return lib.shn_exclusive_scan_u32_noalloc_status(C.c_void_p(torch.cuda.current_stream().cuda_stream))
+
+
 def test_noalloc_scan_matches_pooled_scan_twice(gpu):
     import torch
 
@@ -44,6 +49,39 @@ def test_noalloc_scan_matches_pooled_scan_twice(gpu):
         ref, out = _scan_both(shn, torch, x)
         assert np.array_equal(out, ref)
         assert out[-1] == np.uint32(x.astype(np.uint64).sum() & 0xFFFFFFFF)
+        assert _status(shn, torch) == 0
+
+
+@pytest.mark.parametrize("n", [0, 1, 2047, 2048, 2049, 1 << 24])
+def test_noalloc_scan_boundary_sizes(gpu, n):
+    """Empty input, one element, one tile and a bit more, and the maximum size
+    (all 8192 tiles of the fixed array)."""
+    import torch
+
+    import shinobi_b200 as shn
+    rng = np.random.default_rng(n + 3)
+    x = rng.integers(0, 50, size=n, dtype=np.uint32)
+    ref, out = _scan_both(shn, torch, x)
+    assert np.array_equal(out, ref)
+    assert _status(shn, torch) == 0
+
+
+def test_noalloc_scan_reports_a_wait_that_gave_up(gpu):
+    """A call whose first tile is withheld: the other tiles' bounded look-back
+    waits run out and shn_exclusive_scan_u32_noalloc_status reports it; the
+    report clears the error, and the next call is correct."""
+    import torch
+
+    import shinobi_b200 as shn
+    lib = shn._abi.load()
+    rng = np.random.default_rng(11)
+    x = rng.integers(0, 1000, size=100_000, dtype=np.uint32)
+    assert lib.shn_debug_force_lookback_timeout(shn._abi.SHN_FORCE_NOALLOC_SCAN, None, None) == 0
+    _scan_both(shn, torch, x)
+    assert _status(shn, torch) == shn._abi.SHN_ERR_TIMEOUT
+    ref, out = _scan_both(shn, torch, x)
+    assert np.array_equal(out, ref)
+    assert _status(shn, torch) == 0
 
 
 def test_noalloc_scan_rejects_sizes_beyond_the_maximum(gpu):
