@@ -122,6 +122,46 @@ shn_status shn_scene_bounds(const shn_scene* s, float out_min_max[6]);
 uint32_t shn_scene_num_triangles(const shn_scene* s);
 void shn_scene_destroy(shn_scene* s);
 
+/* ---- scene files -------------------------------------------------------------
+ * Wavefront OBJ + MTL, camera and area-light configuration files, read with
+ * the reference's parsing rules so that a scene loads into the same
+ * vertices, faces, materials, camera and light:
+ *  - FWObject::read / readMtlLib      -> shn_obj_read
+ *      (src/Loaders/FWObjectReader.cpp:96-502): v / vn / vt, f with v, v/t,
+ *      v//n or v/t/n references (1-based), polygons fanned around their
+ *      first vertex, usemtl (material 0 is "Default", diffuse 0.9774; others
+ *      in order of first use), mtllib files (read after the OBJ, relative to
+ *      its directory; Kd / Ks / Ka / Ns of used materials), then diffuse /= pi
+ *      and specular *= (Ns + 2) / (2 pi) (Material::setupPhongCoefficients,
+ *      src/Loaders/FWObject.hpp:87-91).  Lines the reference rejects are
+ *      skipped and counted.  A face index that is not positive or names a
+ *      missing vertex, or an .mtl file that cannot be opened, makes the call
+ *      fail with SHN_ERR_INVALID (the reference reads out of bounds / throws).
+ *  - CameraManager::read               -> shn_camera_read
+ *      (src/Loaders/CameraManager.cpp:94-158, rotation: :29-63): position,
+ *      orientation, up, rotation (degrees, applied to orientation and up),
+ *      resX, resY, FOV; lines holding '#' are skipped; entries missing from
+ *      the file keep the values *cam holds on entry.
+ *  - LightSourceLoader::loadFromFile   -> shn_light_read
+ *      (src/Loaders/LightSourceLoader.cpp:26-89): position, normal,
+ *      intensity, edge1, edge2; a missing normal is normalize(edge1 x edge2). */
+typedef struct shn_obj shn_obj;
+typedef struct shn_obj_info {
+  uint32_t num_vertices, num_faces, num_materials, num_normals, num_texcoords;
+  uint64_t skipped_lines;
+} shn_obj_info;
+shn_status shn_obj_read(const char* path, shn_obj** out);
+shn_status shn_obj_get_info(const shn_obj* o, shn_obj_info* info);
+/* Copies (any pointer may be NULL): vertices 3*num_vertices floats, faces
+ * 3*num_faces vertex indices (0-based), face_material num_faces material ids,
+ * diffuse and specular 4*num_materials floats (rgb after the Phong setup;
+ * diffuse .w = 0, specular .w = Ns). */
+shn_status shn_obj_copy(const shn_obj* o, float* vertices, uint32_t* faces, uint32_t* face_material,
+                        float* diffuse, float* specular);
+/* Name of material m (valid until shn_obj_destroy), NULL if out of range. */
+const char* shn_obj_material_name(const shn_obj* o, uint32_t m);
+void shn_obj_destroy(shn_obj* o);
+
 /* ---- grid build ------------------------------------------------------------ */
 #define SHN_GRID_UNIFORM 0u
 #define SHN_GRID_TWO_LEVEL 1u
@@ -266,6 +306,9 @@ typedef struct shn_di_params {
 } shn_di_params;
 
 void shn_di_params_default(shn_di_params* p);
+/* Scene files of the camera and the area light (see "scene files" above). */
+shn_status shn_camera_read(const char* path, shn_camera* cam);
+shn_status shn_light_read(const char* path, shn_area_light* light);
 shn_status shn_shade_direct(const shn_grid* g, const shn_camera* cam, const shn_hits* primary,
                             const shn_di_params* p, float* d_frame, float* d_final,
                             uint32_t* d_num_rays, void* stream);
@@ -479,9 +522,10 @@ shn_status shn_selftest_lookback_timeout(shn_ctx* ctx, void* stream);
  * order; *d_count = m (device). */
 shn_status shn_compact_u32(shn_ctx* ctx, const uint32_t* d_flags, uint32_t n, uint32_t* d_out_idx,
                            uint32_t* d_count, void* stream);
-/* Stable LSD radix sort of 64-bit keys on bits [lo_bit, hi_bit) (8-bit
- * digits, one onesweep pass per digit).  d_tmp has n entries; the sorted
- * keys end in d_keys.  n < 2^30. */
+/* Stable LSD radix sort of 64-bit keys on bits [lo_bit, hi_bit), at most 32
+ * bits (one onesweep pass per 8- or 9-bit digit, whichever width needs fewer
+ * passes; bits outside the range do not affect the order).  d_tmp has n
+ * entries; the sorted keys end in d_keys.  n < 2^30. */
 shn_status shn_sort_keys_u64(shn_ctx* ctx, uint64_t* d_keys, uint64_t* d_tmp, uint32_t n,
                              uint32_t lo_bit, uint32_t hi_bit, void* stream);
 

@@ -58,6 +58,8 @@ def lib():
         L.orc_build_two_level.argtypes = [vp, u32, vp, u32, vp, vp, f32, u32]
         L.orc_build_two_level.restype = vp
         L.orc_grid_free.argtypes = [vp]
+        L.orc_set_reference_arithmetic.argtypes = [i32]
+        L.orc_leaf_res_reference.argtypes = [vp, f32, u32, vp]
         L.orc_grid_from_arrays.argtypes = [i32, vp, vp, vp, vp, C.c_uint64, vp, C.c_uint64, vp, u32, vp, u32]
         L.orc_grid_from_arrays.restype = vp
         L.orc_grid_info.argtypes = [vp, vp]
@@ -104,6 +106,12 @@ def ref_lib():
         R.ref_mt_closest.argtypes = [vp, vp, u32, vp, vp, u32, vp, vp]
         R.ref_cosine_sample.argtypes = [vp, vp, u32, vp]
         R.ref_cell_word.argtypes = [u32, u32, u32, i32, u32, vp]
+        R.ref_obj_read.argtypes = [C.c_char_p, vp]
+        R.ref_obj_read.restype = vp
+        R.ref_obj_copy.argtypes = [vp, vp, vp, vp, vp]
+        R.ref_obj_free.argtypes = [vp]
+        R.ref_camera_read.argtypes = [C.c_char_p, vp]
+        R.ref_light_read.argtypes = [C.c_char_p, vp]
         _ref = R
     return _ref
 
@@ -198,6 +206,38 @@ def ref_host_build(vtx, idx, b, res):
     R.ref_host_build_copy(h, _p(cells), _p(leaves), _p(refs))
     R.ref_host_build_free(h)
     return cells, leaves, refs
+
+
+def ref_read_obj(path: str) -> dict:
+    """The reference's FWObject::read (compiled in place): vertices, indices,
+    face_material, and per material diffuse rgb, specular rgb, Ns."""
+    R = ref_lib()
+    if R is None:
+        raise RuntimeError("reference checker library not built (oracle/_ref)")
+    sizes = np.zeros(3, np.uint64)
+    h = R.ref_obj_read(str(path).encode(), _p(sizes))
+    nv, nf, nm = (int(x) for x in sizes)
+    v = np.zeros((nv, 3), np.float32)
+    f = np.zeros((nf, 3), np.uint64)
+    fm = np.zeros(nf, np.uint64)
+    mt = np.zeros((nm, 7), np.float32)
+    R.ref_obj_copy(h, _p(v), _p(f), _p(fm), _p(mt))
+    R.ref_obj_free(h)
+    return {"vertices": v, "indices": f, "face_material": fm, "materials": mt}
+
+
+def ref_read_camera(path: str) -> np.ndarray:
+    """CameraManager::read from its defaults: position, orientation, up, FOV, resX, resY."""
+    out = np.zeros(12, np.float32)
+    ref_lib().ref_camera_read(str(path).encode(), _p(out))
+    return out
+
+
+def ref_read_light(path: str) -> np.ndarray:
+    """LightSourceLoader::loadFromFile: position, edge1, edge2, normal, intensity (15 floats)."""
+    out = np.zeros(15, np.float32)
+    ref_lib().ref_light_read(str(path).encode(), _p(out))
+    return out
 
 
 def trace_closest(g: Grid, org, dirs, tmax=None):
@@ -377,6 +417,25 @@ def compact(flags) -> np.ndarray:
     out = np.zeros(flags.size, np.uint32)
     m = lib().orc_compact(_p(flags), flags.size, _p(out))
     return out[:m]
+
+
+DIRECT_CENTRES, REF_LEAF_POW = 1, 2
+
+
+def set_reference_arithmetic(flags: int) -> None:
+    """Switch the oracle's build to other arithmetic in the given places, to
+    count how far it is from the canonical build: DIRECT_CENTRES (plane-test
+    centres computed per cell instead of accumulated as the reference does),
+    REF_LEAF_POW (the reference's powf leaf-resolution rule instead of the exact
+    cube root); 0 restores the canonical build."""
+    lib().orc_set_reference_arithmetic(int(flags))
+
+
+def leaf_res_reference(g: Grid, lambda_leaf: float, threshold: int = 16) -> np.ndarray:
+    """(C_top, 3) leaf resolutions as the reference's powf rule gives them, unclamped."""
+    out = np.zeros((int(np.prod(g.res)), 3), np.uint32)
+    lib().orc_leaf_res_reference(g.handle, lambda_leaf, threshold, _p(out))
+    return out
 
 
 def set_threads(n: int) -> None:

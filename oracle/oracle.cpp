@@ -17,8 +17,6 @@
 //  * candidate cells rejected by the plane test are not emitted at all, so
 //    no sentinel pairs reach the sorted arrays or indices[]
 //    (reference: src/Control/Algorithm/FastBuildKernels.h:185-192);
-//  * cell centres for the plane test are (i*s + o) + s/2 per cell instead
-//    of an accumulated "+= cellSize" (see lattice_centre);
 //  * normals use 1/sqrtf instead of rsqrtf, divisions are IEEE instead of
 //    __fdividef;
 //  * leaf resolution is floor(cbrt(cs_a^3 * lambda * refs / V)) evaluated
@@ -118,15 +116,35 @@ Geom make_geom(const float b[6], const int res[3]) {
 }
 
 // ---------------------------------------------------------------------------
-// Centre of cell i along one axis of a lattice with cell size s and origin o:
-// (i*s + o) + s/2, evaluated directly for every cell.  The reference starts
-// from the same expression at the first candidate cell and then accumulates
-// "+= cellSize" (src/Control/Algorithm/FastBuildKernels.h:144-164,
-// src/Control/Algorithm/TwoLevelBuildKernels.h:396-420); the direct form
-// differs from the accumulated one only by rounding and makes every cell's
-// plane test independent of the others, which the CUDA build relies on to
-// find the passing cells of a row as one interval.
+// Cell centres for the plane test, as the reference computes them: along each
+// axis the centre of the first candidate cell is (lo*s + o) + s/2, the loop
+// starts one cell before it and adds "+= cellSize" per cell
+// (src/Control/Algorithm/FastBuildKernels.h:144-164,
+// src/Control/Algorithm/TwoLevelBuildKernels.h:396-420).
+inline void accumulated_centres(uint32_t lo, uint32_t hi, float s, float o, float half, std::vector<float>& out) {
+  out.resize(hi - lo + 1);
+  float c = (((float)lo * s + o) + half) - s;
+  for (uint32_t i = lo; i <= hi; ++i) {
+    c += s;
+    out[i - lo] = c;
+  }
+}
+
+// The same centre computed directly per cell, (i*s + o) + s/2: an earlier
+// canonical form of this build, kept to count how far it was from the
+// reference's (kDirectCentres).
 inline float lattice_centre(uint32_t i, float s, float o) { return ((float)i * s + o) + s * 0.5f; }
+
+// Variants, used only to count how far other arithmetic is from the build
+// above (the counts are asserted by a test so that a change cannot move them
+// silently):
+//  kDirectCentres: centres computed per cell instead of accumulated;
+//  kRefLeafPow: leaf resolution cs_a * powf(lambda * refs / V, 0.3333333f)
+//    truncated, as countLeafLevelCells evaluates it (host powf), then clamped
+//    to [1, 255] like the canonical rule (the reference's zero and 8-bit-wrap
+//    cases are counted separately by orc_leaf_res_reference).
+const int kDirectCentres = 1, kRefLeafPow = 2;
+int g_ref_arith = 0;
 
 // ---------------------------------------------------------------------------
 // Candidate cell range of a triangle in a uniform grid.
@@ -152,12 +170,19 @@ inline void for_each_cell(const Tri& tri, const Geom& g, F&& emit) {
   if (hi[0] - lo[0] > 0 && hi[1] - lo[1] > 0 && hi[2] - lo[2] > 0) {
     const V3 n = normalize(cross(sub(tri.v[1], tri.v[0]), sub(tri.v[2], tri.v[0])));
     const V3 half = muls(g.cs, 0.5f);
+    const bool acc = (g_ref_arith & kDirectCentres) == 0;
+    thread_local std::vector<float> ax, ay, az;
+    if (acc) {
+      accumulated_centres(lo[0], hi[0], g.cs.x, g.gmin.x, half.x, ax);
+      accumulated_centres(lo[1], hi[1], g.cs.y, g.gmin.y, half.y, ay);
+      accumulated_centres(lo[2], hi[2], g.cs.z, g.gmin.z, half.z, az);
+    }
     for (uint32_t z = lo[2]; z <= hi[2]; ++z) {
-      const float cz = lattice_centre(z, g.cs.z, g.gmin.z);
+      const float cz = acc ? az[z - lo[2]] : lattice_centre(z, g.cs.z, g.gmin.z);
       for (uint32_t y = lo[1]; y <= hi[1]; ++y) {
-        const float cy = lattice_centre(y, g.cs.y, g.gmin.y);
+        const float cy = acc ? ay[y - lo[1]] : lattice_centre(y, g.cs.y, g.gmin.y);
         for (uint32_t x = lo[0]; x <= hi[0]; ++x) {
-          const float cx = lattice_centre(x, g.cs.x, g.gmin.x);
+          const float cx = acc ? ax[x - lo[0]] : lattice_centre(x, g.cs.x, g.gmin.x);
           const float d = dot(sub(mk(cx, cy, cz), tri.v[0]), n);
           const V3 dist = muls(n, d);
           if (fabsf(dist.x) <= half.x + kEps && fabsf(dist.y) <= half.y + kEps &&
@@ -197,6 +222,16 @@ uint32_t largest_cube_root_floor(double q) {
 void leaf_res(const Geom& g, float lambda, uint32_t refs, uint32_t threshold, uint32_t out[3]) {
   if (refs <= threshold) {
     out[0] = out[1] = out[2] = 1;
+    return;
+  }
+  if (g_ref_arith & kRefLeafPow) {
+    const float vol = (g.cs.x * g.cs.y) * g.cs.z;
+    const float magic = powf(lambda * (float)refs / vol, 0.3333333f);
+    for (int a = 0; a < 3; ++a) {
+      const float r = at(g.cs, a) * magic;
+      const uint32_t ri = r >= 4294967296.f ? 0xFFFFFFFFu : (uint32_t)r;
+      out[a] = std::min<uint32_t>(255u, std::max<uint32_t>(1u, ri));
+    }
     return;
   }
   const double vol = ((double)g.cs.x * (double)g.cs.y) * (double)g.cs.z;
@@ -239,12 +274,19 @@ inline void for_each_leaf(const Tri& tri, const Geom& g, uint32_t topCell, uint3
   if (hp[0] - lo[0] > 1 && hp[1] - lo[1] > 1 && hp[2] - lo[2] > 1) {
     const V3 n = normalize(cross(sub(tri.v[1], tri.v[0]), sub(tri.v[2], tri.v[0])));
     const V3 scs = divv(g.cs, cres);
+    const bool acc = (g_ref_arith & kDirectCentres) == 0;
+    thread_local std::vector<float> ax, ay, az;
+    if (acc) {
+      accumulated_centres((uint32_t)lo[0], (uint32_t)hp[0] - 1, scs.x, origin.x, scs.x * 0.5f, ax);
+      accumulated_centres((uint32_t)lo[1], (uint32_t)hp[1] - 1, scs.y, origin.y, scs.y * 0.5f, ay);
+      accumulated_centres((uint32_t)lo[2], (uint32_t)hp[2] - 1, scs.z, origin.z, scs.z * 0.5f, az);
+    }
     for (int z = lo[2]; z < hp[2]; ++z) {
-      const float cz = lattice_centre((uint32_t)z, scs.z, origin.z);
+      const float cz = acc ? az[z - lo[2]] : lattice_centre((uint32_t)z, scs.z, origin.z);
       for (int y = lo[1]; y < hp[1]; ++y) {
-        const float cy = lattice_centre((uint32_t)y, scs.y, origin.y);
+        const float cy = acc ? ay[y - lo[1]] : lattice_centre((uint32_t)y, scs.y, origin.y);
         for (int x = lo[0]; x < hp[0]; ++x) {
-          const float cx = lattice_centre((uint32_t)x, scs.x, origin.x);
+          const float cx = acc ? ax[x - lo[0]] : lattice_centre((uint32_t)x, scs.x, origin.x);
           const float d = dot(sub(mk(cx, cy, cz), tri.v[0]), n);
           const V3 dist = muls(n, d);
           if (fabsf(dist.x) <= scs.x * 0.5f + kEps && fabsf(dist.y) <= scs.y * 0.5f + kEps &&
@@ -408,6 +450,31 @@ orc_grid* orc_grid_from_arrays(int kind, const float bounds[6], const int res[3]
 }
 
 void orc_grid_free(orc_grid* G) { delete G; }
+
+void orc_set_reference_arithmetic(int flags) { g_ref_arith = flags; }
+
+// The reference's leaf resolution of every top cell of a two-level grid
+// exactly as countLeafLevelCells evaluates it on the host (powf, truncation,
+// no clamping: src/Control/Algorithm/TwoLevelBuildKernels.h:48-81): out
+// receives 3 uint32 per top cell (1,1,1 for cells of <= threshold refs).
+void orc_leaf_res_reference(const orc_grid* G, float lambda, uint32_t threshold, uint32_t* out) {
+  const Geom& g = G->g;
+  const size_t C = (size_t)g.res[0] * g.res[1] * g.res[2];
+  std::vector<uint32_t> refs(C, 0u);
+  for (uint64_t k : G->top_pairs) ++refs[(size_t)(k >> 32)];
+  const float vol = (g.cs.x * g.cs.y) * g.cs.z;
+  for (size_t c = 0; c < C; ++c) {
+    if (refs[c] <= threshold) {
+      out[3 * c] = out[3 * c + 1] = out[3 * c + 2] = 1u;
+      continue;
+    }
+    const float magic = powf(lambda * (float)refs[c] / vol, 0.3333333f);
+    for (int a = 0; a < 3; ++a) {
+      const float r = at(g.cs, a) * magic;
+      out[3 * c + a] = r >= 4294967296.f ? 0xFFFFFFFFu : (uint32_t)r;
+    }
+  }
+}
 
 void orc_grid_info(const orc_grid* G, uint64_t out[8]) {
   out[0] = (uint64_t)G->kind;

@@ -20,6 +20,8 @@ orc_grid* orc_grid_from_arrays(int kind, const float bounds[6], const int res[3]
                                const uint32_t* indices, uint64_t nrefs, const float* vtx,
                                uint32_t nv, const uint32_t* idx, uint32_t nt);
 void orc_grid_free(orc_grid* g);
+void orc_set_reference_arithmetic(int flags);
+void orc_leaf_res_reference(const orc_grid* G, float lambda, uint32_t threshold, uint32_t* out);
 void orc_grid_info(const orc_grid* g, uint64_t out[8]);
 const uint32_t* orc_grid_cells(const orc_grid* g);
 const uint32_t* orc_grid_leaves(const orc_grid* g);

@@ -18,6 +18,9 @@
 #include <vector>
 
 #include "Control/Algorithm/TwoLevelGridBuilder.hpp"
+#include "Loaders/CameraManager.hpp"
+#include "Loaders/FWObject.hpp"
+#include "Loaders/LightSourceLoader.hpp"
 #include "Intersector/SimpleIntersector.hpp"
 #include "Primitive/Camera.h"
 #include "Primitive/PixelSampler.h"
@@ -198,6 +201,67 @@ void ref_cell_word(uint32_t rx, uint32_t ry, uint32_t rz, int not_empty, uint32_
   c.setLeafRangeBegin(leaf_begin);
   out[0] = c.data.x;
   out[1] = c.data.y;
+}
+
+// FWObject::read (src/Loaders/FWObjectReader.cpp:193-502): sizes = {vertices,
+// faces, materials}; the object is returned for ref_obj_copy.
+void* ref_obj_read(const char* path, uint64_t sizes[3]) {
+  FWObject* o = new FWObject();
+  o->read(path);
+  sizes[0] = o->getNumVertices();
+  sizes[1] = o->getNumFaces();
+  sizes[2] = o->getNumMaterials();
+  return o;
+}
+
+// vertices 3*nv, faces 3*nf (vert1..3), face material nf, per material
+// diffuse rgb + specular rgb + Ns (7 floats).
+void ref_obj_copy(void* h, float* vertices, uint64_t* faces, uint64_t* face_material, float* materials) {
+  FWObject* o = (FWObject*)h;
+  for (size_t i = 0; i < o->getNumVertices(); ++i) {
+    const vec3f v = o->getVertex(i);
+    vertices[3 * i] = v.x; vertices[3 * i + 1] = v.y; vertices[3 * i + 2] = v.z;
+  }
+  for (size_t i = 0; i < o->getNumFaces(); ++i) {
+    const FWObject::Face f = o->getFace(i);
+    faces[3 * i] = f.vert1; faces[3 * i + 1] = f.vert2; faces[3 * i + 2] = f.vert3;
+    face_material[i] = f.material;
+  }
+  for (size_t m = 0; m < o->getNumMaterials(); ++m) {
+    const FWObject::Material& mt = o->getMaterial(m);
+    float* d = materials + 7 * m;
+    d[0] = mt.diffuseCoeff.x; d[1] = mt.diffuseCoeff.y; d[2] = mt.diffuseCoeff.z;
+    d[3] = mt.specularCoeff.x; d[4] = mt.specularCoeff.y; d[5] = mt.specularCoeff.z;
+    d[6] = mt.specularExp;
+  }
+}
+
+void ref_obj_free(void* h) { delete (FWObject*)h; }
+
+// CameraManager::read (src/Loaders/CameraManager.cpp:94-158) from the
+// CameraManager defaults: out = position, orientation, up (after the file's
+// rotation), FOV, resX, resY.
+void ref_camera_read(const char* path, float out[12]) {
+  CameraManager c;
+  c.read(path);
+  const vec3f p = c.getPosition(), o = c.getOrientation(), u = c.getUp();
+  out[0] = p.x; out[1] = p.y; out[2] = p.z;
+  out[3] = o.x; out[4] = o.y; out[5] = o.z;
+  out[6] = u.x; out[7] = u.y; out[8] = u.z;
+  out[9] = c.getFOV();
+  out[10] = (float)c.getResX();
+  out[11] = (float)c.getResY();
+}
+
+// LightSourceLoader::loadFromFile (src/Loaders/LightSourceLoader.cpp:26-89):
+// out = position, edge1, edge2, normal, intensity.
+void ref_light_read(const char* path, float out[15]) {
+  LightSourceLoader l;
+  const AreaLightSource a = l.loadFromFile(path);
+  const vec3f v[5] = {a.position, a.edge1, a.edge2, a.normal, a.intensity};
+  for (int k = 0; k < 5; ++k) {
+    out[3 * k] = v[k].x; out[3 * k + 1] = v[k].y; out[3 * k + 2] = v[k].z;
+  }
 }
 
 }  // extern "C"

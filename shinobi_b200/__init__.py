@@ -25,7 +25,7 @@ from ._abi import (SHN_GRID_TWO_LEVEL, SHN_GRID_UNIFORM, SHN_MEM_DEVICE, SHN_MEM
 
 __all__ = ["ShinobiError", "Context", "FaceSoup", "Grid", "grid_params", "SHN_MISS",
            "SHN_GRID_UNIFORM", "SHN_GRID_TWO_LEVEL", "exclusive_scan", "compact", "sort_keys",
-           "camera_struct", "default_context"]
+           "camera_struct", "default_context", "read_obj", "read_camera", "read_light"]
 
 
 class ShinobiError(RuntimeError):
@@ -578,6 +578,60 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+# ---- scene files ------------------------------------------------------------------
+def read_obj(path: str) -> dict:
+    """Wavefront OBJ + MTL with the reference's parsing rules (FWObject::read):
+    dict(vertices (nv,3) float32, indices (nf,3) uint32, face_material (nf,)
+    uint32, diffuse (nm,4) float32 (Phong-normalised, .w 0), specular (nm,4)
+    (.w = Ns), material_names, skipped_lines)."""
+    lib = _abi.load()
+    h = C.c_void_p()
+    st = lib.shn_obj_read(str(path).encode(), C.byref(h))
+    if st != 0:
+        raise ShinobiError(st, f"shn_obj_read {path}")
+    try:
+        inf = _abi.ObjInfo()
+        lib.shn_obj_get_info(h, C.byref(inf))
+        v = np.zeros((inf.num_vertices, 3), np.float32)
+        f = np.zeros((inf.num_faces, 3), np.uint32)
+        fm = np.zeros(inf.num_faces, np.uint32)
+        d = np.zeros((inf.num_materials, 4), np.float32)
+        sp = np.zeros((inf.num_materials, 4), np.float32)
+        lib.shn_obj_copy(h, v.ctypes.data_as(C.c_void_p), f.ctypes.data_as(C.c_void_p),
+                         fm.ctypes.data_as(C.c_void_p), d.ctypes.data_as(C.c_void_p), sp.ctypes.data_as(C.c_void_p))
+        names = [lib.shn_obj_material_name(h, m).decode() for m in range(inf.num_materials)]
+        return {"vertices": v, "indices": f, "face_material": fm, "diffuse": d, "specular": sp,
+                "material_names": names, "skipped_lines": int(inf.skipped_lines),
+                "num_normals": int(inf.num_normals), "num_texcoords": int(inf.num_texcoords)}
+    finally:
+        lib.shn_obj_destroy(h)
+
+
+def read_camera(path: str, defaults=None):
+    """camera.cfg with the reference's rules (CameraManager::read): returns a
+    scenes.Camera; entries missing from the file keep the defaults' values."""
+    from .scenes import Camera
+    lib = _abi.load()
+    # the reference's CameraManager defaults: position 0, orientation +z, up -y, 512x512, 66 degrees
+    defaults = defaults or Camera((0.0, 0.0, 0.0), (0.0, 0.0, 1.0), (0.0, -1.0, 0.0), 66.0, 512, 512)
+    c = camera_struct(defaults)
+    st = lib.shn_camera_read(str(path).encode(), C.byref(c))
+    if st != 0:
+        raise ShinobiError(st, f"shn_camera_read {path}")
+    return Camera(tuple(c.eye), tuple(c.forward), tuple(c.up), float(c.fov_deg), int(c.res_x), int(c.res_y))
+
+
+def read_light(path: str) -> dict:
+    """light.cfg with the reference's rules (LightSourceLoader::loadFromFile): a
+    dict of the area light's fields, usable as di_params(light=...)."""
+    lib = _abi.load()
+    l = _abi.AreaLight()
+    st = lib.shn_light_read(str(path).encode(), C.byref(l))
+    if st != 0:
+        raise ShinobiError(st, f"shn_light_read {path}")
+    return {k: tuple(getattr(l, k)) for k in ("position", "edge1", "edge2", "normal", "intensity")}
 
 
 def exclusive_scan(x, ctx: Context | None = None, stream=None):

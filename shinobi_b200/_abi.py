@@ -63,6 +63,11 @@ class AreaLight(C.Structure):
                 ("intensity", f32 * 3)]
 
 
+class ObjInfo(C.Structure):
+    _fields_ = [("num_vertices", u32), ("num_faces", u32), ("num_materials", u32), ("num_normals", u32),
+                ("num_texcoords", u32), ("skipped_lines", u64)]
+
+
 class DiParams(C.Structure):
     _fields_ = [("light", AreaLight), ("samples", u32), ("seed", u32), ("image_id", u32),
                 ("tri_material", vp), ("diffuse", vp), ("num_materials", u32),
@@ -153,6 +158,13 @@ SIGNATURES = {
     "shn_grid_sync_status": ([vp, vp], i32),
     "shn_batch_sync_status": ([vp, vp], i32),
     "shn_debug_force_lookback_timeout": ([u32, vp, vp], i32),
+    "shn_obj_read": ([C.c_char_p, C.POINTER(vp)], i32),
+    "shn_obj_get_info": ([vp, C.POINTER(ObjInfo)], i32),
+    "shn_obj_copy": ([vp, vp, vp, vp, vp, vp], i32),
+    "shn_obj_material_name": ([vp, u32], C.c_char_p),
+    "shn_obj_destroy": ([vp], None),
+    "shn_camera_read": ([C.c_char_p, C.POINTER(Camera)], i32),
+    "shn_light_read": ([C.c_char_p, C.POINTER(AreaLight)], i32),
     "shn_server_get_records": ([vp, u32, vp, vp], i32),
     "shn_sort_keys_u64": ([vp, vp, vp, u32, u32, u32, vp], i32),
 }

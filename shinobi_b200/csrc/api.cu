@@ -492,15 +492,14 @@ shn_status shn_sort_keys_u64(shn_ctx* ctx, uint64_t* keys, uint64_t* tmp, uint32
                              uint32_t lo_bit, uint32_t hi_bit, void* stream) {
   if (!ctx || (n && (!keys || !tmp)) || hi_bit > 64 || lo_bit > hi_bit) return SHN_ERR_INVALID;
   if (n >= (1u << 30)) return set_error(ctx, SHN_ERR_INVALID, "n >= 2^30");
-  const uint32_t passes = (hi_bit - lo_bit + 7) / 8;
-  if (passes > 4) return set_error(ctx, SHN_ERR_INVALID, "at most 32 key bits per sort");
-  if (lo_bit + 8 * passes > 64) return set_error(ctx, SHN_ERR_INVALID, "digit range beyond bit 64");
+  if (hi_bit - lo_bit > 32) return set_error(ctx, SHN_ERR_INVALID, "at most 32 key bits per sort");
+  const SortPlan plan = sort_plan(hi_bit - lo_bit);
   cudaStream_t st = (cudaStream_t)stream;
   void* ws = nullptr;
   const size_t wb = sort_workspace_bytes(n);
   cudaError_t e = dev_alloc(ctx, &ws, wb, st);
   if (e != cudaSuccess) return alloc_status(ctx, e, "sort workspace");
-  uint64_t* res = onesweep_sort(keys, tmp, n, lo_bit, passes, ws, ctx->d_err, st);
+  uint64_t* res = onesweep_sort(keys, tmp, n, lo_bit, plan, ws, ctx->d_err, st);
   if (res != keys && n) cudaMemcpyAsync(keys, res, (size_t)n * 8, cudaMemcpyDeviceToDevice, st);
   dev_free(ctx, ws, wb, st);
   e = cudaGetLastError();

@@ -42,7 +42,7 @@ struct shn_batch {
   uint32_t* h_pinned = nullptr;
   uint64_t total_cells = 0;
   uint32_t P = 0;                      // planned pair count
-  uint32_t passes = 0;
+  shn::SortPlan plan{0, 8, 0};             // digit plan of the sort over the global cell bits
   uint64_t* sorted = nullptr;
   bool planned = false, built = false;
   std::vector<std::pair<void*, size_t>> owned;   // (ptr, bytes) of plan-time buffers
@@ -214,7 +214,7 @@ shn_status plan(shn_batch* b, cudaStream_t st) {
   if (b->h_pinned[1]) return set_error(b->ctx, SHN_ERR_TIMEOUT, "bounded device wait gave up (batch plan)");
   b->P = b->h_pinned[0];
   if (b->P >= (1u << 30)) return set_error(b->ctx, SHN_ERR_INVALID, "more than 2^30 cell references in the batch");
-  b->passes = sort_passes_for(co ? co - 1 : 0);
+  b->plan = sort_plan(key_bits_for(co ? co - 1 : 0));
   e = own(b, (void**)&b->keys[0], (size_t)b->P * 8, st);
   if (e == cudaSuccess) e = own(b, (void**)&b->keys[1], (size_t)b->P * 8, st);
   if (e == cudaSuccess) e = own(b, &b->sort_ws, sort_workspace_bytes(b->P), st);
@@ -229,8 +229,10 @@ shn_status plan(shn_batch* b, cudaStream_t st) {
 void enqueue_build(shn_batch* b, cudaStream_t st) {
   cudaMemsetAsync(b->d_err, 0, 4, st);
   launch_batch_count(b->tri, b->T, b->d_tri_off, b->d_scenes, b->ns, b->scan_ws, b->d_err, b->offs, st);
-  launch_batch_emit(b->tri, b->T, b->d_tri_off, b->d_scenes, b->ns, b->offs, b->keys[0], b->P, b->d_err, st);
-  b->sorted = onesweep_sort(b->keys[0], b->keys[1], b->P, 32, b->passes, b->sort_ws, b->d_err, st);
+  sort_prepare(b->sort_ws, st);
+  launch_batch_emit(b->tri, b->T, b->d_tri_off, b->d_scenes, b->ns, b->offs, b->keys[0], b->P, b->d_err,
+                    sort_hist_counts(b->sort_ws), b->plan, st);
+  b->sorted = onesweep_sort(b->keys[0], b->keys[1], b->P, 32, b->plan, b->sort_ws, b->d_err, st, true);
   cudaMemsetAsync(b->cells, 0, b->total_cells * 8, st);
   // no reference-ordered triangle copy: the batch's cells hold a few
   // references each and the trace reads a reference's triangle through its

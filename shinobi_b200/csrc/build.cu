@@ -235,21 +235,34 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_inplace(uint32_t* data, uin
 }
 
 // Keys of every item at offs[item]: 32 items per warp step, coalesced stores.
+// hist (optional): the sort's digit counts ([pass][512]) of the keys' cell
+// bits under the sort plan hp, counted here so that the sort needs no
+// histogram pass over the keys.
 template <class Maker>
 __global__ void __launch_bounds__(kScanBlock) k_emit_units(Maker mk, uint32_t n,
                                                           const uint32_t* __restrict__ offs,
                                                           uint64_t* __restrict__ keys, uint32_t cap,
-                                                          uint32_t* err) {
+                                                          uint32_t* err, uint32_t* hist, SortPlan hp) {
   __shared__ Unit su[kUnitWarps][32];
+  __shared__ uint32_t shist[4 * 512];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (hist) {
+    for (int i = threadIdx.x; i < 4 * 512; i += kScanBlock) shist[i] = 0u;
+    __syncthreads();
+  }
   const uint32_t groups = (n + 31u) / 32u;
   for (uint32_t gi = blockIdx.x * kUnitWarps + warp; gi < groups; gi += gridDim.x * kUnitWarps) {
     const uint32_t i = gi * 32u + lane;
     const bool valid = i < n && mk(i, su[warp][lane]);
     const uint32_t out = offs[gi * 32u];
     __syncwarp();
-    warp_emit_units(su[warp], valid, out, keys, cap, err);
+    warp_emit_units(su[warp], valid, out, keys, cap, err, hist ? shist : nullptr, hist ? hp.passes : 0u, hp.width);
     __syncwarp();
+  }
+  if (hist) {
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < hp.passes * 512; i += kScanBlock)
+      if (shist[i]) atomicAdd(hist + i, shist[i]);
   }
 }
 
@@ -882,10 +895,10 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
     uint32_t* mh = (uint32_t*)g->mhi.ptr;
     const int blocks = grid_for(nt, 256, 148 * 16);
     k_morton_keys<<<blocks, 256, 0, st>>>(tri, nt, lo3, scale, tb, m0, mh);
-    uint64_t* s1 = onesweep_sort(m0, m1, nt, tb, 4, g->sortws.ptr, g->d_err, st);
+    uint64_t* s1 = onesweep_sort(m0, m1, nt, tb, sort_plan(30), g->sortws.ptr, g->d_err, st);
     uint64_t* o1 = s1 == m0 ? m1 : m0;
     k_morton_second<<<blocks, 256, 0, st>>>(s1, mh, nt, tb, o1);
-    uint64_t* s2 = onesweep_sort(o1, s1, nt, tb, 4, g->sortws.ptr, g->d_err, st);
+    uint64_t* s2 = onesweep_sort(o1, s1, nt, tb, sort_plan(30), g->sortws.ptr, g->d_err, st);
     k_permute_tris<<<blocks, 256, 0, st>>>(s2, tri, nt, tb, (float4*)g->perm_tri.ptr);
     tri = TriArr{(const float4*)g->perm_tri.ptr};
   }
@@ -908,10 +921,12 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   if ((rc = ensure_buf(g, g->sortws, sort_workspace_bytes(P), st))) return rc;
   uint64_t* k0 = (uint64_t*)g->keys[0].ptr;
   uint64_t* k1 = (uint64_t*)g->keys[1].ptr;
+  const SortPlan top_plan = sort_plan(key_bits_for(C ? C - 1 : 0));
+  sort_prepare(g->sortws.ptr, st);
   if (nt)
-    k_emit_units<<<emit_blocks(nt), kScanBlock, 0, st>>>(TopMaker{tri, g->geom}, nt, offs, k0, P, g->d_err);
-  uint64_t* sortedTop =
-      onesweep_sort(k0, k1, P, 32, sort_passes_for(C ? C - 1 : 0), g->sortws.ptr, g->d_err, st);
+    k_emit_units<<<emit_blocks(nt), kScanBlock, 0, st>>>(TopMaker{tri, g->geom}, nt, offs, k0, P, g->d_err,
+                                                        sort_hist_counts(g->sortws.ptr), top_plan);
+  uint64_t* sortedTop = onesweep_sort(k0, k1, P, 32, top_plan, g->sortws.ptr, g->d_err, st, true);
   const int topBuf = sortedTop == k0 ? 0 : 1;
 
   g->num_cells = C;
@@ -973,11 +988,13 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   if ((rc = ensure_buf(g, g->sortws, sort_workspace_bytes(R), st))) return rc;
   uint64_t* lk0 = (uint64_t*)g->keys[bA].ptr;
   uint64_t* lk1 = (uint64_t*)g->keys[bB].ptr;
+  const SortPlan leaf_plan = sort_plan(key_bits_for(Lc ? Lc - 1 : 0));
+  sort_prepare(g->sortws.ptr, st);
   if (P)
     k_emit_units<<<emit_blocks(P), kScanBlock, 0, st>>>(LeafMaker{tri, sortedTop, g->cells, g->geom}, P,
-                                                       pairOffs, lk0, R, g->d_err);
-  uint64_t* sortedLeaf = onesweep_sort(lk0, lk1, R, 32, sort_passes_for(Lc ? Lc - 1 : 0),
-                                       g->sortws.ptr, g->d_err, st);
+                                                       pairOffs, lk0, R, g->d_err,
+                                                       sort_hist_counts(g->sortws.ptr), leaf_plan);
+  uint64_t* sortedLeaf = onesweep_sort(lk0, lk1, R, 32, leaf_plan, g->sortws.ptr, g->d_err, st, true);
   if ((rc = ensure(g, (void**)&g->leaves, &g->cap_leaves, (size_t)std::max<uint32_t>(Lc, 1) * 8, st))) return rc;
   if ((rc = ensure(g, (void**)&g->indices, &g->cap_refs, (size_t)std::max<uint32_t>(R, 1) * 4, st))) return rc;
   if ((rc = ensure(g, (void**)&g->rtri, &g->cap_rtri, (size_t)std::max<uint32_t>(R, 1) * 48, st))) return rc;
@@ -1043,11 +1060,11 @@ void launch_batch_count(const float4* tri, uint32_t T, const uint32_t* tri_off, 
 
 void launch_batch_emit(const float4* tri, uint32_t T, const uint32_t* tri_off, const BatchScene* scenes,
                        uint32_t ns, const uint32_t* offs, uint64_t* keys, uint32_t capacity,
-                       uint32_t* err, cudaStream_t st) {
+                       uint32_t* err, uint32_t* hist, SortPlan hplan, cudaStream_t st) {
   const TriArr ts{tri};
   if (T)
     k_emit_units<<<emit_blocks(T), kScanBlock, 0, st>>>(BatchMaker{ts, tri_off, scenes, ns}, T, offs, keys,
-                                                       capacity, err);
+                                                       capacity, err, hist, hplan);
 }
 
 void launch_ranges(const uint64_t* keys, uint32_t n, uint2* ranges, uint32_t* indices,

@@ -117,11 +117,20 @@ shn_status set_error(shn_ctx* ctx, shn_status s, const std::string& msg);
 shn_status cuda_status(shn_ctx* ctx, cudaError_t e, const char* where);
 
 // sort.cu
+// Digit plan of a stable LSD sort: `passes` passes of `width`-bit digits (8 or 9).
+struct SortPlan {
+  uint32_t passes, width, bits;  // the last pass takes only the bits left of `bits`
+};
+SortPlan sort_plan(uint32_t bits);          // fewest passes for `bits` key bits (<= 32)
+uint32_t key_bits_for(uint64_t max_key_value);
 size_t sort_workspace_bytes(uint32_t n);
 uint32_t sort_tiles(uint32_t n);
-uint64_t* onesweep_sort(uint64_t* buf0, uint64_t* buf1, uint32_t n, uint32_t lo_bit,
-                        uint32_t passes, void* ws, uint32_t* d_err, cudaStream_t st);
-uint32_t sort_passes_for(uint64_t max_key_value);
+uint64_t* onesweep_sort(uint64_t* buf0, uint64_t* buf1, uint32_t n, uint32_t lo_bit, SortPlan plan,
+                        void* ws, uint32_t* d_err, cudaStream_t st, bool counts_ready = false);
+// digit counts [pass][512] in the sort workspace, for producers that count
+// the digits of the keys they write (sort_prepare zeroes them first)
+uint32_t* sort_hist_counts(void* ws);
+void sort_prepare(void* ws, cudaStream_t st);
 
 // build.cu
 Geom make_geom(const float b[6], const int res[3]);
@@ -148,7 +157,7 @@ void launch_batch_count(const float4* tri, uint32_t T, const uint32_t* tri_off, 
                         uint32_t ns, void* scan_ws, uint32_t* err, uint32_t* offs, cudaStream_t st);
 void launch_batch_emit(const float4* tri, uint32_t T, const uint32_t* tri_off, const BatchScene* scenes,
                        uint32_t ns, const uint32_t* offs, uint64_t* keys, uint32_t capacity,
-                       uint32_t* err, cudaStream_t st);
+                       uint32_t* err, uint32_t* hist, SortPlan hplan, cudaStream_t st);
 void launch_ranges(const uint64_t* keys, uint32_t n, uint2* ranges, uint32_t* indices,
                    const float4* tri, uint32_t T, float4* rtri, cudaStream_t st);
 

@@ -8,19 +8,29 @@
 // box spans two or more cells on every axis a candidate is kept only if the
 // plane-distance test passes at the cell centre.
 //
+// Cell centres.  As in the reference, the centres along each axis are
+// accumulated from the first candidate cell: c(lo - 1) = ((lo*s + o) + s/2) - s,
+// then c(i + 1) = c(i) + s, in FP32 (FastBuildKernels.h:144-164,
+// TwoLevelBuildKernels.h:396-420).  Each axis restarts its sequence for every
+// row of the enclosing loops, so the centre of index i along an axis depends
+// on i and lo only.
+//
 // Row intervals.  Fix the two indices of a row and let i run along the third
-// axis r.  The centre (i*s + o) + s/2 is non-decreasing in i (every IEEE
-// operation is monotone), so the plane distance
+// axis r.  Adding a positive s to a float never decreases it, so the centre is
+// non-decreasing in i, and the plane distance
 //   d = ((c0 - a0)*n0 + (c1 - a1)*n1) + (c2 - a2)*n2
-// is monotone in i (direction = sign of n_r), and the test
+// is monotone in i (direction = sign of n_r; every IEEE operation is
+// monotone), and the test
 //   |n_k * d| <= s_k/2 + eps  for k = 0, 1, 2
 // holds on an interval of d values that contains 0.  The cells of the row
 // that pass are therefore one interval of i, and every cell before it fails
 // on one side of the plane and every cell after it on the other.  The row's
-// interval is found with a real-arithmetic estimate followed by an exact
-// search that evaluates the IEEE expression above at a handful of cells, so
-// the result is bit-identical to testing every candidate (the oracle does the
-// latter).
+// interval is found by walking the accumulated centres from lo: a
+// real-arithmetic estimate says how far the walk may go by additions alone
+// (one test confirms that the cell before the estimate still fails on the
+// near side; if not, the walk restarts from lo and tests every cell), then
+// cells are tested until the first one on the far side.  The result is
+// bit-identical to testing every candidate (the oracle does the latter).
 //
 // Work is balanced across the 32 lanes of a warp: the rows of 32 units are
 // flattened and processed 32 at a time, and the emitted pairs of 32 rows are
@@ -38,7 +48,7 @@ struct Unit {
   float a[3];          // triangle vertex 0
   float n[3];          // unit normal (plane units)
   float s[3];          // lattice cell size
-  float o[3];          // lattice origin: centre_k(i) = (i*s_k + o_k) + s_k*0.5
+  float o[3];          // lattice origin: centres start at ((lo_k*s_k + o_k) + s_k*0.5) - s_k
   uint32_t lo[3];      // first candidate index per axis
   uint32_t span[3];    // number of candidate indices per axis (0 = none)
   uint32_t meta;       // bits 0-1: row axis r; bit 2: plane test applies
@@ -84,12 +94,16 @@ SHN_HD uint32_t unit_rows(const Unit& U) {
 
 SHN_HD uint32_t unit_cells(const Unit& U) { return U.span[0] * U.span[1] * U.span[2]; }
 
-// (c_k(i) - a_k) * n_k
-SHN_HD float unit_term(const Unit& U, int k, uint32_t i) {
+// Accumulated centre of index i >= lo_k along axis k (see the header).
+SHN_HD float acc_centre(const Unit& U, int k, uint32_t i) {
   const float s = U.s[k];
-  const float c = ((float)i * s + U.o[k]) + s * 0.5f;
-  return (c - U.a[k]) * U.n[k];
+  float c = (((float)U.lo[k] * s + U.o[k]) + s * 0.5f) - s;
+  for (uint32_t q = U.lo[k]; q <= i; ++q) c += s;
+  return c;
 }
+
+// (c_k(i) - a_k) * n_k
+SHN_HD float unit_term(const Unit& U, int k, uint32_t i) { return (acc_centre(U, k, i) - U.a[k]) * U.n[k]; }
 
 SHN_HD float combine(int r, float tr, float tu, float tv) {
   if (r == 0) return (tr + tu) + tv;
@@ -97,9 +111,10 @@ SHN_HD float combine(int r, float tr, float tu, float tv) {
   return (tu + tv) + tr;
 }
 
-// 0 = the cell passes, -1 = fails with d < 0 (or NaN), +1 = fails with d > 0.
-SHN_HD int unit_class(const Unit& U, int r, uint32_t i, float tu, float tv) {
-  const float d = combine(r, unit_term(U, r, i), tu, tv);
+// Class of the cell whose centre along the row axis is c:
+// 0 = passes, -1 = fails with d < 0 (or NaN), +1 = fails with d > 0.
+SHN_HD int class_at(const Unit& U, int r, float c, float tu, float tv) {
+  const float d = combine(r, (c - U.a[r]) * U.n[r], tu, tv);
   const bool pass = fabsf(U.n[0] * d) <= U.s[0] * 0.5f + kEps &&
                     fabsf(U.n[1] * d) <= U.s[1] * 0.5f + kEps &&
                     fabsf(U.n[2] * d) <= U.s[2] * 0.5f + kEps;
@@ -121,30 +136,62 @@ SHN_HD void row_interval(const Unit& U, uint32_t j, uint32_t& f, uint32_t& e) {
   const uint32_t iu = U.lo[u] + j % su, iv = U.lo[v] + j / su;
   const float tu = unit_term(U, u, iu), tv = unit_term(U, v, iv);
   const uint32_t lo = U.lo[r], hi1 = U.lo[r] + U.span[r];  // [lo, hi1)
+  const float s = U.s[r];
+  const float c0 = ((((float)lo * s + U.o[r]) + s * 0.5f) - s) + s;  // centre of lo
   const float nr = U.n[r];
   if (!(nr > 0.f) && !(nr < 0.f)) {  // the class is the same along the whole row
-    if (unit_class(U, r, lo, tu, tv) == 0) { f = lo; e = hi1; }
+    if (class_at(U, r, c0, tu, tv) == 0) { f = lo; e = hi1; }
     else { f = lo; e = lo; }
     return;
   }
   const int before = nr > 0.f ? -1 : 1;
+  const int after = -before;
   // real-arithmetic estimate of the interval: |d| <= R
   const float S = tu + tv;
-  const float ca = (U.a[r] - U.o[r]) - U.s[r] * 0.5f;
+  const float ca = (U.a[r] - U.o[r]) - s * 0.5f;
   const float x1 = ((-U.R - S) * U.inv_nr + ca) * U.inv_sr;
   const float x2 = ((U.R - S) * U.inv_nr + ca) * U.inv_sr;
-  uint32_t x = clamp_index(ceilf(fminf(x1, x2)), lo, hi1);
-  // exact: first index whose class is not `before`
-  while (x > lo && unit_class(U, r, x - 1, tu, tv) != before) --x;
-  while (x < hi1 && unit_class(U, r, x, tu, tv) == before) ++x;
+  const uint32_t xs = clamp_index(ceilf(fminf(x1, x2)) - 1.0f, lo, hi1);  // walk without tests up to here
+  // f: first index whose class is not `before`
+  uint32_t x = lo;
+  float c = c0;
+  if (xs > lo + 1) {
+    while (x + 1 < xs) {  // centre of xs - 1
+      c += s;
+      ++x;
+    }
+    if (class_at(U, r, c, tu, tv) != before) {  // the estimate overshot: test every cell from lo
+      x = lo;
+      c = c0;
+    } else {
+      c += s;
+      ++x;
+    }
+  }
+  while (x < hi1 && class_at(U, r, c, tu, tv) == before) {
+    c += s;
+    ++x;
+  }
   f = x;
   if (x == hi1) { e = x; return; }
-  const int after = -before;
-  uint32_t y = clamp_index(floorf(fmaxf(x1, x2)) + 1.0f, x, hi1);
-  // exact: first index >= f whose class is `after`
-  while (y > x && unit_class(U, r, y - 1, tu, tv) == after) --y;
-  while (y < hi1 && unit_class(U, r, y, tu, tv) != after) ++y;
-  e = y;
+  // e: first index >= f whose class is `after`; cells between pass
+  const float cf = c;
+  const uint32_t ys = clamp_index(floorf(fmaxf(x1, x2)), x, hi1);
+  if (ys > x + 1) {
+    while (x + 1 < ys) {  // centre of ys - 1
+      c += s;
+      ++x;
+    }
+    if (class_at(U, r, c, tu, tv) == after) {  // overshot: test every cell from f
+      x = f;
+      c = cf;
+    }
+  }
+  while (x < hi1 && class_at(U, r, c, tu, tv) != after) {
+    c += s;
+    ++x;
+  }
+  e = x;
 }
 
 // Largest lane l with v_l <= q (v non-decreasing across lanes, v_0 <= q).
@@ -208,9 +255,12 @@ SHN_D uint32_t warp_count_units(Unit* su, uint32_t* acc, bool valid) {
 
 // Writes the keys (cell << 32 | id) of the 32 lanes' units (slots filled as
 // for warp_count_units), unit after unit and row after row, to keys[out ...].
-// Stores beyond `cap` are dropped and flagged with kErrCapacity.
+// Stores beyond `cap` are dropped and flagged with kErrCapacity.  When shist
+// is non-null, the hwidth-bit digits (cell >> hwidth*p) of every key, p <
+// hpasses, are counted into shist[p * 512 + digit] (shared memory).
 SHN_D void warp_emit_units(Unit* su, bool valid, uint32_t out, uint64_t* __restrict__ keys, uint32_t cap,
-                           uint32_t* err) {
+                           uint32_t* err, uint32_t* shist = nullptr, uint32_t hpasses = 0,
+                           uint32_t hwidth = 8) {
   const int lane = threadIdx.x & 31;
   const uint32_t rows = valid ? unit_rows(su[lane]) : 0u;
   const uint32_t incl = warp_incl_sum(rows);
@@ -260,6 +310,10 @@ SHN_D void warp_emit_units(Unit* su, bool valid, uint32_t out, uint64_t* __restr
         const uint32_t cell = sc + (q - sp) * ss;
         if (o < cap) __stcs(keys + o, ((uint64_t)cell << 32) | sid);
         else atomicOr(err, kErrCapacity);
+        // the cells are below 2^bits of the sort plan: the last pass's digit
+        // needs no narrower mask
+        const uint32_t hmask = (1u << hwidth) - 1u;
+        for (uint32_t p = 0; p < hpasses; ++p) atomicAdd(shist + p * 512 + ((cell >> (hwidth * p)) & hmask), 1u);
       }
     }
     out += L;

@@ -1,13 +1,23 @@
-// Onesweep LSD radix sort of 64-bit keys on an 8-bit digit per pass
-// (Adinets and Merrill, "Onesweep: A Faster Least Significant Digit Radix
-// Sort for GPUs", 2022), written for sm_100a:
-//  * one histogram kernel computes the digit counts of every pass in a
-//    single read of the keys;
-//  * each pass is ONE kernel: a 4096-key tile is staged into shared memory
-//    with a bulk asynchronous copy (cp.async.bulk + mbarrier), ranked with
-//    warp match/popc (stable), its per-digit counts are combined across
-//    tiles with decoupled look-back, the tile is reordered in shared memory
-//    and written out with coalesced stores.
+// Onesweep LSD radix sort of 64-bit keys (Adinets and Merrill, "Onesweep: A
+// Faster Least Significant Digit Radix Sort for GPUs", 2022), written for
+// sm_100a:
+//  * digits are 8 or 9 bits wide, whichever sorts the key bits in fewer
+//    passes (27 cell bits: three 9-bit passes instead of four 8-bit ones);
+//  * the digit counts of every pass come from one histogram kernel over the
+//    keys, or from the producer of the keys while it writes them (the grid
+//    build's key emission does this; see sort_hist_counts);
+//  * each pass is ONE kernel over 8192-key tiles: a tile is staged into
+//    shared memory with a bulk asynchronous copy (cp.async.bulk +
+//    mbarrier), each warp's digit counts are taken with order-free shared
+//    atomics, the tile's counts are published at once and combined across
+//    tiles with decoupled look-back, then every key is ranked stably (a
+//    ballot-built warp match in input order) straight into its digit-ordered
+//    place in shared memory, and the tile is written out with coalesced
+//    stores.  Publishing before ranking lets the look-back of later tiles
+//    find this tile's counts early.  Ordinary stores: a digit's run of a
+//    tile ends in a sector that the next tile's run of the same digit
+//    completes, and the two merge in L2 instead of reaching DRAM as partial
+//    writes.
 // Replaces the reference's 2-bit split radix sort with three launches per
 // pass (src/Utils/Sort.cu:28-56, src/Utils/chag/pp/detail/sort.cu.inl:436-597).
 // Stability makes the result identical to a stable sort on the digit bits,
@@ -18,10 +28,12 @@ namespace shn {
 
 namespace {
 
-constexpr int kSortBlock = 256;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortBlock * kSortItems;  // 4096 keys, 32 KB
+constexpr int kSortBlock = 512;
 constexpr int kSortWarps = kSortBlock / 32;
+constexpr int kPassItems = 16;            // keys per thread: 8192-key tiles, two per SM
+constexpr int kMinTile = kSortBlock * 8;  // sizes the look-back status array
+constexpr int kMaxBins = 512;             // 9-bit digits
+constexpr int kHistBlock = 256;
 constexpr uint32_t kDigFlagAgg = 1u << 30;
 constexpr uint32_t kDigFlagPrefix = 2u << 30;
 // A tile that gave up (its staged keys never arrived, or its own look-back
@@ -31,40 +43,55 @@ constexpr uint32_t kDigFlagPoison = 3u << 30;
 constexpr uint32_t kDigValueMask = (1u << 30) - 1u;
 constexpr int kLookback = 8;
 
-__global__ void __launch_bounds__(kSortBlock) k_sort_hist(const uint64_t* __restrict__ keys,
+__global__ void __launch_bounds__(kHistBlock) k_sort_hist(const uint64_t* __restrict__ keys,
                                                           uint32_t n, uint32_t lo_bit,
-                                                          uint32_t passes, uint32_t* hist) {
-  __shared__ uint32_t sh[kSortWarps][4][256];
-  const int warp = threadIdx.x >> 5;
-  for (int i = threadIdx.x; i < kSortWarps * 4 * 256; i += kSortBlock) (&sh[0][0][0])[i] = 0u;
+                                                          uint32_t passes, uint32_t width, uint32_t bits,
+                                                          uint32_t* hist) {
+  __shared__ uint32_t sh[4 * kMaxBins];
+  for (int i = threadIdx.x; i < 4 * kMaxBins; i += kHistBlock) sh[i] = 0u;
   __syncthreads();
-  const uint64_t stride = (uint64_t)gridDim.x * kSortBlock;
-  for (uint64_t i = (uint64_t)blockIdx.x * kSortBlock + threadIdx.x; i < n; i += stride) {
+  const uint64_t stride = (uint64_t)gridDim.x * kHistBlock;
+  for (uint64_t i = (uint64_t)blockIdx.x * kHistBlock + threadIdx.x; i < n; i += stride) {
     const uint64_t k = keys[i];
     for (uint32_t p = 0; p < passes; ++p) {
-      const uint32_t d = (uint32_t)(k >> (lo_bit + 8u * p)) & 255u;
-      atomicAdd(&sh[warp][p][d], 1u);
+      const uint32_t w = min(width, bits - width * p);
+      const uint32_t d = (uint32_t)(k >> (lo_bit + width * p)) & ((1u << w) - 1u);
+      atomicAdd(&sh[p * kMaxBins + d], 1u);
     }
   }
   __syncthreads();
-  for (uint32_t p = 0; p < passes; ++p) {
-    uint32_t s = 0;
-    for (int w = 0; w < kSortWarps; ++w) s += sh[w][p][threadIdx.x];
-    if (s) atomicAdd(&hist[p * 256 + threadIdx.x], s);
-  }
+  for (uint32_t i = threadIdx.x; i < passes * kMaxBins; i += kHistBlock)
+    if (sh[i]) atomicAdd(&hist[i], sh[i]);
 }
 
-// Exclusive scan of each pass's 256 digit counts (one block per pass).
-__global__ void __launch_bounds__(256) k_sort_hist_scan(uint32_t* hist) {
-  __shared__ ScanSmem<256> sm;
-  uint32_t* h = hist + blockIdx.x * 256;
+// Exclusive scan of each pass's digit counts (one block per pass).
+__global__ void __launch_bounds__(kMaxBins) k_sort_hist_scan(uint32_t* hist) {
+  __shared__ ScanSmem<kMaxBins> sm;
+  uint32_t* h = hist + blockIdx.x * kMaxBins;
   const uint32_t v = h[threadIdx.x];
   uint32_t tot;
-  const uint32_t ex = block_excl_scan<256>(v, sm, &tot);
+  const uint32_t ex = block_excl_scan<kMaxBins>(v, sm, &tot);
   h[threadIdx.x] = ex;
 }
 
 SHN_D uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Lanes of the warp holding the same BITS-bit digit as this lane (and the
+// same validity), from BITS + 1 ballots: an ALU-only stand-in for
+// __match_any_sync, whose cost grows with the number of distinct values in
+// the warp (about 30 for random 8-bit digits).
+template <int BITS>
+SHN_D uint32_t match_digit(uint32_t d, bool valid) {
+  uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
+  if (!valid) peers = ~peers;
+#pragma unroll
+  for (int b = 0; b < BITS; ++b) {
+    const bool bit = (d >> b) & 1u;
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
+    peers &= bit ? m : ~m;
+  }
+  return peers;
+}
 
 SHN_D uint32_t mbar_try_wait(uint32_t bar) {
   uint32_t done;
@@ -76,22 +103,43 @@ SHN_D uint32_t mbar_try_wait(uint32_t bar) {
   return done;
 }
 
-__global__ void __launch_bounds__(kSortBlock, 3) k_onesweep(const uint64_t* __restrict__ in,
-                                                         uint64_t* __restrict__ out, uint32_t n,
-                                                         uint32_t shift,
-                                                         const uint32_t* __restrict__ digit_base,
-                                                         uint32_t* status, uint32_t* ticket,
-                                                         uint32_t* err, int use_bulk) {
-  __shared__ alignas(128) uint64_t s_keys[kSortTile];
-  __shared__ uint32_t s_whist[kSortWarps][256];
-  __shared__ uint32_t s_gbase[256];
+// Per tile: stage the keys, count the digits of every warp's slice (shared
+// atomics, order-free), publish the tile's digit counts at once, look back
+// for the tile's global digit offsets, then rank every key stably
+// (warp match in input order) straight into its digit-ordered place in
+// shared memory and write the tile out.  Publishing before ranking lets the
+// look-back of later tiles find this tile's counts early, so the prefix
+// front does not wait on ranking; status words are published with relaxed
+// stores (flag and value share one word, nothing else is read through them).
+template <int ITEMS, int MINB, int BITS>
+__global__ void __launch_bounds__(kSortBlock, MINB) k_onesweep(const uint64_t* __restrict__ in,
+                                                            uint64_t* __restrict__ out, uint32_t n,
+                                                            uint32_t shift, uint32_t kMask,
+                                                            const uint32_t* __restrict__ digit_base,
+                                                            uint32_t* status, uint32_t* ticket,
+                                                            uint32_t* err, int use_bulk) {
+  // kMask: the pass's digit mask (BITS bits, fewer in the last pass when the
+  // sorted bits are not a multiple of BITS; bits above the range never count)
+  constexpr int kSortTile = kSortBlock * ITEMS;
+  constexpr int kWarpSlice = 32 * ITEMS;  // keys ranked per warp (<= 512: 16-bit counters)
+  constexpr uint32_t kBins = 1u << BITS;
+  constexpr int kPerThread = (int)kBins / kSortBlock > 0 ? (int)kBins / kSortBlock : 1;
+  static_assert(kBins <= kSortBlock, "one digit per thread");
+  extern __shared__ __align__(128) uint64_t s_keys[];  // kSortTile keys (dynamic)
+  // per-warp digit counts, then each warp's running position per digit
+  // (both <= the tile size): two 16-bit counters per word, so that the
+  // counting can use 32-bit shared atomics
+  __shared__ uint32_t s_wcnt[kSortWarps][kBins / 2];
+  __shared__ uint32_t s_gbase[kBins];
   __shared__ ScanSmem<kSortBlock> s_scan;
   __shared__ alignas(8) uint64_t s_mbar;
   __shared__ uint32_t s_tile;
+  uint16_t(*s_w16)[kBins] = reinterpret_cast<uint16_t(*)[kBins]>(s_wcnt);
+  (void)kPerThread;
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
-  for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortBlock) (&s_whist[0][0])[i] = 0u;
+  for (int i = threadIdx.x; i < kSortWarps * (int)kBins / 2; i += kSortBlock) (&s_wcnt[0][0])[i] = 0u;
   __syncthreads();
   const uint32_t tile = s_tile;
   const uint64_t base = (uint64_t)tile * kSortTile;
@@ -124,7 +172,7 @@ __global__ void __launch_bounds__(kSortBlock, 3) k_onesweep(const uint64_t* __re
   __syncthreads();
   // Bounded wait for the staged tile, taken by the whole block: if any
   // thread's wait runs out, every thread leaves together.  The tile then
-  // publishes a poisoned status for all 256 digits, so later tiles stop
+  // publishes a poisoned status for all its digits, so later tiles stop
   // looking back at once instead of spending their own wait budget on it.
   int timed_out = 0;
   {
@@ -139,7 +187,7 @@ __global__ void __launch_bounds__(kSortBlock, 3) k_onesweep(const uint64_t* __re
   }
   if (__syncthreads_or(timed_out)) {
     if (threadIdx.x == 0) atomicOr(err, kErrTmaTimeout);
-    st_release(status + (uint64_t)tile * 256 + threadIdx.x, kDigFlagPoison);
+    if (threadIdx.x < kBins) st_relaxed(status + (uint64_t)tile * kBins + threadIdx.x, kDigFlagPoison);
     // the copy may still be in flight into this block's shared memory: wait
     // for it once more (bounded) before the block exits
     uint32_t spins = 0;
@@ -148,145 +196,198 @@ __global__ void __launch_bounds__(kSortBlock, 3) k_onesweep(const uint64_t* __re
     return;
   }
 
-  // ---- stable rank within each warp's 512-key slice ------------------------
-  uint64_t key[kSortItems];
-  uint32_t rank[kSortItems];
+  // ---- keys into registers; count each warp slice's digits ------------------
+  uint64_t key[ITEMS];
 #pragma unroll
-  for (int k = 0; k < kSortItems; ++k) {
-    const uint32_t idx = warp * (32 * kSortItems) + k * 32 + lane;
-    const bool valid = idx < count;
-    key[k] = valid ? s_keys[idx] : 0ull;
-    const uint32_t d = valid ? ((uint32_t)(key[k] >> shift) & 255u) : 256u;
-    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-    const int leader = __ffs(peers) - 1;
-    uint32_t old = 0;
-    if (lane == leader && d < 256u) old = s_whist[warp][d];
-    old = __shfl_sync(0xFFFFFFFFu, old, leader);
-    rank[k] = old + __popc(peers & ((1u << lane) - 1u));
-    if (lane == leader && d < 256u) s_whist[warp][d] = old + __popc(peers);
-    __syncwarp();
+  for (int k = 0; k < ITEMS; ++k) {
+    const uint32_t idx = warp * kWarpSlice + k * 32 + lane;
+    key[k] = idx < count ? s_keys[idx] : 0ull;
+    if (idx < count) {
+      const uint32_t d = (uint32_t)(key[k] >> shift) & kMask;
+      atomicAdd(&s_wcnt[warp][d >> 1], 1u << (16u * (d & 1u)));
+    }
   }
   __syncthreads();
 
-  // ---- per digit: warp prefixes and tile count; publish the tile count ------
-  const uint32_t dgt = threadIdx.x;  // 256 threads <-> 256 digits
+  // ---- per digit: warp starts, tile count, publish, look back -------------------
+  const uint32_t dgt = threadIdx.x;  // threads 0..kBins-1 <-> digits
+  const bool has_digit = dgt < kBins;
   uint32_t tcount = 0;
+  uint32_t* my = status + (uint64_t)tile * kBins + dgt;
+  if (has_digit) {
 #pragma unroll
-  for (int w = 0; w < kSortWarps; ++w) {
-    const uint32_t c = s_whist[w][dgt];
-    s_whist[w][dgt] = tcount;
-    tcount += c;
+    for (int w = 0; w < kSortWarps; ++w) {
+      const uint32_t c = s_w16[w][dgt];
+      s_w16[w][dgt] = (uint16_t)tcount;
+      tcount += c;
+    }
+    st_relaxed(my, (tile == 0 ? kDigFlagPrefix : kDigFlagAgg) | tcount);
   }
-  uint32_t* my = status + (uint64_t)tile * 256 + dgt;
-  st_release(my, (tile == 0 ? kDigFlagPrefix : kDigFlagAgg) | tcount);
   uint32_t tot;
   const uint32_t bstart = block_excl_scan<kSortBlock>(tcount, s_scan, &tot);
-  // s_whist[w][d] becomes the tile-local start of warp w's digit-d keys
+  uint32_t excl = 0;
+  if (has_digit) {
+    // warp w's digit-d keys go to tile-local positions from here on
 #pragma unroll
-  for (int w = 0; w < kSortWarps; ++w) s_whist[w][dgt] += bstart;
+    for (int w = 0; w < kSortWarps; ++w) s_w16[w][dgt] = (uint16_t)(s_w16[w][dgt] + bstart);
+    if (tile != 0) {
+      // kLookback predecessors per round trip; relaxed loads suffice (see above)
+      bool poisoned = false;
+      int64_t j = (int64_t)tile - 1;
+      bool done = false;
+      while (!done) {
+        uint32_t w[kLookback];
+#pragma unroll
+        for (int q = 0; q < kLookback; ++q)
+          w[q] = (j - q >= 0) ? ld_relaxed(status + (uint64_t)(j - q) * kBins + dgt) : kDigFlagPrefix;
+#pragma unroll
+        for (int q = 0; q < kLookback; ++q) {
+          if (done) break;
+          uint32_t v = w[q];
+          if ((v >> 30) == 0u) {  // not published yet: poll this one
+            const uint32_t* p = status + (uint64_t)(j - q) * kBins + dgt;
+            uint32_t spins = 0;
+            while (((v = ld_relaxed(p)) >> 30) == 0u) {
+              if (++spins > kSpinLimit) {
+                v = kDigFlagPoison;
+                break;
+              }
+              __nanosleep(20);
+            }
+          }
+          if ((v >> 30) == 3u) {  // a predecessor gave up, or this wait ran out
+            atomicOr(err, kErrLookbackTimeout);
+            poisoned = true;
+            done = true;
+            break;
+          }
+          excl += v & kDigValueMask;
+          if ((v >> 30) == 2u) done = true;
+        }
+        j -= kLookback;
+      }
+      st_relaxed(my, poisoned ? kDigFlagPoison : (kDigFlagPrefix | (excl + tcount)));
+    }
+    s_gbase[dgt] = digit_base[dgt] + excl - bstart;  // global index = s_gbase[d] + tile-local index
+  }
   __syncthreads();
 
-  // ---- reorder the tile in shared memory (digit order, stable) -------------
+  // ---- stable rank straight into digit order (input order (warp, k, lane)) --
+  const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
-  for (int k = 0; k < kSortItems; ++k) {
-    const uint32_t idx = warp * (32 * kSortItems) + k * 32 + lane;
-    if (idx < count) {
-      const uint32_t d = (uint32_t)(key[k] >> shift) & 255u;
-      s_keys[s_whist[warp][d] + rank[k]] = key[k];
-    }
+  for (int k = 0; k < ITEMS; ++k) {
+    const uint32_t idx = warp * kWarpSlice + k * 32 + lane;
+    const bool valid = idx < count;
+    const uint32_t d = (uint32_t)(key[k] >> shift) & kMask;
+    const uint32_t peers = match_digit<BITS>(d, valid);
+    const int leader = __ffs(peers) - 1;
+    uint32_t pos0 = 0;
+    if (lane == leader && valid) pos0 = s_w16[warp][d];
+    pos0 = __shfl_sync(0xFFFFFFFFu, pos0, leader);
+    if (lane == leader && valid) s_w16[warp][d] = (uint16_t)(pos0 + __popc(peers));
+    if (valid) s_keys[pos0 + __popc(peers & lt)] = key[k];
+    __syncwarp();
   }
-
-  // ---- look-back across tiles for this digit ----------------------------------
-  uint32_t excl = 0;
-  bool poisoned = false;
-  if (tile != 0) {
-    // kLookback predecessors per round trip: the status word carries flag
-    // and value together, so relaxed loads suffice and all of a round's
-    // loads are in flight at once.
-    int64_t j = (int64_t)tile - 1;
-    bool done = false;
-    while (!done) {
-      uint32_t w[kLookback];
-#pragma unroll
-      for (int q = 0; q < kLookback; ++q)
-        w[q] = (j - q >= 0) ? ld_relaxed(status + (uint64_t)(j - q) * 256 + dgt) : kDigFlagPrefix;
-#pragma unroll
-      for (int q = 0; q < kLookback; ++q) {
-        if (done) break;
-        uint32_t v = w[q];
-        if ((v >> 30) == 0u) {  // not published yet: poll this one
-          const uint32_t* p = status + (uint64_t)(j - q) * 256 + dgt;
-          uint32_t spins = 0;
-          while (((v = ld_relaxed(p)) >> 30) == 0u) {
-            if (++spins > kSpinLimit) {
-              v = kDigFlagPoison;
-              break;
-            }
-            __nanosleep(20);
-          }
-        }
-        if ((v >> 30) == 3u) {  // a predecessor gave up, or this wait ran out
-          atomicOr(err, kErrLookbackTimeout);
-          poisoned = true;
-          done = true;
-          break;
-        }
-        excl += v & kDigValueMask;
-        if ((v >> 30) == 2u) done = true;
-      }
-      j -= kLookback;
-    }
-    st_release(my, poisoned ? kDigFlagPoison : (kDigFlagPrefix | (excl + tcount)));
-  }
-  s_gbase[dgt] = digit_base[dgt] + excl - bstart;  // global index = s_gbase[d] + local index
   __syncthreads();
 
   // ---- coalesced write-out ---------------------------------------------------
   for (uint32_t i = threadIdx.x; i < count; i += kSortBlock) {
     const uint64_t k = s_keys[i];
-    const uint32_t d = (uint32_t)(k >> shift) & 255u;
-    __stcs(out + s_gbase[d] + i, k);
+    const uint32_t d = (uint32_t)(k >> shift) & kMask;
+    out[s_gbase[d] + i] = k;
   }
 }
 
 }  // namespace
 
 size_t sort_workspace_bytes(uint32_t n) {
-  const size_t tiles = ((size_t)n + kSortTile - 1) / kSortTile;
-  return (4 * 256 + 8) * sizeof(uint32_t) + tiles * 256 * sizeof(uint32_t);
+  const size_t tiles = ((size_t)n + kMinTile - 1) / kMinTile;
+  return (4 * kMaxBins + 8) * sizeof(uint32_t) + tiles * kMaxBins * sizeof(uint32_t);
 }
 
-uint32_t sort_tiles(uint32_t n) { return (uint32_t)(((size_t)n + kSortTile - 1) / kSortTile); }
+uint32_t sort_tiles(uint32_t n) { return (uint32_t)(((size_t)n + kMinTile - 1) / kMinTile); }
 
-// Sorts keys held in buf0 on bits [lo_bit, lo_bit + 8*passes); returns the
-// buffer holding the result (buf0 or buf1).  ws: sort_workspace_bytes(n).
-uint64_t* onesweep_sort(uint64_t* buf0, uint64_t* buf1, uint32_t n, uint32_t lo_bit,
-                        uint32_t passes, void* ws, uint32_t* d_err, cudaStream_t st) {
-  if (n <= 1 || passes == 0) return buf0;
+uint32_t* sort_hist_counts(void* ws) { return (uint32_t*)ws; }
+
+void sort_prepare(void* ws, cudaStream_t st) {
+  cudaMemsetAsync(ws, 0, (4 * kMaxBins + 8) * sizeof(uint32_t), st);
+}
+
+uint32_t key_bits_for(uint64_t max_key_value) {
+  uint32_t bits = 0;
+  while (bits < 32 && (max_key_value >> bits) != 0) ++bits;
+  return bits;
+}
+
+SortPlan sort_plan(uint32_t bits) {
+  SortPlan p;
+  p.bits = bits;
+  p.width = 8;
+  p.passes = (bits + 7) / 8;
+  const uint32_t p9 = (bits + 8) / 9;
+  if (p9 < p.passes) {
+    p.width = 9;
+    p.passes = p9;
+  }
+  return p;
+}
+
+namespace {
+
+template <int ITEMS, int MINB, int BITS>
+void launch_pass(const uint64_t* src, uint64_t* dst, uint32_t n, uint32_t shift, uint32_t mask,
+                 const uint32_t* digit_base, uint32_t* status, uint32_t* ticket, uint32_t* err, cudaStream_t st) {
+  constexpr int tile = kSortBlock * ITEMS;
+  constexpr size_t smem = (size_t)tile * sizeof(uint64_t);
+  // the dynamic shared-memory limit is a per-device attribute: set it once per device
+  static std::atomic<uint64_t> done_mask{0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const uint64_t bit = 1ull << (dev & 63);
+  if (!(done_mask.load() & bit)) {
+    cudaFuncSetAttribute(k_onesweep<ITEMS, MINB, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    done_mask.fetch_or(bit);
+  }
+  const uint32_t tiles = (uint32_t)(((size_t)n + tile - 1) / tile);
+  cudaMemsetAsync(status, 0, (size_t)tiles * (1u << BITS) * sizeof(uint32_t), st);
+  const int bulk = (((uintptr_t)src) & 15u) == 0u;
+  k_onesweep<ITEMS, MINB, BITS><<<tiles, kSortBlock, smem, st>>>(src, dst, n, shift, mask, digit_base, status,
+                                                                 ticket, err, bulk);
+}
+
+}  // namespace
+
+// Sorts keys held in buf0 on the plan's digits of bits [lo_bit, ...);
+// returns the buffer holding the result (buf0 or buf1).  ws:
+// sort_workspace_bytes(n).  counts_ready: the caller ran sort_prepare(ws)
+// before producing the keys and its producer added every key's digits to
+// sort_hist_counts(ws) ([pass][512]).
+uint64_t* onesweep_sort(uint64_t* buf0, uint64_t* buf1, uint32_t n, uint32_t lo_bit, SortPlan plan, void* ws,
+                        uint32_t* d_err, cudaStream_t st, bool counts_ready) {
+  if (n <= 1 || plan.passes == 0) return buf0;
   uint32_t* hist = (uint32_t*)ws;
-  uint32_t* tickets = hist + 4 * 256;
+  uint32_t* tickets = hist + 4 * kMaxBins;
   uint32_t* status = tickets + 8;
-  const uint32_t tiles = sort_tiles(n);
-  cudaMemsetAsync(hist, 0, (4 * 256 + 8) * sizeof(uint32_t), st);
-  const int hist_blocks = (int)std::min<uint32_t>(tiles, 4 * 148u);
-  k_sort_hist<<<hist_blocks, kSortBlock, 0, st>>>(buf0, n, lo_bit, passes, hist);
-  k_sort_hist_scan<<<passes, 256, 0, st>>>(hist);
+  if (!counts_ready) {
+    sort_prepare(ws, st);
+    const int hist_blocks = (int)std::min<uint32_t>((n + 4095) / 4096, 4 * 148u);
+    k_sort_hist<<<hist_blocks, kHistBlock, 0, st>>>(buf0, n, lo_bit, plan.passes, plan.width, plan.bits, hist);
+  }
+  k_sort_hist_scan<<<plan.passes, kMaxBins, 0, st>>>(hist);
   uint64_t* src = buf0;
   uint64_t* dst = buf1;
-  for (uint32_t p = 0; p < passes; ++p) {
-    cudaMemsetAsync(status, 0, (size_t)tiles * 256 * sizeof(uint32_t), st);
-    const int bulk = (((uintptr_t)src) & 15u) == 0u;
-    k_onesweep<<<tiles, kSortBlock, 0, st>>>(src, dst, n, lo_bit + 8u * p, hist + p * 256, status,
-                                            tickets + p, d_err, bulk);
+  for (uint32_t p = 0; p < plan.passes; ++p) {
+    const uint32_t shift = lo_bit + plan.width * p;
+    const uint32_t w = std::min(plan.width, plan.bits - plan.width * p);
+    const uint32_t mask = (1u << w) - 1u;
+    if (plan.width == 9)
+      launch_pass<kPassItems, 2, 9>(src, dst, n, shift, mask, hist + p * kMaxBins, status, tickets + p, d_err, st);
+    else
+      launch_pass<kPassItems, 2, 8>(src, dst, n, shift, mask, hist + p * kMaxBins, status, tickets + p, d_err,
+                                    st);
     std::swap(src, dst);
   }
   return src;
-}
-
-uint32_t sort_passes_for(uint64_t max_key_value) {
-  uint32_t bits = 0;
-  while (bits < 32 && (max_key_value >> bits) != 0) ++bits;
-  return (bits + 7) / 8;
 }
 
 }  // namespace shn

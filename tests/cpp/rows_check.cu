@@ -31,6 +31,7 @@ int main(int argc, char** argv) {
       if (l < 0) l = 0;
       u.lo[k] = l; u.span[k] = (uint32_t)(h - l + 1);
       if (u.span[k] < 2) u.span[k] = 2;
+      if (u.span[k] > 64) u.span[k] = 64;
     }
     unit_finish(u, true);
     const uint32_t R = unit_rows(u);
@@ -39,12 +40,17 @@ int main(int argc, char** argv) {
       uint32_t f, e; row_interval(u, j, f, e);
       const uint32_t iu = u.lo[uu] + j % u.span[uu], iv = u.lo[vv] + j / u.span[uu];
       const float tu = unit_term(u, uu, iu), tv = unit_term(u, vv, iv);
-      // brute force in the oracle's form: dot(sub(centre, a), n)
+      // brute force in the oracle's form: centres accumulated from lo per
+      // axis as the reference loops do, dot(sub(centre, a), n)
+      float acc[3][64];
+      for (int k = 0; k < 3; ++k) {
+        float cc = (((float)u.lo[k] * u.s[k] + u.o[k]) + u.s[k] * 0.5f) - u.s[k];
+        for (uint32_t q = 0; q < u.span[k] && q < 64; ++q) { cc += u.s[k]; acc[k][q] = cc; }
+      }
       int first = -1, last = -1, cnt = 0;
       for (uint32_t i = u.lo[r]; i < u.lo[r] + u.span[r]; ++i) {
         uint32_t idx[3]; idx[r] = i; idx[uu] = iu; idx[vv] = iv;
-        V3 cc = mk(((float)idx[0] * u.s[0] + u.o[0]) + u.s[0] * 0.5f, ((float)idx[1] * u.s[1] + u.o[1]) + u.s[1] * 0.5f,
-                   ((float)idx[2] * u.s[2] + u.o[2]) + u.s[2] * 0.5f);
+        V3 cc = mk(acc[0][idx[0] - u.lo[0]], acc[1][idx[1] - u.lo[1]], acc[2][idx[2] - u.lo[2]]);
         const float d = dot(sub(cc, a), n);
         const V3 dist = muls(n, d);
         const bool pass = fabsf(dist.x) <= u.s[0] * 0.5f + kEps && fabsf(dist.y) <= u.s[1] * 0.5f + kEps &&

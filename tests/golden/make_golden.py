@@ -18,6 +18,14 @@ Fixtures
   mt_closest.npz         SimpleIntersector (Moller-Trumbore) brute-force closest hits
   cosine.npz             CosineHemisphereSampler directions
   cellword.npz           TwoLevelGridCell packing
+  ruins.npz              the reference's ruins scene as its own scene-file
+                         readers load it (FWObject::read, CameraManager::read,
+                         LightSourceLoader::loadFromFile on scenes/ruins):
+                         vertices, triangle indices, face materials, the
+                         Phong-normalised diffuse / specular table, camera
+                         and area light
+
+  python tests/golden/make_golden.py --only ruins    (that fixture alone)
 """
 import os
 import sys
@@ -155,5 +163,24 @@ def main():
     print("fixtures written to", HERE)
 
 
+def ruins_fixture():
+    """The ruins scene through the reference's own readers (compiled in place)."""
+    oracle.build()
+    ref = os.environ.get("SHINOBI_REFERENCE", "/root/reference")
+    d = os.path.join(ref, "scenes", "ruins")
+    o = oracle.ref_read_obj(os.path.join(d, "ruins.obj"))
+    cam = oracle.ref_read_camera(os.path.join(d, "camera.cfg"))
+    light = oracle.ref_read_light(os.path.join(d, "light.cfg"))
+    np.savez_compressed(os.path.join(HERE, "ruins.npz"), vertices=o["vertices"],
+                        indices=o["indices"].astype(np.uint32), face_material=o["face_material"].astype(np.uint32),
+                        materials=o["materials"], camera=cam, light=light)
+    print("ruins.npz:", o["vertices"].shape[0], "vertices,", o["indices"].shape[0], "triangles,",
+          o["materials"].shape[0], "materials")
+
+
 if __name__ == "__main__":
-    main()
+    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "ruins":
+        ruins_fixture()
+    else:
+        main()
+        ruins_fixture()

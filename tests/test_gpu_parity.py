@@ -181,18 +181,24 @@ def test_compact(gpu, n):
 
 
 @pytest.mark.parametrize("n,bits", [(1, 8), (4095, 8), (4096, 16), (4097, 19), (1_000_000, 22),
-                                    (3_000_001, 32)])
+                                    (3_000_001, 32), (8191, 9), (8193, 17), (100_000, 18), (2_000_000, 25),
+                                    (700_001, 26), (5_000_000, 27)])
 def test_sort_keys(gpu, n, bits):
+    """Stable sort on bits [32, 32 + bits) (8- or 9-bit digit passes, the
+    last one narrower when bits is not a multiple of the width); the bits
+    above the range are random and must not change the order."""
     import shinobi_b200 as shn
     torch = _torch()
     rng = np.random.default_rng(bits)
-    hi = rng.integers(0, 1 << bits, size=n, dtype=np.uint64)
+    field = rng.integers(0, 1 << bits, size=n, dtype=np.uint64)
+    above = rng.integers(0, 1 << (32 - bits), size=n, dtype=np.uint64) if bits < 32 else np.zeros(n, np.uint64)
     lo = np.arange(n, dtype=np.uint64)
-    keys = (hi << np.uint64(32)) | lo
+    keys = (((above << np.uint64(bits)) | field) << np.uint64(32)) | lo
     t = torch.from_numpy(keys.view(np.int64)).cuda()
     shn.sort_keys(t, 32, 32 + bits)
+    shn.default_context().sync_status()
     got = t.cpu().numpy().view(np.uint64)
-    assert np.array_equal(got, np.sort(keys, kind="stable"))
+    assert np.array_equal(got, keys[np.argsort(field, kind="stable")])
 
 
 @pytest.mark.parametrize("case", [0, 1, 2])
