@@ -69,6 +69,13 @@ class FWObject {
  public:
   struct Face {
     size_t vert1, vert2, vert3;
+    size_t material = 0;
+  };
+  // after Material::setupPhongCoefficients, as FWObject::read leaves them
+  struct Material {
+    std::string name;
+    vec3f diffuseCoeff{0.f, 0.f, 0.f}, specularCoeff{0.f, 0.f, 0.f};
+    float specularExp = 0.f;
   };
   typedef const Face* t_FaceIterator;
 
@@ -76,16 +83,45 @@ class FWObject {
   void allocateFaces(size_t n) { mFaces.resize(n); }
   size_t getNumVertices() const { return mVertices.size(); }
   size_t getNumFaces() const { return mFaces.size(); }
+  size_t getNumMaterials() const { return mMaterials.size(); }
   vec3f getVertex(size_t i) const { return mVertices[i]; }
   vec3f& getVertex(size_t i) { return mVertices[i]; }
   Face getFace(size_t i) const { return mFaces[i]; }
   Face& getFace(size_t i) { return mFaces[i]; }
+  const Material& getMaterial(size_t i) const { return mMaterials[i]; }
   t_FaceIterator facesBegin() const { return mFaces.data(); }
   t_FaceIterator facesEnd() const { return mFaces.data() + mFaces.size(); }
+
+  // FWObject::read (src/Loaders/FWObjectReader.cpp:193-502): Wavefront OBJ
+  // with its MTL libraries, through shn_obj_read.
+  void read(const char* aFileName) {
+    shn_obj* o = nullptr;
+    if (shn_obj_read(aFileName, &o) != SHN_OK) throw Error(SHN_ERR_INVALID, std::string("FWObject::read: ") + aFileName);
+    shn_obj_info inf;
+    shn_obj_get_info(o, &inf);
+    std::vector<float> v(3 * (size_t)inf.num_vertices), d(4 * (size_t)inf.num_materials),
+        sp(4 * (size_t)inf.num_materials);
+    std::vector<uint32_t> f(3 * (size_t)inf.num_faces), fm(inf.num_faces);
+    shn_obj_copy(o, v.data(), f.data(), fm.data(), d.data(), sp.data());
+    mVertices.resize(inf.num_vertices);
+    for (size_t i = 0; i < mVertices.size(); ++i) mVertices[i] = vec3f{v[3 * i], v[3 * i + 1], v[3 * i + 2]};
+    mFaces.resize(inf.num_faces);
+    for (size_t i = 0; i < mFaces.size(); ++i) mFaces[i] = Face{f[3 * i], f[3 * i + 1], f[3 * i + 2], fm[i]};
+    mMaterials.resize(inf.num_materials);
+    for (size_t m = 0; m < mMaterials.size(); ++m) {
+      const char* name = shn_obj_material_name(o, (uint32_t)m);
+      mMaterials[m].name = name ? name : "";
+      mMaterials[m].diffuseCoeff = vec3f{d[4 * m], d[4 * m + 1], d[4 * m + 2]};
+      mMaterials[m].specularCoeff = vec3f{sp[4 * m], sp[4 * m + 1], sp[4 * m + 2]};
+      mMaterials[m].specularExp = sp[4 * m + 3];
+    }
+    shn_obj_destroy(o);
+  }
 
  private:
   std::vector<vec3f> mVertices;
   std::vector<Face> mFaces;
+  std::vector<Material> mMaterials;
 };
 
 // ---- device context ------------------------------------------------------------
@@ -317,6 +353,30 @@ class Camera {
   shn_camera mCam{};
 };
 
+// CameraManager::read (src/Loaders/CameraManager.cpp:94-158): the camera of a
+// camera.cfg file, from the reference's CameraManager defaults.
+class CameraManager {
+ public:
+  void read(const char* aFileName) {
+    shn_camera c{};
+    c.forward[2] = 1.f;
+    c.up[1] = -1.f;
+    c.fov_deg = 66.f;
+    c.res_x = c.res_y = 512u;
+    if (shn_camera_read(aFileName, &c) != SHN_OK) throw Error(SHN_ERR_INVALID, std::string("CameraManager::read: ") + aFileName);
+    mCam = c;
+  }
+  vec3f getPosition() const { return vec3f{mCam.eye[0], mCam.eye[1], mCam.eye[2]}; }
+  vec3f getOrientation() const { return vec3f{mCam.forward[0], mCam.forward[1], mCam.forward[2]}; }
+  vec3f getUp() const { return vec3f{mCam.up[0], mCam.up[1], mCam.up[2]}; }
+  float getFOV() const { return mCam.fov_deg; }
+  uint32_t getResX() const { return mCam.res_x; }
+  uint32_t getResY() const { return mCam.res_y; }
+
+ private:
+  shn_camera mCam{};
+};
+
 // ---- integrators (src/Integrator/DirectIlluminationIntegrator.h:197-362,
 //                   src/Integrator/SimplePathTracer.hpp:65-241) ------------------------
 // Device buffers (cudaMalloc'd by the caller) for one frame.
@@ -330,6 +390,21 @@ struct FrameBuffer {
 struct AreaLightSource {
   vec3f position{-0.05f, 0.2f, -0.05f}, normal{0.f, -1.f, 0.f}, intensity{10.f, 10.f, 10.f},
       edge1{0.1f, 0.f, 0.f}, edge2{0.f, 0.f, 0.1f};
+};
+
+// LightSourceLoader::loadFromFile (src/Loaders/LightSourceLoader.cpp:26-89).
+struct LightSourceLoader {
+  AreaLightSource loadFromFile(const char* aFileName) {
+    shn_area_light l;
+    if (shn_light_read(aFileName, &l) != SHN_OK) throw Error(SHN_ERR_INVALID, std::string("LightSourceLoader: ") + aFileName);
+    AreaLightSource a;
+    a.position = vec3f{l.position[0], l.position[1], l.position[2]};
+    a.normal = vec3f{l.normal[0], l.normal[1], l.normal[2]};
+    a.intensity = vec3f{l.intensity[0], l.intensity[1], l.intensity[2]};
+    a.edge1 = vec3f{l.edge1[0], l.edge1[1], l.edge1[2]};
+    a.edge2 = vec3f{l.edge2[0], l.edge2[1], l.edge2[2]};
+    return a;
+  }
 };
 
 // MaterialContainer (src/Primitive/Material.h:36-46) with the per-face
@@ -363,9 +438,8 @@ class DirectIlluminationIntegrator {
   }
   // shade: oFrameBuffer = this image's radiance (RGB per pixel); oFinalImage
   // (may have null deviceData) = running mean over image ids 0..aImageId.
-  void shade(const GridBase& aGrid, const Camera& aCamera, const shn_hits& aPrimary,
-             const MaterialContainer& aMaterials, FrameBuffer& oFrameBuffer, FrameBuffer& oFinalImage,
-             int aImageId, cudaStream_t aStream = 0) {
+  // the shading parameters of this integrator for one image
+  shn_di_params params(const MaterialContainer& aMaterials, int aImageId) const {
     shn_di_params p;
     shn_di_params_default(&p);
     const vec3f* lv[5] = {&lightSource.position, &lightSource.edge1, &lightSource.edge2, &lightSource.normal,
@@ -385,6 +459,12 @@ class DirectIlluminationIntegrator {
     p.default_diffuse[0] = aMaterials.defaultDiffuse.x;
     p.default_diffuse[1] = aMaterials.defaultDiffuse.y;
     p.default_diffuse[2] = aMaterials.defaultDiffuse.z;
+    return p;
+  }
+  void shade(const GridBase& aGrid, const Camera& aCamera, const shn_hits& aPrimary,
+             const MaterialContainer& aMaterials, FrameBuffer& oFrameBuffer, FrameBuffer& oFinalImage,
+             int aImageId, cudaStream_t aStream = 0) {
+    const shn_di_params p = params(aMaterials, aImageId);
     check(shn_shade_direct(aGrid.handle(), &aCamera.params(), &aPrimary, &p, oFrameBuffer.deviceData,
                            oFinalImage.deviceData, nullptr, aStream),
           "shade", aGrid.context().get());
@@ -444,6 +524,58 @@ class StaticRTEngine {
   Builder mBuilder;
   std::unique_ptr<FaceSoup> mStorage;
   std::unique_ptr<Grid> mGrid;
+};
+
+// ---- dynamic engine (src/Engine/DynamicRTEngine.h:49-158) -----------------------------
+// Two frame slots: renderFrame renders the geometry prepared by the previous
+// call while the keyframe interpolation of the next frame and its rebuild run
+// on the other slot's stream.  The keyframes are device arrays (3 floats per
+// vertex); FaceSoup::uploadVertices's host upload is the caller's copy.
+class DynamicRTEngine {
+ public:
+  DynamicRTEngine() = default;
+  ~DynamicRTEngine() { shn_dynamic_destroy(mEngine); }
+  DynamicRTEngine(const DynamicRTEngine&) = delete;
+  DynamicRTEngine& operator=(const DynamicRTEngine&) = delete;
+
+  void init(const FWObject& aScene, const shn_grid_params& aParams, Context& ctx = Context::instance()) {
+    std::vector<float> v(3 * aScene.getNumVertices());
+    for (size_t i = 0; i < aScene.getNumVertices(); ++i) {
+      const vec3f p = aScene.getVertex(i);
+      v[3 * i] = p.x;
+      v[3 * i + 1] = p.y;
+      v[3 * i + 2] = p.z;
+    }
+    std::vector<uint32_t> idx(3 * aScene.getNumFaces());
+    for (size_t i = 0; i < aScene.getNumFaces(); ++i) {
+      const FWObject::Face f = aScene.getFace(i);
+      idx[3 * i] = (uint32_t)f.vert1;
+      idx[3 * i + 1] = (uint32_t)f.vert2;
+      idx[3 * i + 2] = (uint32_t)f.vert3;
+    }
+    shn_dynamic_destroy(mEngine);
+    mEngine = nullptr;
+    mCtx = &ctx;
+    check(shn_dynamic_create(ctx.get(), v.data(), (uint32_t)aScene.getNumVertices(), idx.data(),
+                             (uint32_t)aScene.getNumFaces(), SHN_MEM_HOST, &aParams, &mEngine),
+          "DynamicRTEngine::init", ctx.get());
+  }
+  // renderFrame: oHits / oFrameBuffer / oFinalImage as for
+  // DirectIlluminationIntegrator::integrate; oRenderTime / oBuildTime in ms.
+  void renderFrame(const float* aKeyFrame1Device, uint32_t aNumVertices1, const float* aKeyFrame2Device,
+                   float aCoeff, DirectIlluminationIntegrator& aIntegrator, const Camera& aCamera,
+                   const MaterialContainer& aMaterials, shn_hits& oHits, FrameBuffer& oFrameBuffer,
+                   FrameBuffer& oFinalImage, int aImageId, float& oRenderTime, float& oBuildTime) {
+    shn_di_params p = aIntegrator.params(aMaterials, aImageId);
+    check(shn_dynamic_render_frame(mEngine, aKeyFrame1Device, aNumVertices1, aKeyFrame2Device, aCoeff,
+                                   &aCamera.params(), &p, &oHits, oFrameBuffer.deviceData, oFinalImage.deviceData,
+                                   &oRenderTime, &oBuildTime, nullptr),
+          "DynamicRTEngine::renderFrame", mCtx ? mCtx->get() : nullptr);
+  }
+
+ private:
+  shn_dynamic* mEngine = nullptr;
+  Context* mCtx = nullptr;
 };
 
 }  // namespace shinobi

@@ -42,6 +42,12 @@
  *  - DirectIlluminationIntegrator::shade occlusion  -> shn_trace_ao (ambient occlusion)
  *    and shn_shade_direct (area light + computeDirectIllumination)
  *      (src/Integrator/DirectIlluminationIntegrator.h:254-315)
+ *  - DynamicRTEngine::init / renderFrame          -> shn_dynamic_create / shn_dynamic_render_frame
+ *      (src/Engine/DynamicRTEngine.h:49-158)
+ *  - FWObject::read, CameraManager::read,
+ *    LightSourceLoader::loadFromFile               -> shn_obj_read, shn_camera_read, shn_light_read
+ *      (src/Loaders/FWObjectReader.cpp:96-502, src/Loaders/CameraManager.cpp:94-158,
+ *       src/Loaders/LightSourceLoader.cpp:26-89)
  *  - SimplePathTracer / render megakernel           -> shn_pt_render
  *      (src/Integrator/SimplePathTracer.hpp:65-241, src/Shinobi.h:152-230)
  *  - InclusiveScan / ExclusiveScan / Sort           -> shn_exclusive_scan_u32 / shn_sort_keys_u64
@@ -174,13 +180,56 @@ typedef struct shn_grid_params {
   float lambda_leaf;        /* two-level: leaf cells per reference in a top cell (reference: 1.2) */
   uint32_t leaf_threshold;  /* two-level: top cells with <= this many references stay one leaf (16) */
   int32_t res[3];           /* if all > 0: use this resolution instead of the lambda rule */
+  uint32_t insertion;       /* SHN_INSERT_PLANE (default) or SHN_INSERT_SAT, for the uniform grid / top level */
 } shn_grid_params;
+
+/* Insertion rules.  PLANE: a candidate cell of a triangle whose box spans two
+ * or more cells on every axis is kept if the triangle's plane passes within
+ * half a cell of its centre (the reference's sort-based builders,
+ * src/Control/Algorithm/FastBuildKernels.h:137-212).  SAT: the plane test and
+ * the nine edge-cross-axis tests of the triangle/box separating-axis test
+ * (the precise insertion of the reference's other builder,
+ * src/Control/Algorithm/BuildKernels.h:117-201): tighter grids, a slower
+ * build.  The leaf level of two-level grids always uses PLANE, as in the
+ * reference. */
+#define SHN_INSERT_PLANE 0u
+#define SHN_INSERT_SAT 1u
 
 /* Reference defaults: uniform lambda=5; two-level lambda=5, divisor 6, min 2,
  * lambda_leaf 1.2, threshold 16 (src/Control/Algorithm/GridBuilder.h:48,
  * src/Control/Algorithm/FastTwoLevelGridBuilder.h:87-102,
  * src/Control/Algorithm/TwoLevelBuildKernels.h:49,73). */
 void shn_grid_params_default(uint32_t kind, shn_grid_params* p);
+
+/* ---- SAH resolution search ------------------------------------------------- */
+typedef struct shn_sah_result {
+  int32_t res[3];       /* resolution of least cost (the first one in z, y, x order) */
+  int32_t res_min[3];   /* the searched window, inclusive */
+  int32_t res_max[3];
+  float cost;           /* its cost */
+  uint64_t refs;        /* its bounding-box cell references */
+  uint64_t num_tested;  /* resolutions in the window */
+} shn_sah_result;
+
+/* SAHGridBuilder::computeResolution (src/Control/Algorithm/SAHGridBuilder.h:117-202):
+ * every resolution from window_lo to window_hi times the lambda estimate of
+ * GridBuilder::computeResolution (reference: lambda 5, window 0.75 .. 1.25),
+ * each bound clamped to [1, 2048], costed as
+ *   0.85 * refs * cellArea / sceneArea + 0.15 * (resX + resY + resZ)
+ * with refs the triangles' bounding-box cell count at that resolution
+ * (countRefs, src/Control/Algorithm/FastBuildKernels.h:31-86), counted
+ * exactly in 64 bits.  counts (optional, host, x fastest then y then z)
+ * receives every tested resolution's refs.  Synchronous on `stream`.
+ * SHN_ERR_INVALID when the window holds more than 2^24 resolutions or
+ * resolutions x triangles exceeds 2e13. */
+shn_status shn_grid_sah_resolution(const shn_scene* scene, float lambda, float window_lo, float window_hi,
+                                   uint64_t* counts, uint64_t counts_capacity, shn_sah_result* out,
+                                   void* stream);
+
+/* The same refs and cost for k <= 32 explicit resolutions res[3*i .. 3*i+2]
+ * (each axis in [1, 2048]); refs or cost may be NULL.  Synchronous. */
+shn_status shn_grid_sah_cost(const shn_scene* scene, const int32_t* res, uint32_t k, uint64_t* refs,
+                             float* cost, void* stream);
 
 typedef struct shn_grid_info {
   uint32_t kind;
@@ -318,6 +367,38 @@ shn_status shn_shade_direct(const shn_grid* g, const shn_camera* cam, const shn_
  * {cell visits, triangle tests} to it (for roofline accounting); NULL turns
  * counting off.  Not part of the reference interface. */
 shn_status shn_grid_set_stats(shn_grid* g, uint64_t* d_counters);
+
+/* ---- dynamic scenes (DynamicRTEngine, src/Engine/DynamicRTEngine.h:49-158) -------
+ * Two frame slots, each a scene with its own grid and stream.  A frame
+ * renders the slot built during the previous frame (primary rays + direct
+ * illumination, shn_trace_primary + shn_shade_direct) on that slot's stream
+ * while, on the other slot's stream, the vertices are interpolated between
+ * two keyframes (shn_scene_interpolate_vertices, FaceSoup::uploadVertices)
+ * and that slot's grid is rebuilt (shn_grid_build), so the rebuild of frame
+ * N+1 overlaps the render of frame N on the GPU.  As in the reference, the
+ * frame a call renders shows the previous call's keyframe geometry (the
+ * first call renders the geometry given to shn_dynamic_create).  Unlike the
+ * reference (one global grid-parameter constant and global textures for
+ * both slots), the two slots share no state. */
+typedef struct shn_dynamic shn_dynamic;
+/* vtx/idx as for shn_scene_create (host or device, mem); builds slot 0.
+ * Synchronises. */
+shn_status shn_dynamic_create(shn_ctx* ctx, const float* vtx_xyz, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                              uint32_t mem, const shn_grid_params* p, shn_dynamic** out);
+/* DynamicRTEngine::renderFrame: renders into hits / d_frame / d_final (as for
+ * shn_shade_direct, with di->image_id) and prepares the next frame from the
+ * device keyframes d_kf1 (3*n1 floats) and d_kf2 (3*nv floats) with coeff
+ * (vertex = kf1 * (1 - coeff) + kf2 * coeff).  Returns when both the render
+ * and the rebuild are done; render_ms, build_ms (device time of each stream)
+ * and frame_ms (first to last, the two overlapping) may be NULL. */
+shn_status shn_dynamic_render_frame(shn_dynamic* e, const float* d_kf1, uint32_t n1, const float* d_kf2,
+                                    float coeff, const shn_camera* cam, const shn_di_params* di,
+                                    shn_hits* hits, float* d_frame, float* d_final, float* render_ms,
+                                    float* build_ms, float* frame_ms);
+/* The grid and scene the next call renders (next = 1) or the last call
+ * rendered (next = 0); owned by the engine. */
+shn_status shn_dynamic_get_grid(const shn_dynamic* e, uint32_t next, shn_grid** grid, shn_scene** scene);
+void shn_dynamic_destroy(shn_dynamic* e);
 
 /* ---- batched multi-scene build and trace ----------------------------------------
  * Many independent scenes, each with its own uniform grid, built by one

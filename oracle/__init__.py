@@ -53,10 +53,20 @@ def lib():
         vp, u32, i32, f32 = C.c_void_p, C.c_uint32, C.c_int, C.c_float
         L.orc_bounds.argtypes = [vp, vp, u32, vp]
         L.orc_resolution.argtypes = [u32, vp, f32, i32, i32, vp]
+        L.orc_sah_window.argtypes = [u32, vp, f32, f32, f32, vp, vp]
+        L.orc_sah_refs.argtypes = [vp, vp, u32, vp, vp]
+        L.orc_sah_refs.restype = C.c_uint64
+        L.orc_sah_cost.argtypes = [vp, vp, C.c_uint64]
+        L.orc_sah_cost.restype = f32
+        L.orc_sah_resolution.argtypes = [vp, vp, u32, vp, f32, f32, f32, vp, vp, vp, vp]
         L.orc_build_uniform.argtypes = [vp, u32, vp, u32, vp, vp]
         L.orc_build_uniform.restype = vp
         L.orc_build_two_level.argtypes = [vp, u32, vp, u32, vp, vp, f32, u32]
         L.orc_build_two_level.restype = vp
+        L.orc_build_uniform_ex.argtypes = [vp, u32, vp, u32, vp, vp, i32]
+        L.orc_build_uniform_ex.restype = vp
+        L.orc_build_two_level_ex.argtypes = [vp, u32, vp, u32, vp, vp, f32, u32, i32]
+        L.orc_build_two_level_ex.restype = vp
         L.orc_grid_free.argtypes = [vp]
         L.orc_set_reference_arithmetic.argtypes = [i32]
         L.orc_leaf_res_reference.argtypes = [vp, f32, u32, vp]
@@ -130,6 +140,37 @@ def resolution(nt: int, b, lam: float, divisor: int = 1, min_res: int = 1) -> np
     return out
 
 
+def sah_window(nt: int, b, lam: float = 5.0, wlo: float = 0.75, whi: float = 1.25):
+    b = _f32(b)
+    lo, hi = np.zeros(3, np.int32), np.zeros(3, np.int32)
+    lib().orc_sah_window(nt, _p(b), lam, wlo, whi, _p(lo), _p(hi))
+    return lo, hi
+
+
+def sah_cost(vtx, idx, b, res):
+    """(refs, cost) of one resolution (SAHGridBuilder.h:164-175)."""
+    vtx, idx, b = _f32(vtx), _u32(idx), _f32(b)
+    r = np.ascontiguousarray(res, np.int32)
+    refs = int(lib().orc_sah_refs(_p(vtx), _p(idx), idx.shape[0], _p(b), _p(r)))
+    return refs, float(np.float32(lib().orc_sah_cost(_p(b), _p(r), refs)))
+
+
+def sah_resolution(vtx, idx, b, lam: float = 5.0, wlo: float = 0.75, whi: float = 1.25):
+    """SAHGridBuilder::computeResolution: dict(res, cost, refs, res_min, res_max, counts[z, y, x])."""
+    vtx, idx, b = _f32(vtx), _u32(idx), _f32(b)
+    lo, hi = sah_window(idx.shape[0], b, lam, wlo, whi)
+    n = hi - lo + 1
+    counts = np.zeros(int(np.prod(n.astype(np.int64))), np.uint64)
+    res = np.zeros(3, np.int32)
+    cost = np.zeros(1, np.float32)
+    refs = np.zeros(1, np.uint64)
+    lib().orc_sah_resolution(_p(vtx), _p(idx), idx.shape[0], _p(b), lam, wlo, whi, _p(res), _p(cost), _p(refs),
+                             _p(counts))
+    return {"res": tuple(int(x) for x in res), "cost": float(cost[0]), "refs": int(refs[0]),
+            "res_min": tuple(int(x) for x in lo), "res_max": tuple(int(x) for x in hi),
+            "counts": counts.reshape(int(n[2]), int(n[1]), int(n[0]))}
+
+
 @dataclass
 class Grid:
     kind: int
@@ -165,18 +206,19 @@ def _wrap(h, kind, res, b) -> Grid:
     return Grid(kind, np.asarray(res, np.int32), np.asarray(b, np.float32), cells, leaves, indices, tp, h)
 
 
-def build_uniform(vtx, idx, b, res) -> Grid:
+def build_uniform(vtx, idx, b, res, insertion: int = 0) -> Grid:
+    """insertion 0: plane test (the GPU sort path); 1: the precise SAT insertion."""
     vtx, idx, b = _f32(vtx), _u32(idx), _f32(b)
     r = np.ascontiguousarray(res, np.int32)
-    h = lib().orc_build_uniform(_p(vtx), vtx.shape[0], _p(idx), idx.shape[0], _p(b), _p(r))
+    h = lib().orc_build_uniform_ex(_p(vtx), vtx.shape[0], _p(idx), idx.shape[0], _p(b), _p(r), insertion)
     return _wrap(h, 0, r, b)
 
 
-def build_two_level(vtx, idx, b, res, lambda_leaf: float, leaf_threshold: int = 16) -> Grid:
+def build_two_level(vtx, idx, b, res, lambda_leaf: float, leaf_threshold: int = 16, insertion: int = 0) -> Grid:
     vtx, idx, b = _f32(vtx), _u32(idx), _f32(b)
     r = np.ascontiguousarray(res, np.int32)
-    h = lib().orc_build_two_level(_p(vtx), vtx.shape[0], _p(idx), idx.shape[0], _p(b), _p(r),
-                                  lambda_leaf, leaf_threshold)
+    h = lib().orc_build_two_level_ex(_p(vtx), vtx.shape[0], _p(idx), idx.shape[0], _p(b), _p(r),
+                                     lambda_leaf, leaf_threshold, insertion)
     return _wrap(h, 1, r, b)
 
 

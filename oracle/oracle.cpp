@@ -158,11 +158,49 @@ inline void cell_range(const Tri& tri, const Geom& g, uint32_t lo[3], uint32_t h
   hi[0] = (uint32_t)maxf.x; hi[1] = (uint32_t)maxf.y; hi[2] = (uint32_t)maxf.z;
 }
 
+// Separating-axis test of one triangle edge against the cell box (the axisTest
+// of src/Control/Algorithm/BuildKernels.h:41-61): the triangle's projection
+// p0/p1 onto the axis against the box's radius rad.
+inline bool sat_axis(float a, float b, float fa, float fb, float v0a, float v0b, float v1a, float v1b, float ha,
+                     float hb) {
+  const float p0 = a * v0a + b * v0b;
+  const float p1 = a * v1a + b * v1b;
+  const float mn = fminf(p0, p1);
+  const float mx = fmaxf(p0, p1);
+  const float rad = fa * ha + fb * hb;
+  return !(mn > rad + kEps || mx + kEps < -rad);
+}
+
+// The nine edge-cross-axis tests of the precise insertion (GridOperator with
+// taPreciseInsertion, src/Control/Algorithm/BuildKernels.h:143-185), in the
+// cell-centred frame: vertices minus the cell centre c, h = half cell size.
+inline bool sat_edges(const Tri& tri, V3 c, V3 h) {
+  const V3 v0 = sub(tri.v[0], c), v1 = sub(tri.v[1], c), v2 = sub(tri.v[2], c);
+  const V3 e[3] = {sub(v1, v0), sub(v2, v1), sub(v0, v2)};
+  bool ok = true;
+  for (int k = 0; k < 3; ++k) {
+    const V3 ed = e[k];
+    const V3 fe = mk(fabsf(ed.x), fabsf(ed.y), fabsf(ed.z));
+    // X axis: X01 for edges 0 and 1, X2 for edge 2
+    if (k < 2) ok = ok && sat_axis(ed.z, -ed.y, fe.z, fe.y, v0.y, v0.z, v2.y, v2.z, h.y, h.z);
+    else ok = ok && sat_axis(ed.z, -ed.y, fe.z, fe.y, v0.y, v0.z, v1.y, v1.z, h.y, h.z);
+    // Y axis: Y02 for edges 0 and 1, Y1 for edge 2
+    if (k < 2) ok = ok && sat_axis(-ed.z, ed.x, fe.z, fe.x, v0.x, v0.z, v2.x, v2.z, h.x, h.z);
+    else ok = ok && sat_axis(-ed.z, ed.x, fe.z, fe.x, v0.x, v0.z, v1.x, v1.z, h.x, h.z);
+    // Z axis: Z12 for edges 0 and 2, Z0 for edge 1
+    if (k == 1) ok = ok && sat_axis(ed.y, -ed.x, fe.y, fe.x, v0.x, v0.y, v1.x, v1.y, h.x, h.y);
+    else ok = ok && sat_axis(ed.y, -ed.x, fe.y, fe.x, v1.x, v1.y, v2.x, v2.y, h.x, h.y);
+  }
+  return ok;
+}
+
 // Visit the cells of one triangle in the reference's emission order (z, y, x)
 // applying the plane-distance test when the bbox spans >= 2 cells on every axis.
-// Restates buildUnsortedGrid, src/Control/Algorithm/FastBuildKernels.h:137-212.
+// Restates buildUnsortedGrid, src/Control/Algorithm/FastBuildKernels.h:137-212;
+// with sat set, the precise insertion of the reference's other builder adds
+// the nine edge tests to the plane test (src/Control/Algorithm/BuildKernels.h:117-201).
 template <class F>
-inline void for_each_cell(const Tri& tri, const Geom& g, F&& emit) {
+inline void for_each_cell(const Tri& tri, const Geom& g, F&& emit, bool sat = false) {
   uint32_t lo[3], hi[3];
   cell_range(tri, g, lo, hi);
   const uint32_t rx = (uint32_t)g.resf.x;
@@ -185,8 +223,8 @@ inline void for_each_cell(const Tri& tri, const Geom& g, F&& emit) {
           const float cx = acc ? ax[x - lo[0]] : lattice_centre(x, g.cs.x, g.gmin.x);
           const float d = dot(sub(mk(cx, cy, cz), tri.v[0]), n);
           const V3 dist = muls(n, d);
-          if (fabsf(dist.x) <= half.x + kEps && fabsf(dist.y) <= half.y + kEps &&
-              fabsf(dist.z) <= half.z + kEps)
+          if ((!sat || sat_edges(tri, mk(cx, cy, cz), half)) && fabsf(dist.x) <= half.x + kEps &&
+              fabsf(dist.y) <= half.y + kEps && fabsf(dist.z) <= half.z + kEps)
             emit(x + y * rx + z * rxy);
         }
       }
@@ -355,8 +393,81 @@ void orc_resolution(uint32_t nt, const float b[6], float lambda, int divisor, in
   }
 }
 
-orc_grid* orc_build_uniform(const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
-                            const float bounds[6], const int res[3]) {
+// ---------------------------------------------------------------------------
+// SAH resolution search, SAHGridBuilder::computeResolution
+// (src/Control/Algorithm/SAHGridBuilder.h:117-202): the window of resolutions
+// from wlo to whi times the lambda estimate (each bound clamped to [1, 2048]),
+// refs = sum over the triangles of their bounding-box cells (countRefs,
+// src/Control/Algorithm/FastBuildKernels.h:31-86, summed exactly in 64 bits),
+// cost = 0.85 refs cellArea / sceneArea + 0.15 (rx + ry + rz); the first
+// least cost in z, y, x order wins.
+static int sah_window_res(float v) {
+  if (!(v == v) || v >= 2048.f) return 2048;
+  return std::min(std::max((int)v, 1), 2048);
+}
+
+void orc_sah_window(uint32_t nt, const float b[6], float lambda, float wlo, float whi, int rmin[3], int rmax[3]) {
+  V3 diag = sub(mk(b[3], b[4], b[5]), mk(b[0], b[1], b[2]));
+  const float volume = diag.x * diag.y * diag.z;
+  const float magic = powf(lambda * (float)nt / volume, 0.3333333f);
+  diag = muls(diag, magic);
+  for (int a = 0; a < 3; ++a) {
+    rmin[a] = sah_window_res(wlo * at(diag, a));
+    rmax[a] = std::max(rmin[a], sah_window_res(whi * at(diag, a)));
+  }
+}
+
+uint64_t orc_sah_refs(const float* vtx, const uint32_t* idx, uint32_t nt, const float b[6], const int res[3]) {
+  const Geom g = make_geom(b, res);
+  uint64_t sum = 0;
+  for (uint32_t t = 0; t < nt; ++t) {
+    uint32_t lo[3], hi[3];
+    cell_range(load_tri(vtx, idx, t), g, lo, hi);
+    uint64_t p = 1;
+    for (int a = 0; a < 3; ++a) p *= hi[a] >= lo[a] ? (uint64_t)(hi[a] - lo[a] + 1) : 0;
+    sum += p;
+  }
+  return sum;
+}
+
+float orc_sah_cost(const float b[6], const int res[3], uint64_t refs) {
+  const V3 bs = sub(mk(b[3], b[4], b[5]), mk(b[0], b[1], b[2]));
+  const float scene_area = 2.f * (bs.x * bs.x + bs.y * bs.y + bs.z * bs.z);
+  const V3 r = mk((float)res[0], (float)res[1], (float)res[2]);
+  const V3 cs = divv(bs, r);
+  const float cell_area = 2.f * (cs.x * cs.x + cs.y * cs.y + cs.z * cs.z);
+  return 0.85f * (float)refs * cell_area / scene_area + 0.15f * (r.x + r.y + r.z);
+}
+
+void orc_sah_resolution(const float* vtx, const uint32_t* idx, uint32_t nt, const float b[6], float lambda,
+                        float wlo, float whi, int res_out[3], float* cost_out, uint64_t* refs_out,
+                        uint64_t* counts) {
+  int rmin[3], rmax[3];
+  orc_sah_window(nt, b, lambda, wlo, whi, rmin, rmax);
+  const int n[3] = {rmax[0] - rmin[0] + 1, rmax[1] - rmin[1] + 1, rmax[2] - rmin[2] + 1};
+  const int64_t N = (int64_t)n[0] * n[1] * n[2];
+  std::vector<uint64_t> refs(N);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t i = 0; i < N; ++i) {
+    const int res[3] = {rmin[0] + (int)(i % n[0]), rmin[1] + (int)((i / n[0]) % n[1]), rmin[2] + (int)(i / ((int64_t)n[0] * n[1]))};
+    refs[i] = orc_sah_refs(vtx, idx, nt, b, res);
+  }
+  float best = FLT_MAX;
+  for (int64_t i = 0; i < N; ++i) {
+    const int res[3] = {rmin[0] + (int)(i % n[0]), rmin[1] + (int)((i / n[0]) % n[1]), rmin[2] + (int)(i / ((int64_t)n[0] * n[1]))};
+    const float c = orc_sah_cost(b, res, refs[i]);
+    if (c < best) {
+      best = c;
+      for (int a = 0; a < 3; ++a) res_out[a] = res[a];
+      *cost_out = c;
+      *refs_out = refs[i];
+    }
+  }
+  if (counts) std::copy(refs.begin(), refs.end(), counts);
+}
+
+orc_grid* orc_build_uniform_ex(const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                               const float bounds[6], const int res[3], int insertion) {
   orc_grid* G = new orc_grid();
   G->kind = 0;
   G->g = make_geom(bounds, res);
@@ -366,7 +477,7 @@ orc_grid* orc_build_uniform(const float* vtx, uint32_t nv, const uint32_t* idx, 
   std::vector<uint64_t> pairs;
   for (uint32_t t = 0; t < nt; ++t) {
     Tri tr = load_tri(vtx, idx, t);
-    for_each_cell(tr, G->g, [&](uint32_t c) { pairs.push_back(((uint64_t)c << 32) | t); });
+    for_each_cell(tr, G->g, [&](uint32_t c) { pairs.push_back(((uint64_t)c << 32) | t); }, insertion == 1);
   }
   std::sort(pairs.begin(), pairs.end());  // == stable sort on the cell key (emission is tri ordered)
   G->cells.assign(2 * C, 0u);
@@ -382,10 +493,17 @@ orc_grid* orc_build_uniform(const float* vtx, uint32_t nv, const uint32_t* idx, 
   return G;
 }
 
-orc_grid* orc_build_two_level(const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
-                              const float bounds[6], const int res[3], float lambda_leaf,
-                              uint32_t leaf_threshold) {
-  orc_grid* G = orc_build_uniform(vtx, nv, idx, nt, bounds, res);
+orc_grid* orc_build_uniform(const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                            const float bounds[6], const int res[3]) {
+  return orc_build_uniform_ex(vtx, nv, idx, nt, bounds, res, 0);
+}
+
+// insertion 1: the precise (SAT) insertion for the top grid; the leaf
+// level keeps the plane test (the reference's two-level kernels have no other)
+orc_grid* orc_build_two_level_ex(const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                                 const float bounds[6], const int res[3], float lambda_leaf,
+                                 uint32_t leaf_threshold, int insertion) {
+  orc_grid* G = orc_build_uniform_ex(vtx, nv, idx, nt, bounds, res, insertion);
   G->kind = 1;
   const Geom& g = G->g;
   const size_t C = (size_t)res[0] * res[1] * res[2];
@@ -428,6 +546,12 @@ orc_grid* orc_build_two_level(const float* vtx, uint32_t nv, const uint32_t* idx
     G->indices[i] = (uint32_t)lp[i];
   }
   return G;
+}
+
+orc_grid* orc_build_two_level(const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                              const float bounds[6], const int res[3], float lambda_leaf,
+                              uint32_t leaf_threshold) {
+  return orc_build_two_level_ex(vtx, nv, idx, nt, bounds, res, lambda_leaf, leaf_threshold, 0);
 }
 
 // Wrap grid arrays built elsewhere (e.g. by the reference's host builder) so

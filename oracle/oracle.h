@@ -15,6 +15,18 @@ orc_grid* orc_build_uniform(const float* vtx, uint32_t nv, const uint32_t* idx, 
 orc_grid* orc_build_two_level(const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
                               const float bounds[6], const int res[3], float lambda_leaf,
                               uint32_t leaf_threshold);
+void orc_sah_window(uint32_t nt, const float bounds[6], float lambda, float wlo, float whi, int rmin[3],
+                    int rmax[3]);
+uint64_t orc_sah_refs(const float* vtx, const uint32_t* idx, uint32_t nt, const float bounds[6], const int res[3]);
+float orc_sah_cost(const float bounds[6], const int res[3], uint64_t refs);
+void orc_sah_resolution(const float* vtx, const uint32_t* idx, uint32_t nt, const float bounds[6], float lambda,
+                        float wlo, float whi, int res_out[3], float* cost_out, uint64_t* refs_out,
+                        uint64_t* counts);
+orc_grid* orc_build_uniform_ex(const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                               const float bounds[6], const int res[3], int insertion);
+orc_grid* orc_build_two_level_ex(const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                                 const float bounds[6], const int res[3], float lambda_leaf,
+                                 uint32_t leaf_threshold, int insertion);
 orc_grid* orc_grid_from_arrays(int kind, const float bounds[6], const int res[3],
                                const uint32_t* cells, const uint32_t* leaves, uint64_t nleaves,
                                const uint32_t* indices, uint64_t nrefs, const float* vtx,

@@ -20,11 +20,11 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _abi
-from ._abi import (SHN_GRID_TWO_LEVEL, SHN_GRID_UNIFORM, SHN_MEM_DEVICE, SHN_MEM_HOST, SHN_MISS,
-                   GridInfo, GridParams)
+from ._abi import (SHN_GRID_TWO_LEVEL, SHN_GRID_UNIFORM, SHN_INSERT_PLANE, SHN_INSERT_SAT, SHN_MEM_DEVICE,
+                   SHN_MEM_HOST, SHN_MISS, GridInfo, GridParams)
 
 __all__ = ["ShinobiError", "Context", "FaceSoup", "Grid", "grid_params", "SHN_MISS",
-           "SHN_GRID_UNIFORM", "SHN_GRID_TWO_LEVEL", "exclusive_scan", "compact", "sort_keys",
+           "SHN_GRID_UNIFORM", "SHN_GRID_TWO_LEVEL", "SHN_INSERT_PLANE", "SHN_INSERT_SAT", "exclusive_scan", "compact", "sort_keys",
            "camera_struct", "default_context", "read_obj", "read_camera", "read_light"]
 
 
@@ -150,6 +150,42 @@ class FaceSoup:
         self.ctx.check(self.ctx.lib.shn_scene_bounds(self.handle, out), "bounds")
         return np.array(out[:], np.float32)
 
+    def sah_resolution(self, lambda_: float = 5.0, window=(0.75, 1.25), counts: bool = False, stream=None):
+        """SAHGridBuilder::computeResolution: the least-cost resolution of the window around the
+        lambda estimate.  Returns a dict (res, res_min, res_max, cost, refs, num_tested[, counts]);
+        counts is indexed [z, y, x] over the window."""
+        r = _abi.SahResult()
+        buf, cap = None, 0
+        if counts:
+            probe = _abi.SahResult()
+            self.ctx.check(self.ctx.lib.shn_grid_sah_resolution(self.handle, lambda_, window[0], window[1], None,
+                                                                 0, C.byref(probe), _stream(stream)),
+                           "shn_grid_sah_resolution")
+            cap = int(probe.num_tested)
+            buf = np.zeros(cap, np.uint64)
+        self.ctx.check(self.ctx.lib.shn_grid_sah_resolution(
+            self.handle, lambda_, window[0], window[1],
+            None if buf is None else buf.ctypes.data_as(C.c_void_p), cap, C.byref(r), _stream(stream)),
+            "shn_grid_sah_resolution")
+        out = {"res": tuple(r.res), "res_min": tuple(r.res_min), "res_max": tuple(r.res_max),
+               "cost": float(r.cost), "refs": int(r.refs), "num_tested": int(r.num_tested)}
+        if buf is not None:
+            n = [out["res_max"][a] - out["res_min"][a] + 1 for a in range(3)]
+            out["counts"] = buf.reshape(n[2], n[1], n[0])
+        return out
+
+    def sah_cost(self, resolutions, stream=None):
+        """(refs, cost) arrays of the SAH cost of each (rx, ry, rz) in `resolutions` (<= 32)."""
+        res = np.ascontiguousarray(np.asarray(resolutions, np.int32).reshape(-1, 3))
+        k = res.shape[0]
+        refs = np.zeros(k, np.uint64)
+        cost = np.zeros(k, np.float32)
+        self.ctx.check(self.ctx.lib.shn_grid_sah_cost(self.handle, res.ctypes.data_as(C.c_void_p), k,
+                                                      refs.ctypes.data_as(C.c_void_p),
+                                                      cost.ctypes.data_as(C.c_void_p), _stream(stream)),
+                       "shn_grid_sah_cost")
+        return refs, cost
+
     def close(self):
         if getattr(self, "handle", None):
             self.ctx.lib.shn_scene_destroy(self.handle)
@@ -163,7 +199,7 @@ class FaceSoup:
 
 
 def grid_params(kind: int = SHN_GRID_UNIFORM, lambda_: float | None = None, top_divisor=None,
-                min_res=None, lambda_leaf=None, leaf_threshold=None, res=None) -> GridParams:
+                min_res=None, lambda_leaf=None, leaf_threshold=None, res=None, insertion=None) -> GridParams:
     p = GridParams()
     _abi.load().shn_grid_params_default(kind, C.byref(p))
     if lambda_ is not None:
@@ -179,6 +215,8 @@ def grid_params(kind: int = SHN_GRID_UNIFORM, lambda_: float | None = None, top_
     if res is not None:
         for k in range(3):
             p.res[k] = int(res[k])
+    if insertion is not None:
+        p.insertion = int(insertion)
     return p
 
 
@@ -371,6 +409,51 @@ class Grid:
     def close(self):
         if getattr(self, "handle", None):
             self.ctx.lib.shn_grid_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DynamicEngine:
+    """Rebuild of the next frame overlapped with the render of the current one
+    (DynamicRTEngine): two frame slots with their own scene, grid and stream."""
+
+    def __init__(self, vertices, indices, params: GridParams, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        h = C.c_void_p()
+        if isinstance(vertices, np.ndarray):
+            v = np.ascontiguousarray(vertices, np.float32)
+            i = np.ascontiguousarray(indices, np.uint32)
+            st = self.ctx.lib.shn_dynamic_create(self.ctx.handle, v.ctypes.data_as(C.c_void_p), v.shape[0],
+                                                 i.ctypes.data_as(C.c_void_p), i.shape[0], SHN_MEM_HOST,
+                                                 C.byref(params), C.byref(h))
+        else:
+            v, i = vertices.contiguous(), indices.contiguous()
+            st = self.ctx.lib.shn_dynamic_create(self.ctx.handle, _ptr(v), v.shape[0], _ptr(i), i.shape[0],
+                                                 SHN_MEM_DEVICE, C.byref(params), C.byref(h))
+        self.ctx.check(st, "shn_dynamic_create")
+        self.handle = h
+
+    def render_frame(self, kf1, kf2, coeff: float, cam, di, hits: HitBuffers, frame, final=None):
+        """Renders the previous call's geometry and prepares kf1*(1-coeff)+kf2*coeff
+        (device tensors (n, 3)); returns (render_ms, build_ms, frame_ms)."""
+        kf1 = kf1.contiguous()
+        kf2 = kf2.contiguous()
+        c = camera_struct(cam)
+        hs = hits.struct()
+        t = [C.c_float(), C.c_float(), C.c_float()]
+        self.ctx.check(self.ctx.lib.shn_dynamic_render_frame(
+            self.handle, _ptr(kf1), kf1.shape[0], _ptr(kf2), float(coeff), C.byref(c), C.byref(di), C.byref(hs),
+            _ptr(frame), _ptr(final), C.byref(t[0]), C.byref(t[1]), C.byref(t[2])), "shn_dynamic_render_frame")
+        return t[0].value, t[1].value, t[2].value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx.lib.shn_dynamic_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

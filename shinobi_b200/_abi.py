@@ -22,6 +22,7 @@ SHN_ERR_BUDGET, SHN_ERR_NOT_BUILT, SHN_ERR_BUSY, SHN_ERR_CANCELLED = 5, 6, 7, 8
 
 SHN_MISS = 0xFFFFFFFF
 SHN_FORCE_CTX_SCAN, SHN_FORCE_GRID_COMPACTION, SHN_FORCE_NOALLOC_SCAN = 1, 2, 3
+SHN_INSERT_PLANE, SHN_INSERT_SAT = 0, 1
 SHN_MEM_HOST = 0
 SHN_MEM_DEVICE = 1
 SHN_GRID_UNIFORM = 0
@@ -30,7 +31,7 @@ SHN_GRID_TWO_LEVEL = 1
 
 class GridParams(C.Structure):
     _fields_ = [("kind", u32), ("lambda_", f32), ("top_divisor", i32), ("min_res", i32),
-                ("lambda_leaf", f32), ("leaf_threshold", u32), ("res", i32 * 3)]
+                ("lambda_leaf", f32), ("leaf_threshold", u32), ("res", i32 * 3), ("insertion", u32)]
 
 
 class GridInfo(C.Structure):
@@ -66,6 +67,11 @@ class AreaLight(C.Structure):
 class ObjInfo(C.Structure):
     _fields_ = [("num_vertices", u32), ("num_faces", u32), ("num_materials", u32), ("num_normals", u32),
                 ("num_texcoords", u32), ("skipped_lines", u64)]
+
+
+class SahResult(C.Structure):
+    _fields_ = [("res", i32 * 3), ("res_min", i32 * 3), ("res_max", i32 * 3), ("cost", f32), ("refs", u64),
+                ("num_tested", u64)]
 
 
 class DiParams(C.Structure):
@@ -117,6 +123,8 @@ SIGNATURES = {
     "shn_grid_params_default": ([u32, C.POINTER(GridParams)], None),
     "shn_grid_create": ([vp, C.POINTER(vp)], i32),
     "shn_grid_build": ([vp, vp, C.POINTER(GridParams), vp], i32),
+    "shn_grid_sah_resolution": ([vp, f32, f32, f32, vp, u64, C.POINTER(SahResult), vp], i32),
+    "shn_grid_sah_cost": ([vp, vp, u32, vp, vp, vp], i32),
     "shn_grid_get_info": ([vp, C.POINTER(GridInfo)], i32),
     "shn_grid_export": ([vp, vp, vp, vp, vp], i32),
     "shn_grid_destroy": ([vp], None),
@@ -158,6 +166,11 @@ SIGNATURES = {
     "shn_grid_sync_status": ([vp, vp], i32),
     "shn_batch_sync_status": ([vp, vp], i32),
     "shn_debug_force_lookback_timeout": ([u32, vp, vp], i32),
+    "shn_dynamic_create": ([vp, vp, u32, vp, u32, u32, C.POINTER(GridParams), C.POINTER(vp)], i32),
+    "shn_dynamic_render_frame": ([vp, vp, u32, vp, f32, C.POINTER(Camera), C.POINTER(DiParams), C.POINTER(Hits),
+                                  vp, vp, vp, vp, vp], i32),
+    "shn_dynamic_get_grid": ([vp, u32, C.POINTER(vp), C.POINTER(vp)], i32),
+    "shn_dynamic_destroy": ([vp], None),
     "shn_obj_read": ([C.c_char_p, C.POINTER(vp)], i32),
     "shn_obj_get_info": ([vp, C.POINTER(ObjInfo)], i32),
     "shn_obj_copy": ([vp, vp, vp, vp, vp, vp], i32),

@@ -266,6 +266,107 @@ __global__ void __launch_bounds__(kScanBlock) k_emit_units(Maker mk, uint32_t n,
   }
 }
 
+// ---- precise (SAT) insertion --------------------------------------------------------
+// The reference's other uniform-grid builder keeps a candidate cell only if
+// the plane test AND the nine edge-cross-axis tests of the triangle/box
+// separating-axis test pass (GridOperator with taPreciseInsertion,
+// src/Control/Algorithm/BuildKernels.h:41-201); cell centres are accumulated
+// as in the plane-test path.  One thread walks one triangle's candidates
+// (this insertion is a build option, not the hot path).
+SHN_D bool sat_axis(float a, float b, float fa, float fb, float v0a, float v0b, float v1a, float v1b, float ha,
+                    float hb) {
+  const float p0 = a * v0a + b * v0b;
+  const float p1 = a * v1a + b * v1b;
+  const float mn = fminf(p0, p1);
+  const float mx = fmaxf(p0, p1);
+  const float rad = fa * ha + fb * hb;
+  return !(mn > rad + kEps || mx + kEps < -rad);
+}
+
+SHN_D bool sat_edges(V3 t0, V3 t1, V3 t2, V3 c, V3 h) {
+  const V3 v0 = sub(t0, c), v1 = sub(t1, c), v2 = sub(t2, c);
+  const V3 e[3] = {sub(v1, v0), sub(v2, v1), sub(v0, v2)};
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const V3 ed = e[k];
+    const V3 fe = mk(fabsf(ed.x), fabsf(ed.y), fabsf(ed.z));
+    ok = ok && (k < 2 ? sat_axis(ed.z, -ed.y, fe.z, fe.y, v0.y, v0.z, v2.y, v2.z, h.y, h.z)
+                      : sat_axis(ed.z, -ed.y, fe.z, fe.y, v0.y, v0.z, v1.y, v1.z, h.y, h.z));
+    ok = ok && (k < 2 ? sat_axis(-ed.z, ed.x, fe.z, fe.x, v0.x, v0.z, v2.x, v2.z, h.x, h.z)
+                      : sat_axis(-ed.z, ed.x, fe.z, fe.x, v0.x, v0.z, v1.x, v1.z, h.x, h.z));
+    ok = ok && (k == 1 ? sat_axis(ed.y, -ed.x, fe.y, fe.x, v0.x, v0.y, v1.x, v1.y, h.x, h.y)
+                       : sat_axis(ed.y, -ed.x, fe.y, fe.x, v1.x, v1.y, v2.x, v2.y, h.x, h.y));
+  }
+  return ok;
+}
+
+// Cells of triangle t in (z, y, x) order; emit(cell) for each kept one.
+template <class F>
+SHN_D void sat_cells(const TriArr& tri, const Geom& g, uint32_t t, F&& emit) {
+  V3 a, b, c;
+  load_tri(tri, t, a, b, c);
+  uint32_t lo[3], hi[3];
+  cell_range(a, b, c, g, lo, hi);
+  const uint32_t rx = (uint32_t)g.resf.x, rxy = (uint32_t)(g.resf.x * g.resf.y);
+  if (!(hi[0] - lo[0] > 0 && hi[1] - lo[1] > 0 && hi[2] - lo[2] > 0)) {
+    for (uint32_t z = lo[2]; z <= hi[2]; ++z)
+      for (uint32_t y = lo[1]; y <= hi[1]; ++y)
+        for (uint32_t x = lo[0]; x <= hi[0]; ++x) emit(x + y * rx + z * rxy);
+    return;
+  }
+  const V3 n = normalize(cross(sub(b, a), sub(c, a)));
+  const V3 h = muls(g.cs, 0.5f);
+  float cz = (((float)lo[2] * g.cs.z + g.gmin.z) + h.z) - g.cs.z;
+  for (uint32_t z = lo[2]; z <= hi[2]; ++z) {
+    cz += g.cs.z;
+    float cy = (((float)lo[1] * g.cs.y + g.gmin.y) + h.y) - g.cs.y;
+    for (uint32_t y = lo[1]; y <= hi[1]; ++y) {
+      cy += g.cs.y;
+      float cx = (((float)lo[0] * g.cs.x + g.gmin.x) + h.x) - g.cs.x;
+      for (uint32_t x = lo[0]; x <= hi[0]; ++x) {
+        cx += g.cs.x;
+        const V3 cc = mk(cx, cy, cz);
+        const float d = dot(sub(cc, a), n);
+        const V3 dist = muls(n, d);
+        if (sat_edges(a, b, c, cc, h) && fabsf(dist.x) <= h.x + kEps && fabsf(dist.y) <= h.y + kEps &&
+            fabsf(dist.z) <= h.z + kEps)
+          emit(x + y * rx + z * rxy);
+      }
+    }
+  }
+}
+
+__global__ void k_count_sat(TriArr tri, uint32_t n, Geom g, uint32_t* __restrict__ counts) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    uint32_t k = 0;
+    sat_cells(tri, g, t, [&](uint32_t) { ++k; });
+    counts[t] = k;
+  }
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_emit_sat(TriArr tri, uint32_t n, Geom g,
+                                                        const uint32_t* __restrict__ offs,
+                                                        uint64_t* __restrict__ keys, uint32_t cap, uint32_t* err,
+                                                        uint32_t* hist, SortPlan hp) {
+  __shared__ uint32_t shist[4 * 512];
+  for (int i = threadIdx.x; i < 4 * 512; i += kScanBlock) shist[i] = 0u;
+  __syncthreads();
+  const uint32_t hmask = (1u << hp.width) - 1u;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    uint32_t o = offs[t];
+    sat_cells(tri, g, t, [&](uint32_t cell) {
+      if (o < cap) keys[o] = ((uint64_t)cell << 32) | t;
+      else atomicOr(err, kErrCapacity);
+      ++o;
+      for (uint32_t p = 0; p < hp.passes; ++p) atomicAdd(shist + p * 512 + ((cell >> (hp.width * p)) & hmask), 1u);
+    });
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < hp.passes * 512; i += kScanBlock)
+    if (shist[i]) atomicAdd(hist + i, shist[i]);
+}
+
 // ---------------------------------------------------------------------------
 __global__ void k_pack_triangles(const float* __restrict__ vtx, const uint32_t* __restrict__ idx,
                                  uint32_t nt, float4* __restrict__ tri) {
@@ -724,6 +825,16 @@ void launch_counts(Maker mk, uint32_t n, uint32_t* offs, void* ws, uint32_t* err
   k_scan_inplace<<<(unsigned)tiles, kScanBlock, 0, st>>>(offs, n, LookbackState{status, ticket, err});
 }
 
+// The counts and offsets of the precise insertion (as launch_counts).
+void launch_counts_sat(TriArr tri, Geom g, uint32_t n, uint32_t* offs, void* ws, uint32_t* err, cudaStream_t st) {
+  const size_t tiles = ((size_t)n + kScanTile - 1) / kScanTile;
+  uint64_t* status = (uint64_t*)ws;
+  cudaMemsetAsync(status, 0, (tiles + 2) * 8, st);
+  uint32_t* ticket = (uint32_t*)(status + tiles + 1);
+  k_count_sat<<<grid_for(n, 128, 148 * 16), 128, 0, st>>>(tri, n, g, offs);
+  k_scan_inplace<<<(unsigned)tiles, kScanBlock, 0, st>>>(offs, n, LookbackState{status, ticket, err});
+}
+
 shn_status ensure(shn_grid* g, void** p, size_t* cap, size_t bytes, cudaStream_t st) {
   if (*cap >= bytes && *p) return SHN_OK;
   if (*p) dev_free(g->ctx, *p, *cap, st);
@@ -852,6 +963,7 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   if (C >= (1ull << 31)) return set_error(ctx, SHN_ERR_INVALID, "grid resolution too large");
   g->kind = p->kind;
   g->geom = make_geom(s->bounds, res);
+  const bool sat = p->insertion == SHN_INSERT_SAT;
   g->built = false;
   g->src_tri = s->ids ? s->ids : s->tri;
   g->src_nt = s->nt;
@@ -909,7 +1021,8 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   uint32_t P = 0;
   if (nt) {
     if ((rc = ensure_buf(g, g->scan, (((size_t)nt + kScanTile - 1) / kScanTile + 2) * 8, st))) return rc;
-    launch_counts(TopMaker{tri, g->geom}, nt, offs, g->scan.ptr, g->d_err, st);
+    if (sat) launch_counts_sat(tri, g->geom, nt, offs, g->scan.ptr, g->d_err, st);
+    else launch_counts(TopMaker{tri, g->geom}, nt, offs, g->scan.ptr, g->d_err, st);
     const uint32_t* src[1] = {offs + nt};
     if ((rc = read_words(g, src, 1, &P, st))) return rc;
   }
@@ -923,7 +1036,10 @@ shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p,
   uint64_t* k1 = (uint64_t*)g->keys[1].ptr;
   const SortPlan top_plan = sort_plan(key_bits_for(C ? C - 1 : 0));
   sort_prepare(g->sortws.ptr, st);
-  if (nt)
+  if (nt && sat)
+    k_emit_sat<<<grid_for(nt, kScanBlock, 148 * 8), kScanBlock, 0, st>>>(tri, nt, g->geom, offs, k0, P, g->d_err,
+                                                                        sort_hist_counts(g->sortws.ptr), top_plan);
+  else if (nt)
     k_emit_units<<<emit_blocks(nt), kScanBlock, 0, st>>>(TopMaker{tri, g->geom}, nt, offs, k0, P, g->d_err,
                                                         sort_hist_counts(g->sortws.ptr), top_plan);
   uint64_t* sortedTop = onesweep_sort(k0, k1, P, 32, top_plan, g->sortws.ptr, g->d_err, st, true);

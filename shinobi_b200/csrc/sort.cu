@@ -6,12 +6,13 @@
 //  * the digit counts of every pass come from one histogram kernel over the
 //    keys, or from the producer of the keys while it writes them (the grid
 //    build's key emission does this; see sort_hist_counts);
-//  * each pass is ONE kernel over 8192-key tiles: a tile is staged into
+//  * each pass is ONE kernel over 6144-key tiles (two per SM): a tile is staged into
 //    shared memory with a bulk asynchronous copy (cp.async.bulk +
 //    mbarrier), each warp's digit counts are taken with order-free shared
 //    atomics, the tile's counts are published at once and combined across
-//    tiles with decoupled look-back, then every key is ranked stably (a
-//    ballot-built warp match in input order) straight into its digit-ordered
+//    tiles with decoupled look-back, then every key is ranked stably (in
+//    input order; the lanes of a warp holding the same digit find each other
+//    through a shared match word per digit) straight into its digit-ordered
 //    place in shared memory, and the tile is written out with coalesced
 //    stores.  Publishing before ranking lets the look-back of later tiles
 //    find this tile's counts early.  Ordinary stores: a digit's run of a
@@ -30,7 +31,7 @@ namespace {
 
 constexpr int kSortBlock = 512;
 constexpr int kSortWarps = kSortBlock / 32;
-constexpr int kPassItems = 16;            // keys per thread: 8192-key tiles, two per SM
+constexpr int kPassItems = 12;            // keys per thread: 6144-key tiles, two per SM
 constexpr int kMinTile = kSortBlock * 8;  // sizes the look-back status array
 constexpr int kMaxBins = 512;             // 9-bit digits
 constexpr int kHistBlock = 256;
@@ -76,23 +77,6 @@ __global__ void __launch_bounds__(kMaxBins) k_sort_hist_scan(uint32_t* hist) {
 
 SHN_D uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Lanes of the warp holding the same BITS-bit digit as this lane (and the
-// same validity), from BITS + 1 ballots: an ALU-only stand-in for
-// __match_any_sync, whose cost grows with the number of distinct values in
-// the warp (about 30 for random 8-bit digits).
-template <int BITS>
-SHN_D uint32_t match_digit(uint32_t d, bool valid) {
-  uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
-  if (!valid) peers = ~peers;
-#pragma unroll
-  for (int b = 0; b < BITS; ++b) {
-    const bool bit = (d >> b) & 1u;
-    const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
-    peers &= bit ? m : ~m;
-  }
-  return peers;
-}
-
 SHN_D uint32_t mbar_try_wait(uint32_t bar) {
   uint32_t done;
   asm volatile(
@@ -125,7 +109,10 @@ __global__ void __launch_bounds__(kSortBlock, MINB) k_onesweep(const uint64_t* _
   constexpr uint32_t kBins = 1u << BITS;
   constexpr int kPerThread = (int)kBins / kSortBlock > 0 ? (int)kBins / kSortBlock : 1;
   static_assert(kBins <= kSortBlock, "one digit per thread");
-  extern __shared__ __align__(128) uint64_t s_keys[];  // kSortTile keys (dynamic)
+  // dynamic: the tile's keys, then per-warp match words (the lane bits of
+  // the keys holding each digit)
+  extern __shared__ __align__(128) uint64_t s_keys[];
+  uint32_t(*s_match)[kBins] = reinterpret_cast<uint32_t(*)[kBins]>(s_keys + kSortTile);
   // per-warp digit counts, then each warp's running position per digit
   // (both <= the tile size): two 16-bit counters per word, so that the
   // counting can use 32-bit shared atomics
@@ -140,6 +127,7 @@ __global__ void __launch_bounds__(kSortBlock, MINB) k_onesweep(const uint64_t* _
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
   for (int i = threadIdx.x; i < kSortWarps * (int)kBins / 2; i += kSortBlock) (&s_wcnt[0][0])[i] = 0u;
+  for (int i = threadIdx.x; i < kSortWarps * (int)kBins; i += kSortBlock) (&s_match[0][0])[i] = 0u;
   __syncthreads();
   const uint32_t tile = s_tile;
   const uint64_t base = (uint64_t)tile * kSortTile;
@@ -273,18 +261,28 @@ __global__ void __launch_bounds__(kSortBlock, MINB) k_onesweep(const uint64_t* _
   __syncthreads();
 
   // ---- stable rank straight into digit order (input order (warp, k, lane)) --
-  const uint32_t lt = (1u << lane) - 1u;
+  // The lanes holding the same digit find each other through the warp's
+  // match word of that digit (shared atomicOr of the lane bits); the lowest
+  // of them advances the warp's running position and clears the word.
+  const uint32_t lbit = 1u << lane, lt = lbit - 1u;
+  uint32_t* wm = s_match[warp];
 #pragma unroll
   for (int k = 0; k < ITEMS; ++k) {
     const uint32_t idx = warp * kWarpSlice + k * 32 + lane;
     const bool valid = idx < count;
     const uint32_t d = (uint32_t)(key[k] >> shift) & kMask;
-    const uint32_t peers = match_digit<BITS>(d, valid);
-    const int leader = __ffs(peers) - 1;
+    if (valid) atomicOr(wm + d, lbit);
+    __syncwarp();
+    const uint32_t peers = valid ? wm[d] : lbit;
+    __syncwarp();
+    const bool leader = valid && (peers & lt) == 0u;
     uint32_t pos0 = 0;
-    if (lane == leader && valid) pos0 = s_w16[warp][d];
-    pos0 = __shfl_sync(0xFFFFFFFFu, pos0, leader);
-    if (lane == leader && valid) s_w16[warp][d] = (uint16_t)(pos0 + __popc(peers));
+    if (leader) {
+      wm[d] = 0u;
+      pos0 = s_w16[warp][d];
+      s_w16[warp][d] = (uint16_t)(pos0 + __popc(peers));
+    }
+    pos0 = __shfl_sync(0xFFFFFFFFu, pos0, __ffs(peers) - 1);
     if (valid) s_keys[pos0 + __popc(peers & lt)] = key[k];
     __syncwarp();
   }
@@ -338,7 +336,7 @@ template <int ITEMS, int MINB, int BITS>
 void launch_pass(const uint64_t* src, uint64_t* dst, uint32_t n, uint32_t shift, uint32_t mask,
                  const uint32_t* digit_base, uint32_t* status, uint32_t* ticket, uint32_t* err, cudaStream_t st) {
   constexpr int tile = kSortBlock * ITEMS;
-  constexpr size_t smem = (size_t)tile * sizeof(uint64_t);
+  constexpr size_t smem = (size_t)tile * sizeof(uint64_t) + (size_t)kSortWarps * (1u << BITS) * sizeof(uint32_t);
   // the dynamic shared-memory limit is a per-device attribute: set it once per device
   static std::atomic<uint64_t> done_mask{0};
   int dev = 0;
