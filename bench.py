@@ -619,7 +619,8 @@ def run_batch(args, emit=True):
     bt.ctx, bt.handle, bt.num_scenes, bt.tri_offsets = ctx, h, ns, to
     t0 = time.perf_counter()
     cands = np.array([0.5, 0.75, 1.0, 1.5, 2.0, 3.0], np.float32)
-    chosen = bt.autotune(cands, expected_rays=rays.astype(np.uint32), sample_rays=16384)
+    chosen, chosen_sah, tune_report = bt.autotune_ex(cands, expected_rays=rays.astype(np.uint32),
+                                                     sample_rays=16384, blocks_per_sm=(0, 4, 6))
     t_tune = time.perf_counter() - t0
     bt.build()
     torch.cuda.synchronize()
@@ -697,6 +698,10 @@ def run_batch(args, emit=True):
         "batched_vs_plain": batched / plain,
         "results_identical_to_plain": same,
         "build_ms": bms, "build_ms_per_mtri": bms / (n_tris / 1e6), "autotune_s": t_tune,
+        "autotune": {"timed_candidates": tune_report["timed_candidates"],
+                     "trace_blocks_per_sm": tune_report["blocks_per_sm"],
+                     "shape_ms": dict(zip(("occupancy", "4", "6"), tune_report["shape_ms"])),
+                     "sah_cost_chosen_median": float(np.median(chosen_sah))},
         "roofline_build": {"bound": "hbm", "achieved": b_build / (bms * 1e-3) / 1e9, "peak": peaks["hbm_gbs"],
                            "unit": "GB/s", "frac": b_build / (bms * 1e-3) / 1e9 / peaks["hbm_gbs"],
                            "traffic": None, "note": f"whole batched build, algorithmic bytes {b_build}; peak {peak_kind}"},

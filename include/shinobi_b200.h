@@ -423,6 +423,31 @@ shn_status shn_batch_set_lambdas(shn_batch* b, const float* lambdas);
 shn_status shn_batch_autotune(shn_batch* b, const float* candidates, uint32_t num_candidates,
                               const uint32_t* expected_rays, uint32_t sample_rays, uint32_t seed,
                               float* chosen, void* stream);
+/* The autotuner with two more terms.
+ *  sah_keep > 0: per scene, every candidate's resolution is costed with the
+ *    SAH cost of shn_grid_sah_cost (SAHGridBuilder.h:164-175) and only the
+ *    sah_keep cheapest are built and timed; 0 times them all.
+ *  blocks_per_sm[0 .. num_block_shapes): resident blocks per SM of the
+ *    batch's persistent closest-hit trace kernel (block of 128 threads) to
+ *    time on the chosen grids with sample_rays rays spread over the scenes
+ *    like expected_rays; the fastest is kept for later traces and captures.
+ *    0 entries: the occupancy limit.
+ * sah_cost (optional, num_scenes) receives the chosen candidate's SAH cost;
+ * report (optional) the work done and the shape timings.  Synchronises. */
+typedef struct shn_autotune_config {
+  uint32_t sah_keep;
+  uint32_t num_block_shapes;  /* <= 8 */
+  uint32_t blocks_per_sm[8];
+} shn_autotune_config;
+typedef struct shn_autotune_report {
+  uint32_t timed_candidates;  /* (scene, lambda) builds timed */
+  uint32_t blocks_per_sm;     /* chosen (0: occupancy limit) */
+  float shape_ms[8];          /* median sample trace time per blocks_per_sm entry */
+} shn_autotune_report;
+shn_status shn_batch_autotune_ex(shn_batch* b, const float* candidates, uint32_t num_candidates,
+                                 const uint32_t* expected_rays, uint32_t sample_rays, uint32_t seed,
+                                 const shn_autotune_config* cfg, float* chosen, float* sah_cost,
+                                 shn_autotune_report* report, void* stream);
 /* Builds every scene's grid (plans buffers with one read-back on the first
  * call or after a lambda change).  Synchronises. */
 shn_status shn_batch_build(shn_batch* b, void* stream);

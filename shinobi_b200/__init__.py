@@ -498,6 +498,29 @@ class Batch:
             seed, out.ctypes.data_as(C.c_void_p), _stream(stream)), "shn_batch_autotune")
         return out
 
+    def autotune_ex(self, candidates, expected_rays, sample_rays=16384, seed=7, sah_keep=0,
+                    blocks_per_sm=(), stream=None):
+        """The autotuner with the SAH pruning term (time only the sah_keep candidates of least SAH
+        cost per scene) and the trace kernel's blocks per SM as a timed term.
+        -> (chosen lambdas, SAH cost of each, report dict)."""
+        c = np.ascontiguousarray(candidates, np.float32)
+        e = np.ascontiguousarray(expected_rays, np.uint32)
+        cfg = _abi.AutotuneConfig()
+        cfg.sah_keep = sah_keep
+        cfg.num_block_shapes = len(blocks_per_sm)
+        for i, v in enumerate(blocks_per_sm):
+            cfg.blocks_per_sm[i] = int(v)
+        rep = _abi.AutotuneReport()
+        out = np.zeros(self.num_scenes, np.float32)
+        sah = np.zeros(self.num_scenes, np.float32)
+        self.ctx.check(self.ctx.lib.shn_batch_autotune_ex(
+            self.handle, c.ctypes.data_as(C.c_void_p), c.size, e.ctypes.data_as(C.c_void_p), sample_rays,
+            seed, C.byref(cfg), out.ctypes.data_as(C.c_void_p), sah.ctypes.data_as(C.c_void_p), C.byref(rep),
+            _stream(stream)), "shn_batch_autotune_ex")
+        report = {"timed_candidates": int(rep.timed_candidates), "blocks_per_sm": int(rep.blocks_per_sm),
+                  "shape_ms": [float(x) for x in rep.shape_ms[:len(blocks_per_sm)]]}
+        return out, sah, report
+
     def build(self, stream=None):
         self.ctx.check(self.ctx.lib.shn_batch_build(self.handle, _stream(stream)), "shn_batch_build")
         return self

@@ -74,6 +74,14 @@ class SahResult(C.Structure):
                 ("num_tested", u64)]
 
 
+class AutotuneConfig(C.Structure):
+    _fields_ = [("sah_keep", u32), ("num_block_shapes", u32), ("blocks_per_sm", u32 * 8)]
+
+
+class AutotuneReport(C.Structure):
+    _fields_ = [("timed_candidates", u32), ("blocks_per_sm", u32), ("shape_ms", f32 * 8)]
+
+
 class DiParams(C.Structure):
     _fields_ = [("light", AreaLight), ("samples", u32), ("seed", u32), ("image_id", u32),
                 ("tri_material", vp), ("diffuse", vp), ("num_materials", u32),
@@ -136,6 +144,8 @@ SIGNATURES = {
     "shn_batch_create": ([vp, u32, vp, vp, vp, vp, u32, vp, C.POINTER(vp)], i32),
     "shn_batch_set_lambdas": ([vp, vp], i32),
     "shn_batch_autotune": ([vp, vp, u32, vp, u32, u32, vp, vp], i32),
+    "shn_batch_autotune_ex": ([vp, vp, u32, vp, u32, u32, C.POINTER(AutotuneConfig), vp, vp,
+                               C.POINTER(AutotuneReport), vp], i32),
     "shn_batch_build": ([vp, vp], i32),
     "shn_batch_trace": ([vp, C.POINTER(Rays), vp, C.POINTER(Hits), vp, vp], i32),
     "shn_batch_capture": ([vp, C.POINTER(Rays), vp, C.POINTER(Hits), vp], i32),

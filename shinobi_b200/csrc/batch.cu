@@ -55,6 +55,7 @@ struct shn_batch {
   uint32_t* d_counter = nullptr;
   float build_ms = 0.f;
   int blocks_closest = 0, blocks_any = 0;  // persistent grid sizes (computed before any capture)
+  uint32_t bps_closest = 0;                // autotuned blocks per SM of the closest-hit trace (0: occupancy)
 };
 
 namespace shn {
@@ -197,7 +198,8 @@ shn_status plan(shn_batch* b, cudaStream_t st) {
   }
   if (co >= (1ull << 32)) return set_error(b->ctx, SHN_ERR_INVALID, "batch has more than 2^32 cells");
   b->total_cells = co;
-  b->blocks_closest = batch_blocks(k_batch_trace<false>, b->ctx->num_sms);
+  b->blocks_closest = b->bps_closest ? (int)b->bps_closest * b->ctx->num_sms
+                                      : batch_blocks(k_batch_trace<false>, b->ctx->num_sms);
   b->blocks_any = batch_blocks(k_batch_trace<true>, b->ctx->num_sms);
   cudaError_t e = own(b, (void**)&b->d_scenes, sizeof(BatchScene) * b->ns, st);
   if (e == cudaSuccess) e = own(b, (void**)&b->offs, ((size_t)b->T + 1) * 4, st);
@@ -469,7 +471,18 @@ shn_status shn_batch_sync_status(shn_batch* b, void* stream) {
 shn_status shn_batch_autotune(shn_batch* b, const float* candidates, uint32_t num_candidates,
                               const uint32_t* expected_rays, uint32_t sample_rays, uint32_t seed,
                               float* chosen, void* stream) {
+  return shn_batch_autotune_ex(b, candidates, num_candidates, expected_rays, sample_rays, seed, nullptr, chosen,
+                               nullptr, nullptr, stream);
+}
+
+shn_status shn_batch_autotune_ex(shn_batch* b, const float* candidates, uint32_t num_candidates,
+                                 const uint32_t* expected_rays, uint32_t sample_rays, uint32_t seed,
+                                 const shn_autotune_config* cfg, float* chosen, float* sah_out,
+                                 shn_autotune_report* report, void* stream) {
   if (!b || !candidates || num_candidates == 0 || !expected_rays || sample_rays == 0) return SHN_ERR_INVALID;
+  const uint32_t keep = cfg ? cfg->sah_keep : 0u;
+  const uint32_t nshapes = cfg ? cfg->num_block_shapes : 0u;
+  if (nshapes > 8 || (keep && num_candidates > 32)) return SHN_ERR_INVALID;
   cudaStream_t st = (cudaStream_t)stream;
   shn_ctx* ctx = b->ctx;
   // sample rays (same distribution as the batched workload)
@@ -484,13 +497,16 @@ shn_status shn_batch_autotune(shn_batch* b, const float* candidates, uint32_t nu
   shn_rays rays{cols[0], cols[1], cols[2], cols[3], cols[4], cols[5], nullptr};
   shn_hits hits{(uint32_t*)cols[6], cols[7], nullptr, nullptr};
   shn_status rc = SHN_OK;
-  cudaEvent_t e0, e1, e2;
-  cudaEventCreate(&e0);
+  cudaEvent_t e1, e2;
   cudaEventCreate(&e1);
   cudaEventCreate(&e2);
   shn_grid* g = nullptr;
   shn_grid_create(ctx, &g);
-  std::vector<float> best(b->ns, candidates[0]);
+  std::vector<float> best(b->ns, candidates[0]), best_sah(b->ns, 0.f);
+  std::vector<int32_t> cres(3 * (size_t)num_candidates);
+  std::vector<float> ccost(num_candidates);
+  std::vector<uint32_t> order(num_candidates);
+  uint32_t timed = 0;
   for (uint32_t s = 0; s < b->ns && rc == SHN_OK; ++s) {
     const uint32_t nt = b->tri_off[s + 1] - b->tri_off[s];
     if (nt == 0) continue;
@@ -502,14 +518,27 @@ shn_status shn_batch_autotune(shn_batch* b, const float* candidates, uint32_t nu
     sc.tri = b->tri + 3 * (size_t)b->tri_off[s];  // the scene's records, in place
     sc.ids = b->tri;                               // their ids count from the batch's first record
     memcpy(sc.bounds, &b->bounds[6 * s], 24);
-    double best_cost = 1e300;
     for (uint32_t c = 0; c < num_candidates; ++c) {
+      compute_resolution(nt, sc.bounds, candidates[c], 1, 1, &cres[3 * (size_t)c]);
+      order[c] = c;
+    }
+    if (keep || sah_out) {
+      // the SAH term: one counting launch over the scene for all candidates
+      for (uint32_t c0 = 0; c0 < num_candidates && rc == SHN_OK; c0 += 32)
+        rc = sah_refs_list(ctx, sc.tri, nt, sc.bounds, &cres[3 * (size_t)c0], std::min(32u, num_candidates - c0),
+                           nullptr, &ccost[c0], st);
+      if (rc) break;
+      if (keep)
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return ccost[x] < ccost[y]; });
+    }
+    const uint32_t ntime = keep ? std::min(keep, num_candidates) : num_candidates;
+    double best_cost = 1e300;
+    for (uint32_t k = 0; k < ntime; ++k) {
+      const uint32_t c = order[k];
       shn_grid_params p;
       shn_grid_params_default(SHN_GRID_UNIFORM, &p);
       p.lambda = candidates[c];
-      const auto t0 = std::chrono::steady_clock::now();
       rc = build_grid(g, &sc, &p, st);
-      const double build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
       if (rc) break;
       const uint32_t m = std::min(sample_rays, std::max<uint32_t>(expected_rays[s], 1024u));
       cudaEventRecord(e1, st);
@@ -517,25 +546,78 @@ shn_status shn_batch_autotune(shn_batch* b, const float* candidates, uint32_t nu
       cudaEventRecord(e2, st);
       cudaEventSynchronize(e2);
       if (rc) break;
+      ++timed;
       float trace_ms = 0.f;
       cudaEventElapsedTime(&trace_ms, e1, e2);
       const double cost = (double)g->build_ms + (double)trace_ms * ((double)expected_rays[s] / (double)m);
-      (void)build_ms;
       if (cost < best_cost) {
         best_cost = cost;
         best[s] = candidates[c];
+        best_sah[s] = ccost[c];
       }
     }
   }
   shn_grid_destroy(g);
-  cudaEventDestroy(e0);
+  if (rc == SHN_OK) rc = shn_batch_set_lambdas(b, best.data());
+  // the block-shape term: the persistent trace's resident blocks per SM, timed
+  // on the chosen grids with the sample rays spread over the scenes like the
+  // expected rays
+  float shape_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (rc == SHN_OK && nshapes) {
+    rc = shn_batch_build(b, st);
+    double total = 0.0;
+    for (uint32_t s = 0; s < b->ns; ++s) total += expected_rays[s];
+    std::vector<uint32_t> offs(b->ns + 1, 0u);
+    double acc = 0.0;
+    for (uint32_t s = 0; s < b->ns; ++s) {
+      acc += expected_rays[s];
+      offs[s + 1] = total > 0.0 ? (uint32_t)std::min<double>(sample_rays, std::floor(sample_rays * (acc / total)))
+                                : sample_rays;
+    }
+    offs[b->ns] = sample_rays;
+    if (rc == SHN_OK) rc = upload_ray_offsets(b, offs.data(), st);
+    float best_ms = FLT_MAX;
+    uint32_t best_bps = 0;
+    for (uint32_t i = 0; i < nshapes && rc == SHN_OK; ++i) {
+      const uint32_t bps = cfg->blocks_per_sm[i];
+      b->blocks_closest = bps ? (int)bps * ctx->num_sms : batch_blocks(k_batch_trace<false>, ctx->num_sms);
+      float t[3];
+      for (int r = 0; r < 3; ++r) {
+        cudaEventRecord(e1, st);
+        enqueue_trace(b, &rays, sample_rays, &hits, nullptr, st);
+        cudaEventRecord(e2, st);
+        e = cudaEventSynchronize(e2);
+        if (e != cudaSuccess) {
+          rc = cuda_status(ctx, e, "autotune shapes");
+          break;
+        }
+        cudaEventElapsedTime(&t[r], e1, e2);
+      }
+      if (rc) break;
+      std::sort(t, t + 3);
+      shape_ms[i] = t[1];
+      if (t[1] < best_ms) {
+        best_ms = t[1];
+        best_bps = bps;
+      }
+    }
+    b->bps_closest = best_bps;
+    b->blocks_closest = best_bps ? (int)best_bps * ctx->num_sms : batch_blocks(k_batch_trace<false>, ctx->num_sms);
+    if (report) report->blocks_per_sm = best_bps;
+  }
   cudaEventDestroy(e1);
   cudaEventDestroy(e2);
   dev_free(ctx, rb, rbytes, st);
   cudaStreamSynchronize(st);
   if (rc) return rc;
   if (chosen) memcpy(chosen, best.data(), 4 * (size_t)b->ns);
-  return shn_batch_set_lambdas(b, best.data());
+  if (sah_out) memcpy(sah_out, best_sah.data(), 4 * (size_t)b->ns);
+  if (report) {
+    report->timed_candidates = timed;
+    if (!nshapes) report->blocks_per_sm = b->bps_closest;
+    memcpy(report->shape_ms, shape_ms, sizeof(shape_ms));
+  }
+  return SHN_OK;
 }
 
 shn_status shn_batch_info(const shn_batch* b, uint64_t* num_pairs, uint64_t* total_cells, float* build_ms) {

@@ -137,6 +137,10 @@ Geom make_geom(const float b[6], const int res[3]);
 void compute_resolution(uint32_t nt, const float b[6], float lambda, int divisor, int min_res,
                         int out[3]);
 shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p, cudaStream_t st);
+// Bounding-box cell references (countRefs) and SAH cost of k <= 32
+// resolutions res[3*i..3*i+2] over nt 48-byte triangle records; synchronous.
+shn_status sah_refs_list(shn_ctx* ctx, const float4* tri, uint32_t nt, const float b[6], const int32_t* res,
+                         uint32_t k, uint64_t* refs, float* cost, cudaStream_t st);
 void launch_pack_triangles(const float* vtx, const uint32_t* idx, uint32_t nt, float4* tri,
                            cudaStream_t st);
 void launch_bounds_reduce(const float4* tri, uint32_t nt, float* d_out6, cudaStream_t st);

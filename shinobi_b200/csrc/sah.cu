@@ -261,28 +261,28 @@ extern "C" shn_status shn_grid_sah_resolution(const shn_scene* s, float lambda, 
   return SHN_OK;
 }
 
-extern "C" shn_status shn_grid_sah_cost(const shn_scene* s, const int32_t* res, uint32_t k, uint64_t* refs,
-                                        float* cost, void* stream) {
-  if (!s || !res || (!refs && !cost) || k == 0 || k > kMaxCandidates) return SHN_ERR_INVALID;
-  shn_ctx* ctx = s->ctx;
+namespace shn {
+
+shn_status sah_refs_list(shn_ctx* ctx, const float4* tri, uint32_t nt, const float b[6], const int32_t* res,
+                         uint32_t k, uint64_t* refs, float* cost, cudaStream_t st) {
+  if (k == 0 || k > (uint32_t)kMaxCandidates) return set_error(ctx, SHN_ERR_INVALID, "1 to 32 resolutions");
   Candidates c{};
   for (uint32_t i = 0; i < k; ++i)
     for (int a = 0; a < 3; ++a) {
-      if (res[3 * i + a] < 1 || res[3 * i + a] > 2048) return set_error(ctx, SHN_ERR_INVALID, "resolution outside [1, 2048]");
+      if (res[3 * i + a] < 1 || res[3 * i + a] > 2048)
+        return set_error(ctx, SHN_ERR_INVALID, "resolution outside [1, 2048]");
       c.res[i][a] = res[3 * i + a];
     }
-  cudaStream_t st = (cudaStream_t)stream;
   std::vector<uint64_t> h(k, 0ull);
-  if (s->nt) {
+  if (nt) {
     void* ws = nullptr;
     cudaError_t e = dev_alloc(ctx, &ws, 8 * (size_t)k, st);
     if (e != cudaSuccess)
       return set_error(ctx, e == cudaErrorNotPermitted ? SHN_ERR_BUDGET : SHN_ERR_OOM, "SAH counts");
     cudaMemsetAsync(ws, 0, 8 * (size_t)k, st);
-    const V3 bmin = mk(s->bounds[0], s->bounds[1], s->bounds[2]), bmax = mk(s->bounds[3], s->bounds[4], s->bounds[5]);
-    const unsigned blocks = std::min<unsigned>((s->nt + 255) / 256, 148u * 8u);
-    k_sah_list<<<blocks, 256, 0, st>>>(s->tri, s->nt, bmin, bmax, c, (int)k,
-                                                               (unsigned long long*)ws);
+    const V3 bmin = mk(b[0], b[1], b[2]), bmax = mk(b[3], b[4], b[5]);
+    const unsigned blocks = std::min<unsigned>((nt + 255) / 256, 148u * 8u);
+    k_sah_list<<<blocks, 256, 0, st>>>(tri, nt, bmin, bmax, c, (int)k, (unsigned long long*)ws);
     cudaMemcpyAsync(h.data(), ws, 8 * (size_t)k, cudaMemcpyDeviceToHost, st);
     dev_free(ctx, ws, 8 * (size_t)k, st);
     e = cudaStreamSynchronize(st);
@@ -290,7 +290,15 @@ extern "C" shn_status shn_grid_sah_cost(const shn_scene* s, const int32_t* res, 
   }
   for (uint32_t i = 0; i < k; ++i) {
     if (refs) refs[i] = h[i];
-    if (cost) cost[i] = sah_cost(s->bounds, res + 3 * i, h[i]);
+    if (cost) cost[i] = sah_cost(b, res + 3 * i, h[i]);
   }
   return SHN_OK;
+}
+
+}  // namespace shn
+
+extern "C" shn_status shn_grid_sah_cost(const shn_scene* s, const int32_t* res, uint32_t k, uint64_t* refs,
+                                        float* cost, void* stream) {
+  if (!s || !res || (!refs && !cost) || k == 0 || k > (uint32_t)kMaxCandidates) return SHN_ERR_INVALID;
+  return sah_refs_list(s->ctx, s->tri, s->nt, s->bounds, res, k, refs, cost, (cudaStream_t)stream);
 }

@@ -97,3 +97,30 @@ def test_batch_autotune_picks_candidates(gpu):
     for s, og in enumerate(_oracle_grids(scs, chosen)):
         ex = bt.export_scene(s, og.cells.shape[0], og.indices.size)
         assert np.array_equal(ex["cells"], og.cells)
+
+
+def test_batch_autotune_sah_and_block_shapes(gpu):
+    import shinobi_b200 as shn
+    scs = _scenes()[:4]
+    bt = shn.Batch(scs)
+    cands = np.array([0.5, 1.0, 3.0, 8.0], np.float32)
+    chosen, sah, rep = bt.autotune_ex(cands, expected_rays=[100000] * 4, sample_rays=8192, sah_keep=2,
+                                      blocks_per_sm=(0, 4, 6))
+    assert set(chosen.tolist()) <= set(cands.tolist())
+    nonempty = sum(1 for sc in scs if sc.num_triangles)
+    assert rep["timed_candidates"] == 2 * nonempty
+    assert rep["blocks_per_sm"] in (0, 4, 6) and all(ms > 0 for ms in rep["shape_ms"])
+    # the chosen candidate is one of the two of least SAH cost, and its cost is the oracle's
+    for s, sc in enumerate(scs):
+        if not sc.num_triangles:
+            continue
+        b = oracle.bounds(sc.vertices, sc.indices)
+        costs = [oracle.sah_cost(sc.vertices, sc.indices, b, oracle.resolution(sc.num_triangles, b, float(l)))[1]
+                 for l in cands]
+        kept = np.argsort(np.array(costs, np.float32), kind="stable")[:2]
+        assert chosen[s] in cands[kept]
+        assert np.float32(sah[s]) == np.float32(costs[int(np.where(cands == chosen[s])[0][0])])
+    bt.build()
+    for s, og in enumerate(_oracle_grids(scs, chosen)):
+        ex = bt.export_scene(s, og.cells.shape[0], og.indices.size)
+        assert np.array_equal(ex["cells"], og.cells)
