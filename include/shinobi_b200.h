@@ -429,8 +429,9 @@ shn_status shn_batch_autotune(shn_batch* b, const float* candidates, uint32_t nu
  *    sah_keep cheapest are built and timed; 0 times them all.
  *  blocks_per_sm[0 .. num_block_shapes): resident blocks per SM of the
  *    batch's persistent closest-hit trace kernel (block of 128 threads) to
- *    time on the chosen grids with sample_rays rays spread over the scenes
- *    like expected_rays; the fastest is kept for later traces and captures.
+ *    time on the chosen grids with max(sample_rays, 2^21) random rays
+ *    spread over the scenes like expected_rays (median of three launches
+ *    each); the fastest is kept for later traces and captures.
  *    0 entries: the occupancy limit.
  * sah_cost (optional, num_scenes) receives the chosen candidate's SAH cost;
  * report (optional) the work done and the shape timings.  Synchronises. */

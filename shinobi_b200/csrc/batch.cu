@@ -565,16 +565,30 @@ shn_status shn_batch_autotune_ex(shn_batch* b, const float* candidates, uint32_t
   float shape_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (rc == SHN_OK && nshapes) {
     rc = shn_batch_build(b, st);
+    // a launch that fills the GPU many times over: at least 2^21 rays
+    const uint32_t m = std::max<uint32_t>(sample_rays, 1u << 21);
+    float* sb = nullptr;
+    const size_t sbytes = (size_t)m * 4 * 8;
+    if (rc == SHN_OK) {
+      e = dev_alloc(ctx, (void**)&sb, sbytes, st);
+      if (e != cudaSuccess) rc = alloc_err(b, e, "autotune shape rays");
+    }
+    float* sc8[8];
+    for (int k = 0; k < 8; ++k) sc8[k] = sb ? sb + (size_t)k * m : nullptr;
+    shn_rays srays{sc8[0], sc8[1], sc8[2], sc8[3], sc8[4], sc8[5], nullptr};
+    shn_hits shits{(uint32_t*)sc8[6], sc8[7], nullptr, nullptr};
+    if (rc == SHN_OK)
+      k_random_rays<<<(m + 255) / 256, 256, 0, st>>>(m, seed + 1u, -1.f, 2.f, sc8[0], sc8[1], sc8[2], sc8[3],
+                                                     sc8[4], sc8[5]);
     double total = 0.0;
     for (uint32_t s = 0; s < b->ns; ++s) total += expected_rays[s];
     std::vector<uint32_t> offs(b->ns + 1, 0u);
     double acc = 0.0;
     for (uint32_t s = 0; s < b->ns; ++s) {
       acc += expected_rays[s];
-      offs[s + 1] = total > 0.0 ? (uint32_t)std::min<double>(sample_rays, std::floor(sample_rays * (acc / total)))
-                                : sample_rays;
+      offs[s + 1] = total > 0.0 ? (uint32_t)std::min<double>(m, std::floor(m * (acc / total))) : m;
     }
-    offs[b->ns] = sample_rays;
+    offs[b->ns] = m;
     if (rc == SHN_OK) rc = upload_ray_offsets(b, offs.data(), st);
     float best_ms = FLT_MAX;
     uint32_t best_bps = 0;
@@ -584,7 +598,7 @@ shn_status shn_batch_autotune_ex(shn_batch* b, const float* candidates, uint32_t
       float t[3];
       for (int r = 0; r < 3; ++r) {
         cudaEventRecord(e1, st);
-        enqueue_trace(b, &rays, sample_rays, &hits, nullptr, st);
+        enqueue_trace(b, &srays, m, &shits, nullptr, st);
         cudaEventRecord(e2, st);
         e = cudaEventSynchronize(e2);
         if (e != cudaSuccess) {
@@ -604,6 +618,7 @@ shn_status shn_batch_autotune_ex(shn_batch* b, const float* candidates, uint32_t
     b->bps_closest = best_bps;
     b->blocks_closest = best_bps ? (int)best_bps * ctx->num_sms : batch_blocks(k_batch_trace<false>, ctx->num_sms);
     if (report) report->blocks_per_sm = best_bps;
+    if (sb) dev_free(ctx, sb, sbytes, st);
   }
   cudaEventDestroy(e1);
   cudaEventDestroy(e2);
