@@ -201,7 +201,7 @@ def load(auto_build: bool = True):
     SHINOBI_B200_LIB may name another build of the library to load instead."""
     global _lib
     if _lib is None:
-        path = os.environ.get("SHINOBI_B200_LIB", _build.LIB)
+        path = os.environ.get("SHINOBI_B200_LIB") or _build.LIB
         if path == _build.LIB and auto_build and _build.stale():
             _build.build()
         if not os.path.exists(path):

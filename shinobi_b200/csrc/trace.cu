@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kTraceBlock, 8) k_trace_camera(GridView G, Cam
                                                               float* ot, float* ou, float* ov,
                                                               unsigned long long* stats,
                                                               uint32_t* err) {
-  warp_trace<KIND, false>(
+  warp_trace<KIND, false, true>(
       G, n, counter,
       [&](uint32_t i, V3& o, V3& d, float& tmax) {
         o = cam.eye;
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kTraceBlock, 9) k_trace_ao(GridView G, AoParam
                                                           unsigned long long* stats,
                                                           uint32_t* err) {
   const uint32_t n = (*d_m) * A.spp;
-  warp_trace<KIND, true>(
+  warp_trace<KIND, true, true>(
       G, n, counter,
       [&](uint32_t r, V3& o, V3& dir, float& tmax) {
         const uint32_t k = r / A.spp, s = r - k * A.spp;
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(kTraceBlock, 9) k_trace_direct(GridView G, DiP
                                                               unsigned long long* stats,
                                                               uint32_t* err) {
   const uint32_t n = (*d_m) * P.spp;
-  warp_trace<KIND, true>(
+  warp_trace<KIND, true, true>(
       G, n, counter,
       [&](uint32_t r, V3& o, V3& dir, float& tmax) {
         const uint32_t k = r / P.spp, s = r - k * P.spp;

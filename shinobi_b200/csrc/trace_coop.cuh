@@ -15,7 +15,8 @@
 //    When several lanes wait on the same large range, each 32-reference chunk
 //    is loaded once and tested against all of their rays (group_range).
 // Lanes whose ray has finished take a new ray from the global pool at the
-// top of the loop (persistent threads with per-lane replenishment).
+// top of the loop (persistent threads), one by one or, for coherent rays, as
+// a warp of 32 once all lanes are done (PACKET).
 //
 // The per-ray sequence of cell visits, tests and continuation decisions is
 // exactly that of trace_uniform / trace_two_level (trace.cuh) (block culling
@@ -872,7 +873,14 @@ SHN_D void lane_result(const Refs& G, const LT& L, Hit& h) {
 // tests) consumes its result.  n rays are taken from *counter (pre-zeroed).
 // GROUP: lanes waiting on the same large range test it together
 // (group_range); worth it for coherent rays (camera, AO, shadow segments).
-template <int KIND, bool ANY, bool GROUP = true, class Acc, class Src, class Sink>
+// PACKET: the warp takes its next 32 rays only when all 32 lanes are idle,
+// so a warp traces 32 consecutive rays (neighbouring pixels, or the samples
+// of neighbouring hits) side by side from their start: their DDA walks stay
+// in step, where lanes refilled one by one drift apart.  On the 1M-triangle
+// cluster at 1920x1080 the camera kernel went from 5.24 to 2.22 ms and the AO
+// kernel from 2.91 to 2.47 ms (identical results); lanes whose ray ends early
+// wait for the warp's last ray instead of starting a new one.
+template <int KIND, bool ANY, bool GROUP = true, bool PACKET = false, class Acc, class Src, class Sink>
 SHN_D void warp_trace_acc(const Acc& acc, uint32_t n, uint32_t* counter, Src&& src, Sink&& sink) {
   using LaneT = typename std::conditional<GROUP, LaneG, Lane>::type;
   // grids without a reference-ordered triangle copy (batched scenes)
@@ -890,7 +898,7 @@ SHN_D void warp_trace_acc(const Acc& acc, uint32_t n, uint32_t* counter, Src&& s
   bool pool_empty = false;
   while (true) {
     const uint32_t idle = __ballot_sync(0xFFFFFFFFu, !has);
-    if (idle && !pool_empty) {
+    if ((PACKET ? idle == 0xFFFFFFFFu : idle != 0u) && !pool_empty) {
       const uint32_t cnt = __popc(idle);
       uint32_t base = 0;
       if (lane == 0) base = atomicAdd(counter, cnt);
@@ -1006,9 +1014,9 @@ struct OneGrid {
   SHN_D Refs refs(uint32_t) const { return refs_of(*G); }
 };
 
-template <int KIND, bool ANY, class Src, class Sink>
+template <int KIND, bool ANY, bool PACKET = false, class Src, class Sink>
 SHN_D void warp_trace(const GridView& G, uint32_t n, uint32_t* counter, Src&& src, Sink&& sink) {
-  warp_trace_acc<KIND, ANY>(
+  warp_trace_acc<KIND, ANY, true, PACKET>(
       OneGrid{&G}, n, counter,
       [&](uint32_t i, V3& o, V3& d, float& tmax, uint32_t& scene, uint32_t&) {
         scene = 0;
