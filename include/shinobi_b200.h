@@ -7,8 +7,9 @@
  * Conventions
  *  - every call returns shn_status; shn_ctx_last_error() gives a message;
  *  - bounded device-side waits (look-back scans, bulk copies) that give up
- *    set an error bit instead of hanging.  Calls that synchronise (builds,
- *    exports) report it themselves; asynchronous calls (traces, AO, direct
+ *    set an error bit instead of hanging.  Calls that synchronise (exports,
+ *    builds up to their last stage) report it themselves; asynchronous calls
+ *    (a build's last stage, traces, AO, direct
  *    illumination, the path tracer, scans, compaction, sorts, batch replays)
  *    leave it in a device word that shn_grid_sync_status /
  *    shn_ctx_sync_status / shn_batch_sync_status /
@@ -246,8 +247,13 @@ typedef struct shn_grid_info {
 
 shn_status shn_grid_create(shn_ctx* ctx, shn_grid** out);
 /* Builds (or rebuilds) the grid over the scene on stream.  Synchronises the
- * stream up to twice (uniform) / four times (two-level) to size buffers from
- * device-side counts, as the reference does.  Traces of the grid read the
+ * stream once (uniform: the pair count) or twice (two-level: the pair count,
+ * then the leaf and leaf-reference counts) to size buffers from device-side
+ * counts, as the reference does, and returns SHN_ERR_TIMEOUT if a bounded
+ * device wait gave up before those points.  The last stage (sort, ranges and
+ * what follows) runs asynchronously on stream: traces, exports and info calls
+ * of the grid, on any stream, are ordered after it, and a wait that gives up
+ * there is reported by shn_grid_sync_status.  Traces of the grid read the
  * scene's triangles (hit records, normals), so the scene must outlive them. */
 shn_status shn_grid_build(shn_grid* g, const shn_scene* s, const shn_grid_params* p, void* stream);
 shn_status shn_grid_get_info(const shn_grid* g, shn_grid_info* out);

@@ -384,7 +384,7 @@ shn_status shn_grid_get_info(const shn_grid* g, shn_grid_info* o) {
                     g->offs_pair.bytes + g->scan.bytes + g->top_ranges.bytes + g->keys[0].bytes +
                     g->keys[1].bytes + g->keys[2].bytes + g->sortws.bytes + g->mhi.bytes + g->perm_tri.bytes +
                     g->cbox.bytes + g->sbox.bytes + g->ldist.bytes;
-  o->build_ms = g->build_ms;
+  o->build_ms = g->built ? grid_build_ms(g) : 0.f;
   return g->built ? SHN_OK : SHN_ERR_NOT_BUILT;
 }
 
@@ -392,8 +392,8 @@ shn_status shn_grid_export(const shn_grid* g, uint32_t* cells, uint32_t* leaves,
                            uint64_t* top_pairs) {
   if (!g) return SHN_ERR_INVALID;
   if (!g->built) return set_error(g->ctx, SHN_ERR_NOT_BUILT, "grid not built");
-  cudaError_t e = cudaSuccess;
-  if (cells && g->num_cells) e = cudaMemcpy(cells, g->cells, g->num_cells * 8, cudaMemcpyDeviceToHost);
+  cudaError_t e = g->ev1 ? cudaEventSynchronize(g->ev1) : cudaSuccess;  // the build's end
+  if (e == cudaSuccess && cells && g->num_cells) e = cudaMemcpy(cells, g->cells, g->num_cells * 8, cudaMemcpyDeviceToHost);
   if (e == cudaSuccess && leaves && g->num_leaves) e = cudaMemcpy(leaves, g->leaves, g->num_leaves * 8, cudaMemcpyDeviceToHost);
   if (e == cudaSuccess && indices && g->num_refs) e = cudaMemcpy(indices, g->indices, g->num_refs * 4, cudaMemcpyDeviceToHost);
   const uint64_t np = g->kind == SHN_GRID_TWO_LEVEL ? g->num_top_refs : g->num_refs;
@@ -436,6 +436,7 @@ shn_status shn_grid_export(const shn_grid* g, uint32_t* cells, uint32_t* leaves,
 
 void shn_grid_destroy(shn_grid* g) {
   if (!g) return;
+  if (g->ev1) cudaEventSynchronize(g->ev1);  // the last build may still run on its stream
   cudaStream_t st = 0;
   shn_ctx* c = g->ctx;
   dev_free(c, g->cells, g->cap_cells, st);
@@ -549,6 +550,7 @@ shn_status shn_grid_sync_status(const shn_grid* g, void* stream) {
     const cudaError_t e = cudaStreamSynchronize(st);
     return e == cudaSuccess ? SHN_OK : cuda_status(g->ctx, e, "grid status");
   }
+  if (g->ev1) cudaEventSynchronize(g->ev1);  // the build's tail, whatever its stream
   return read_and_clear(g->ctx, g->d_err, st, "grid");
 }
 

@@ -549,7 +549,7 @@ shn_status shn_batch_autotune_ex(shn_batch* b, const float* candidates, uint32_t
       ++timed;
       float trace_ms = 0.f;
       cudaEventElapsedTime(&trace_ms, e1, e2);
-      const double cost = (double)g->build_ms + (double)trace_ms * ((double)expected_rays[s] / (double)m);
+      const double cost = (double)grid_build_ms(g) + (double)trace_ms * ((double)expected_rays[s] / (double)m);
       if (cost < best_cost) {
         best_cost = cost;
         best[s] = candidates[c];

@@ -937,18 +937,31 @@ shn_status read_words(shn_grid* g, const uint32_t* d_src[], int k, uint32_t* out
   return SHN_OK;
 }
 
+// The build's last stage is not waited for: the end event orders every
+// consumer (traces on any stream, exports, info), and a bounded wait that
+// gives up in it is reported through the grid's error word
+// (shn_grid_sync_status), like the traces' own.  The two size read-backs
+// before it have already checked the word for the earlier stages.
 shn_status finish(shn_grid* g, cudaStream_t st) {
   cudaEventRecord(g->ev1, st);
-  const uint32_t* none[1] = {g->d_err};
-  uint32_t dummy;
-  shn_status rc = read_words(g, none, 1, &dummy, st);
-  if (rc) return rc;
-  cudaEventElapsedTime(&g->build_ms, g->ev0, g->ev1);
+  g->build_ms_pending = true;
   g->built = true;
   return SHN_OK;
 }
 
 }  // namespace
+
+void grid_fence(const shn_grid* g, cudaStream_t st) {
+  if (g->ev1) cudaStreamWaitEvent(st, g->ev1, 0);
+}
+
+float grid_build_ms(const shn_grid* g) {
+  if (g->build_ms_pending && g->ev1 && cudaEventSynchronize(g->ev1) == cudaSuccess) {
+    cudaEventElapsedTime(&g->build_ms, g->ev0, g->ev1);
+    g->build_ms_pending = false;
+  }
+  return g->build_ms;
+}
 
 shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p, cudaStream_t st) {
   shn_ctx* ctx = g->ctx;

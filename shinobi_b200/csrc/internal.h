@@ -94,8 +94,11 @@ struct shn_grid {
   // failure-detection self test: the next hit compaction of an AO or
   // direct-illumination call withholds its first tile
   mutable std::atomic<uint32_t> force_lookback{0};
+  // ev1: end of the last build on its stream (the build's tail runs
+  // asynchronously; every consumer waits for it, see grid_fence)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  float build_ms = 0.f;
+  mutable float build_ms = 0.f;
+  mutable bool build_ms_pending = false;
   size_t bytes = 0;
   // scene the grid was built over (triangles by id, for shading / AO frames)
   const float4* src_tri = nullptr;
@@ -137,6 +140,10 @@ Geom make_geom(const float b[6], const int res[3]);
 void compute_resolution(uint32_t nt, const float b[6], float lambda, int divisor, int min_res,
                         int out[3]);
 shn_status build_grid(shn_grid* g, const shn_scene* s, const shn_grid_params* p, cudaStream_t st);
+// Orders work on st after the grid's last build (a no-op on the build's own stream).
+void grid_fence(const shn_grid* g, cudaStream_t st);
+// Device time of the last build; waits for its end.
+float grid_build_ms(const shn_grid* g);
 // Bounding-box cell references (countRefs) and SAH cost of k <= 32
 // resolutions res[3*i..3*i+2] over nt 48-byte triangle records; synchronous.
 shn_status sah_refs_list(shn_ctx* ctx, const float4* tri, uint32_t nt, const float b[6], const int32_t* res,

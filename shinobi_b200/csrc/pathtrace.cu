@@ -230,6 +230,7 @@ shn_status shn_pt_render(const shn_grid* g, const shn_scene* s, const shn_camera
                          const shn_pt_params* prm, float* d_image, uint32_t* d_stats, void* stream) {
   if (!g || !s || !cam || !prm || !d_image || prm->spp == 0 || prm->max_depth == 0) return SHN_ERR_INVALID;
   if (!g->built) return set_error(g->ctx, SHN_ERR_NOT_BUILT, "grid not built");
+  grid_fence(g, (cudaStream_t)stream);
   if (!(prm->albedo > 0.f && prm->albedo <= 1.f)) return set_error(g->ctx, SHN_ERR_INVALID, "albedo must be in (0,1]");
   const uint64_t npix = (uint64_t)cam->res_x * cam->res_y;
   if (npix == 0) return SHN_OK;

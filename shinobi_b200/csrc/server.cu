@@ -192,7 +192,12 @@ shn_status build_slot(shn_server* s, const float* vtx, uint32_t nv, const uint32
     shn_scene_destroy(sc);
     return rc;
   }
-  cudaStreamSynchronize(st);
+  rc = shn_grid_sync_status(g, st);  // the build's last stage, then its error word
+  if (rc) {
+    shn_grid_destroy(g);
+    shn_scene_destroy(sc);
+    return rc;
+  }
   out->scene = sc;
   out->grid = g;
   return SHN_OK;

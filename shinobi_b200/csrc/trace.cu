@@ -417,6 +417,7 @@ shn_status shn_trace_closest(const shn_grid* g, const shn_rays* rays, uint32_t n
                              void* stream) {
   if (!g || !rays || !hits) return SHN_ERR_INVALID;
   if (!g->built) return set_error(g->ctx, SHN_ERR_NOT_BUILT, "grid not built");
+  grid_fence(g, (cudaStream_t)stream);
   if (n == 0) return SHN_OK;
   if (!rays->ox || !rays->oy || !rays->oz || !rays->dx || !rays->dy || !rays->dz || !hits->tri || !hits->t)
     return set_error(g->ctx, SHN_ERR_INVALID, "null ray or hit array");
@@ -447,6 +448,7 @@ shn_status shn_trace_any(const shn_grid* g, const shn_rays* rays, uint32_t n, ui
                          void* stream) {
   if (!g || !rays || !d_occluded) return SHN_ERR_INVALID;
   if (!g->built) return set_error(g->ctx, SHN_ERR_NOT_BUILT, "grid not built");
+  grid_fence(g, (cudaStream_t)stream);
   if (n == 0) return SHN_OK;
   if (!rays->ox || !rays->oy || !rays->oz || !rays->dx || !rays->dy || !rays->dz)
     return set_error(g->ctx, SHN_ERR_INVALID, "null ray array");
@@ -477,6 +479,7 @@ shn_status shn_trace_primary(const shn_grid* g, const shn_camera* cam, uint32_t 
                              shn_hits* hits, void* stream) {
   if (!g || !cam || !hits || !hits->tri || !hits->t) return SHN_ERR_INVALID;
   if (!g->built) return set_error(g->ctx, SHN_ERR_NOT_BUILT, "grid not built");
+  grid_fence(g, (cudaStream_t)stream);
   const uint64_t n64 = (uint64_t)cam->res_x * cam->res_y;
   if (n64 == 0) return SHN_OK;
   if (n64 > (1u << 24)) return set_error(g->ctx, SHN_ERR_INVALID, "more than 2^24 pixels");
@@ -509,6 +512,7 @@ shn_status shn_trace_ao(const shn_grid* g, const shn_camera* cam, const shn_hits
                         uint32_t* d_num_rays, void* stream) {
   if (!g || !cam || !primary || !primary->tri || !primary->t || !d_ao || spp == 0) return SHN_ERR_INVALID;
   if (!g->built) return set_error(g->ctx, SHN_ERR_NOT_BUILT, "grid not built");
+  grid_fence(g, (cudaStream_t)stream);
   if (!g->src_tri) return set_error(g->ctx, SHN_ERR_INVALID, "grid has no scene");
   const uint64_t n64 = (uint64_t)cam->res_x * cam->res_y;
   if (n64 == 0) return SHN_OK;
@@ -582,6 +586,7 @@ shn_status shn_shade_direct(const shn_grid* g, const shn_camera* cam, const shn_
   if (!g || !cam || !primary || !primary->tri || !primary->t || !prm || !d_frame || prm->samples == 0)
     return SHN_ERR_INVALID;
   if (!g->built) return set_error(g->ctx, SHN_ERR_NOT_BUILT, "grid not built");
+  grid_fence(g, (cudaStream_t)stream);
   if (!g->src_tri) return set_error(g->ctx, SHN_ERR_INVALID, "grid has no scene");
   if (prm->diffuse && prm->num_materials == 0)
     return set_error(g->ctx, SHN_ERR_INVALID, "diffuse table without materials");
