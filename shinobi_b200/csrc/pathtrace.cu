@@ -8,7 +8,7 @@
 // (64-byte records) for the next bounce, so warps only ever see live paths.
 //
 // Semantics (restated by the oracle path for path):
-//  * path g = sample * npix + pixel; camera ray through the pixel with a
+//  * path g = sample * npix + (the pixel's number in 8x4-tile order); camera ray through the pixel with a
 //    Philox jitter (RandomPixelSampler, src/Primitive/PixelSampler.h:56-70);
 //  * at a hit: facing geometric normal n; next-event estimation to one
 //    point of the parallelogram light (shadow segment, any hit, t < 0.9999
@@ -52,7 +52,10 @@ __global__ void k_pt_camera(PtView P, uint64_t g0, uint32_t count, PathRec* __re
   if (k == 0) *d_n = count;
   if (k >= count) return;
   const uint64_t g = g0 + k;
-  const uint32_t s = (uint32_t)(g / P.npix), p = (uint32_t)(g - (uint64_t)s * P.npix);
+  // path g = sample s, camera ray number g - s * npix, numbered by 8x4 pixel
+  // tiles: a warp's 32 paths are one compact tile of one sample
+  const uint32_t s = (uint32_t)(g / P.npix);
+  const uint32_t p = tile_pixel(P.cam, (uint32_t)(g - (uint64_t)s * P.npix));
   const uint4 w = philox4x32(make_uint4(p, s, 0u, kTagJitter), P.seed, 0u);
   float ox = u01(w.x), oy = u01(w.y);
   const float tmp = (float)p / P.cam.resx;
