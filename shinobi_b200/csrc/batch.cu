@@ -235,12 +235,11 @@ void enqueue_build(shn_batch* b, cudaStream_t st) {
   launch_batch_emit(b->tri, b->T, b->d_tri_off, b->d_scenes, b->ns, b->offs, b->keys[0], b->P, b->d_err,
                     sort_hist_counts(b->sort_ws), b->plan, st);
   b->sorted = onesweep_sort(b->keys[0], b->keys[1], b->P, 32, b->plan, b->sort_ws, b->d_err, st, true);
-  cudaMemsetAsync(b->cells, 0, b->total_cells * 8, st);
   // no reference-ordered triangle copy: the batch's cells hold a few
   // references each and the trace reads a reference's triangle through its
   // id (indices[]), which measured cheaper than gathering and writing 96 bytes
-  // per reference in the build
-  launch_ranges(b->sorted, b->P, b->cells, b->indices, b->tri, b->T, nullptr, st);
+  // per reference in the build; the ranges are written by tiles of cells
+  launch_cell_ranges(b->sorted, b->P, b->total_cells, b->cells, b->indices, st);
 }
 
 GridView batch_view(const shn_batch* b) {

@@ -487,6 +487,62 @@ __global__ void __launch_bounds__(kRangeBlock) k_ranges(const uint64_t* __restri
   }
 }
 
+// Cell ranges by tiles of cells (grids whose range pass writes no triangle
+// copy): block b owns cells [c0, c0 + kCellTile) and their keys [k0, k1)
+// (two binary searches over the sorted keys).  Run starts and ends go to
+// shared memory, then the tile's ranges are written as whole 8-byte words in
+// cell order -- coalesced, every cell written once (empty ones as (0, 0)),
+// so the cell array needs no clearing and no sector of it is written in
+// part -- together with indices[] for its keys.
+constexpr uint32_t kCellTile = 2048;
+
+__global__ void __launch_bounds__(kRangeBlock) k_cell_ranges(const uint64_t* __restrict__ keys, uint32_t n,
+                                                             uint64_t C, uint2* __restrict__ ranges,
+                                                             uint32_t* __restrict__ indices) {
+  __shared__ uint32_t s_b[kCellTile], s_e[kCellTile];
+  __shared__ uint32_t s_k[2];
+  const int lane = threadIdx.x & 31;
+  for (uint64_t c0 = (uint64_t)blockIdx.x * kCellTile; c0 < C; c0 += (uint64_t)gridDim.x * kCellTile) {
+    const uint64_t c1 = c0 + kCellTile < C ? c0 + kCellTile : C;
+    for (uint32_t i = threadIdx.x; i < kCellTile; i += kRangeBlock) {
+      s_b[i] = 0u;
+      s_e[i] = 0u;
+    }
+    if (threadIdx.x < 2) {
+      const uint64_t target = threadIdx.x == 0 ? c0 : c1;
+      uint32_t lo = 0, hi = n;  // first key whose cell >= target
+      while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2;
+        if ((__ldg(keys + mid) >> 32) < target) lo = mid + 1;
+        else hi = mid;
+      }
+      s_k[threadIdx.x] = lo;
+    }
+    __syncthreads();
+    const uint32_t k0 = s_k[0], k1 = s_k[1];
+    // whole warps step through [k0, k1) so that neighbours come by shuffles
+    for (uint32_t w0 = k0 + (threadIdx.x & ~31u); w0 < k1; w0 += kRangeBlock) {
+      const uint32_t i = w0 + lane;
+      const bool in = i < k1;
+      const uint64_t k = in ? __ldcs(keys + i) : 0ull;
+      const uint32_t c = (uint32_t)(k >> 32);
+      uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, c, 1);
+      uint32_t next = __shfl_down_sync(0xFFFFFFFFu, c, 1);
+      if (in) {
+        if (lane == 0) prev = i > k0 ? (uint32_t)(__ldg(keys + i - 1) >> 32) : ~c;
+        if (lane == 31 || i + 1 == k1) next = i + 1 < k1 ? (uint32_t)(__ldg(keys + i + 1) >> 32) : ~c;
+        if (prev != c) s_b[c - (uint32_t)c0] = i;
+        if (next != c) s_e[c - (uint32_t)c0] = i + 1;
+        __stcs(indices + i, (uint32_t)k);
+      }
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < (uint32_t)(c1 - c0); j += kRangeBlock)
+      __stcs(reinterpret_cast<uint2*>(ranges) + c0 + j, make_uint2(s_b[j], s_e[j]));
+    __syncthreads();
+  }
+}
+
 // ---- spatial order and block boxes (two-level grids) -------------------------
 // The build of a two-level grid runs on a copy of the triangles sorted by the
 // Morton code of their vertex sum in the scene box (20 bits per axis), so that
@@ -624,7 +680,16 @@ __global__ void k_leaf_dist(const uint2* __restrict__ cells, uint32_t C, uint2* 
   for (uint32_t li = blockIdx.x * blockDim.x + threadIdx.x; li < L; li += gridDim.x * blockDim.x) {
     uint32_t c;
     if (AXIS == 0) {
-      c = leaf_owner(cells, C, li);
+      // the warp's leaves are consecutive and nearly always share one top
+      // cell: one search for the warp, a search per lane only past its end
+      const unsigned am = __activemask();
+      const int leader = __ffs(am) - 1;
+      uint32_t c0 = 0;
+      if ((int)(threadIdx.x & 31) == leader) c0 = leaf_owner(cells, C, li);
+      c0 = __shfl_sync(am, c0, leader);
+      const uint2 w0 = __ldg(cells + c0);
+      const uint32_t n0 = (w0.y & kNotEmpty) ? (w0.y & 0xFFu) * ((w0.y >> 8) & 0xFFu) * ((w0.y >> 16) & 0xFFu) : 0u;
+      c = (li >= w0.x && li - w0.x < n0) ? c0 : leaf_owner(cells, C, li);
       owner[li] = c;
     } else {
       c = __ldg(owner + li);
@@ -1194,6 +1259,14 @@ void launch_batch_emit(const float4* tri, uint32_t T, const uint32_t* tri_off, c
   if (T)
     k_emit_units<<<emit_blocks(T), kScanBlock, 0, st>>>(BatchMaker{ts, tri_off, scenes, ns}, T, offs, keys,
                                                        capacity, err, hist, hplan);
+}
+
+void launch_cell_ranges(const uint64_t* keys, uint32_t n, uint64_t C, uint2* ranges, uint32_t* indices,
+                        cudaStream_t st) {
+  if (!C) return;
+  const uint64_t tiles = (C + kCellTile - 1) / kCellTile;
+  k_cell_ranges<<<(unsigned)std::min<uint64_t>(tiles, 148u * 16u), kRangeBlock, 0, st>>>(keys, n, C, ranges,
+                                                                                         indices);
 }
 
 void launch_ranges(const uint64_t* keys, uint32_t n, uint2* ranges, uint32_t* indices,

@@ -169,6 +169,10 @@ void launch_batch_count(const float4* tri, uint32_t T, const uint32_t* tri_off, 
 void launch_batch_emit(const float4* tri, uint32_t T, const uint32_t* tri_off, const BatchScene* scenes,
                        uint32_t ns, const uint32_t* offs, uint64_t* keys, uint32_t capacity,
                        uint32_t* err, uint32_t* hist, SortPlan hplan, cudaStream_t st);
+// Ranges of all C cells (empty ones (0, 0)) and indices[], written by tiles
+// of cells: needs no cleared cell array.
+void launch_cell_ranges(const uint64_t* keys, uint32_t n, uint64_t C, uint2* ranges, uint32_t* indices,
+                        cudaStream_t st);
 void launch_ranges(const uint64_t* keys, uint32_t n, uint2* ranges, uint32_t* indices,
                    const float4* tri, uint32_t T, float4* rtri, cudaStream_t st);
 
