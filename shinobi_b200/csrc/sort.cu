@@ -32,13 +32,7 @@ namespace {
 constexpr int kSortBlock = 512;
 constexpr int kSortWarps = kSortBlock / 32;
 constexpr int kPassItems = 12;            // keys per thread: 6144-key tiles, two per SM
-constexpr int kMinTile = kSortBlock * 8;  // sizes the look-back status array (large sorts)
-// Sorts of at most kSmallSort keys run 2048-key tiles, three blocks per SM:
-// with 6144-key tiles they would fill fewer than the 296 resident tile slots
-// of the GPU, and each pass would take a full tile lifetime regardless of n.
-constexpr uint32_t kSmallSort = 1u << 22;
-constexpr int kSmallItems = 4;
-constexpr int kSmallTile = kSortBlock * kSmallItems;
+constexpr int kMinTile = kSortBlock * 8;  // sizes the look-back status array
 constexpr int kMaxBins = 512;             // 9-bit digits
 constexpr int kHistBlock = 256;
 constexpr uint32_t kDigFlagAgg = 1u << 30;
@@ -304,14 +298,12 @@ __global__ void __launch_bounds__(kSortBlock, MINB) k_onesweep(const uint64_t* _
 
 }  // namespace
 
-uint32_t sort_tiles(uint32_t n) {
-  const uint32_t t = n <= kSmallSort ? (uint32_t)kSmallTile : (uint32_t)kMinTile;
-  return (uint32_t)(((size_t)n + t - 1) / t);
+size_t sort_workspace_bytes(uint32_t n) {
+  const size_t tiles = ((size_t)n + kMinTile - 1) / kMinTile;
+  return (4 * kMaxBins + 8) * sizeof(uint32_t) + tiles * kMaxBins * sizeof(uint32_t);
 }
 
-size_t sort_workspace_bytes(uint32_t n) {
-  return (4 * kMaxBins + 8) * sizeof(uint32_t) + (size_t)sort_tiles(n) * kMaxBins * sizeof(uint32_t);
-}
+uint32_t sort_tiles(uint32_t n) { return (uint32_t)(((size_t)n + kMinTile - 1) / kMinTile); }
 
 uint32_t* sort_hist_counts(void* ws) { return (uint32_t*)ws; }
 
@@ -386,18 +378,11 @@ uint64_t* onesweep_sort(uint64_t* buf0, uint64_t* buf1, uint32_t n, uint32_t lo_
     const uint32_t shift = lo_bit + plan.width * p;
     const uint32_t w = std::min(plan.width, plan.bits - plan.width * p);
     const uint32_t mask = (1u << w) - 1u;
-    const bool small = n <= kSmallSort;
-    if (plan.width == 9) {
-      if (small)
-        launch_pass<kSmallItems, 3, 9>(src, dst, n, shift, mask, hist + p * kMaxBins, status, tickets + p, d_err, st);
-      else
-        launch_pass<kPassItems, 2, 9>(src, dst, n, shift, mask, hist + p * kMaxBins, status, tickets + p, d_err, st);
-    } else {
-      if (small)
-        launch_pass<kSmallItems, 3, 8>(src, dst, n, shift, mask, hist + p * kMaxBins, status, tickets + p, d_err, st);
-      else
-        launch_pass<kPassItems, 2, 8>(src, dst, n, shift, mask, hist + p * kMaxBins, status, tickets + p, d_err, st);
-    }
+    if (plan.width == 9)
+      launch_pass<kPassItems, 2, 9>(src, dst, n, shift, mask, hist + p * kMaxBins, status, tickets + p, d_err, st);
+    else
+      launch_pass<kPassItems, 2, 8>(src, dst, n, shift, mask, hist + p * kMaxBins, status, tickets + p, d_err,
+                                    st);
     std::swap(src, dst);
   }
   return src;
