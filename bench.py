@@ -717,7 +717,8 @@ def run_batch(args, emit=True):
     t0 = time.perf_counter()
     cands = np.array([0.5, 0.75, 1.0, 1.5, 2.0, 3.0], np.float32)
     chosen, chosen_sah, tune_report = bt.autotune_ex(cands, expected_rays=rays.astype(np.uint32),
-                                                     sample_rays=16384, blocks_per_sm=(0, 4, 6))
+                                                     sample_rays=16384, blocks_per_sm=(0, 4, 6),
+                                                     sort_tiles=(6144, 4096))
     t_tune = time.perf_counter() - t0
     bt.build()
     torch.cuda.synchronize()
@@ -798,6 +799,8 @@ def run_batch(args, emit=True):
         "autotune": {"timed_candidates": tune_report["timed_candidates"],
                      "trace_blocks_per_sm": tune_report["blocks_per_sm"],
                      "shape_ms": dict(zip(("occupancy", "4", "6"), tune_report["shape_ms"])),
+                     "sort_tile_keys": tune_report["sort_tile_keys"],
+                     "sort_tile_build_ms": dict(zip(("6144", "4096"), tune_report["sort_tile_ms"])),
                      "sah_cost_chosen_median": float(np.median(chosen_sah))},
         "roofline_build": {"bound": "hbm", "achieved": b_build / (bms * 1e-3) / 1e9, "peak": peaks["hbm_gbs"],
                            "unit": "GB/s", "frac": b_build / (bms * 1e-3) / 1e9 / peaks["hbm_gbs"],

@@ -439,17 +439,24 @@ shn_status shn_batch_autotune(shn_batch* b, const float* candidates, uint32_t nu
  *    spread over the scenes like expected_rays (median of three launches
  *    each); the fastest is kept for later traces and captures.
  *    0 entries: the occupancy limit.
+ *  sort_tile_keys[0 .. num_sort_tiles): keys per tile of the batch's
+ *    onesweep passes (4096 or 6144), each timed as the batch's whole build
+ *    (median of three) on the chosen grids; the fastest is kept.
  * sah_cost (optional, num_scenes) receives the chosen candidate's SAH cost;
  * report (optional) the work done and the shape timings.  Synchronises. */
 typedef struct shn_autotune_config {
   uint32_t sah_keep;
   uint32_t num_block_shapes;  /* <= 8 */
   uint32_t blocks_per_sm[8];
+  uint32_t num_sort_tiles;    /* <= 4: onesweep tile shapes to time on the batch's build */
+  uint32_t sort_tile_keys[4]; /* keys per tile: 4096 or 6144 (0: 6144) */
 } shn_autotune_config;
 typedef struct shn_autotune_report {
   uint32_t timed_candidates;  /* (scene, lambda) builds timed */
   uint32_t blocks_per_sm;     /* chosen (0: occupancy limit) */
   float shape_ms[8];          /* median sample trace time per blocks_per_sm entry */
+  uint32_t sort_tile_keys;    /* chosen keys per onesweep tile */
+  float sort_tile_ms[4];      /* median whole-build time per sort_tile_keys entry */
 } shn_autotune_report;
 shn_status shn_batch_autotune_ex(shn_batch* b, const float* candidates, uint32_t num_candidates,
                                  const uint32_t* expected_rays, uint32_t sample_rays, uint32_t seed,

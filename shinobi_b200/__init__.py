@@ -499,7 +499,7 @@ class Batch:
         return out
 
     def autotune_ex(self, candidates, expected_rays, sample_rays=16384, seed=7, sah_keep=0,
-                    blocks_per_sm=(), stream=None):
+                    blocks_per_sm=(), sort_tiles=(), stream=None):
         """The autotuner with the SAH pruning term (time only the sah_keep candidates of least SAH
         cost per scene) and the trace kernel's blocks per SM as a timed term.
         -> (chosen lambdas, SAH cost of each, report dict)."""
@@ -510,6 +510,9 @@ class Batch:
         cfg.num_block_shapes = len(blocks_per_sm)
         for i, v in enumerate(blocks_per_sm):
             cfg.blocks_per_sm[i] = int(v)
+        cfg.num_sort_tiles = len(sort_tiles)
+        for i, v in enumerate(sort_tiles):
+            cfg.sort_tile_keys[i] = int(v)
         rep = _abi.AutotuneReport()
         out = np.zeros(self.num_scenes, np.float32)
         sah = np.zeros(self.num_scenes, np.float32)
@@ -518,7 +521,9 @@ class Batch:
             seed, C.byref(cfg), out.ctypes.data_as(C.c_void_p), sah.ctypes.data_as(C.c_void_p), C.byref(rep),
             _stream(stream)), "shn_batch_autotune_ex")
         report = {"timed_candidates": int(rep.timed_candidates), "blocks_per_sm": int(rep.blocks_per_sm),
-                  "shape_ms": [float(x) for x in rep.shape_ms[:len(blocks_per_sm)]]}
+                  "shape_ms": [float(x) for x in rep.shape_ms[:len(blocks_per_sm)]],
+                  "sort_tile_keys": int(rep.sort_tile_keys),
+                  "sort_tile_ms": [float(x) for x in rep.sort_tile_ms[:len(sort_tiles)]]}
         return out, sah, report
 
     def build(self, stream=None):

@@ -75,11 +75,13 @@ class SahResult(C.Structure):
 
 
 class AutotuneConfig(C.Structure):
-    _fields_ = [("sah_keep", u32), ("num_block_shapes", u32), ("blocks_per_sm", u32 * 8)]
+    _fields_ = [("sah_keep", u32), ("num_block_shapes", u32), ("blocks_per_sm", u32 * 8),
+                ("num_sort_tiles", u32), ("sort_tile_keys", u32 * 4)]
 
 
 class AutotuneReport(C.Structure):
-    _fields_ = [("timed_candidates", u32), ("blocks_per_sm", u32), ("shape_ms", f32 * 8)]
+    _fields_ = [("timed_candidates", u32), ("blocks_per_sm", u32), ("shape_ms", f32 * 8),
+                ("sort_tile_keys", u32), ("sort_tile_ms", f32 * 4)]
 
 
 class DiParams(C.Structure):

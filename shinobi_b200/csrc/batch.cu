@@ -56,6 +56,7 @@ struct shn_batch {
   float build_ms = 0.f;
   int blocks_closest = 0, blocks_any = 0;  // persistent grid sizes (computed before any capture)
   uint32_t bps_closest = 0;                // autotuned blocks per SM of the closest-hit trace (0: occupancy)
+  uint32_t sort_tile = 0;                  // autotuned keys per onesweep tile (0: 6144)
 };
 
 namespace shn {
@@ -234,7 +235,8 @@ void enqueue_build(shn_batch* b, cudaStream_t st) {
   sort_prepare(b->sort_ws, st);
   launch_batch_emit(b->tri, b->T, b->d_tri_off, b->d_scenes, b->ns, b->offs, b->keys[0], b->P, b->d_err,
                     sort_hist_counts(b->sort_ws), b->plan, st);
-  b->sorted = onesweep_sort(b->keys[0], b->keys[1], b->P, 32, b->plan, b->sort_ws, b->d_err, st, true);
+  b->sorted = onesweep_sort(b->keys[0], b->keys[1], b->P, 32, b->plan, b->sort_ws, b->d_err, st, true,
+                            b->sort_tile);
   // no reference-ordered triangle copy: the batch's cells hold a few
   // references each and the trace reads a reference's triangle through its
   // id (indices[]), which measured cheaper than gathering and writing 96 bytes
@@ -619,6 +621,42 @@ shn_status shn_batch_autotune_ex(shn_batch* b, const float* candidates, uint32_t
     if (report) report->blocks_per_sm = best_bps;
     if (sb) dev_free(ctx, sb, sbytes, st);
   }
+  // the sort-tile term: the batch's whole build timed with each tile shape
+  const uint32_t ntiles = cfg ? cfg->num_sort_tiles : 0u;
+  float tile_ms[4] = {0, 0, 0, 0};
+  if (rc == SHN_OK && ntiles) {
+    if (ntiles > 4) rc = set_error(ctx, SHN_ERR_INVALID, "at most 4 sort tile shapes");
+    if (rc == SHN_OK && !b->planned) rc = plan(b, st);
+    float best_ms = FLT_MAX;
+    uint32_t best_tile = 0;
+    for (uint32_t i = 0; i < ntiles && rc == SHN_OK; ++i) {
+      const uint32_t tk = cfg->sort_tile_keys[i];
+      if (tk != 0 && tk != 4096 && tk != 6144) {
+        rc = set_error(ctx, SHN_ERR_INVALID, "sort tile shapes: 4096 or 6144 keys (0: 6144)");
+        break;
+      }
+      b->sort_tile = tk == 6144 ? 0u : tk;
+      float t[3];
+      for (int r = 0; r < 3 && rc == SHN_OK; ++r) {
+        cudaEventRecord(e1, st);
+        enqueue_build(b, st);
+        cudaEventRecord(e2, st);
+        e = cudaEventSynchronize(e2);
+        if (e != cudaSuccess) rc = cuda_status(ctx, e, "autotune sort tiles");
+        else cudaEventElapsedTime(&t[r], e1, e2);
+      }
+      if (rc) break;
+      std::sort(t, t + 3);
+      tile_ms[i] = t[1];
+      if (t[1] < best_ms) {
+        best_ms = t[1];
+        best_tile = b->sort_tile;
+      }
+    }
+    b->sort_tile = best_tile;
+    // the last timed build used the last shape: build once more with the chosen one
+    if (rc == SHN_OK) rc = shn_batch_build(b, st);
+  }
   cudaEventDestroy(e1);
   cudaEventDestroy(e2);
   dev_free(ctx, rb, rbytes, st);
@@ -630,6 +668,8 @@ shn_status shn_batch_autotune_ex(shn_batch* b, const float* candidates, uint32_t
     report->timed_candidates = timed;
     if (!nshapes) report->blocks_per_sm = b->bps_closest;
     memcpy(report->shape_ms, shape_ms, sizeof(shape_ms));
+    report->sort_tile_keys = b->sort_tile ? b->sort_tile : 6144u;
+    memcpy(report->sort_tile_ms, tile_ms, sizeof(tile_ms));
   }
   return SHN_OK;
 }

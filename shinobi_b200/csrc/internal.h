@@ -128,8 +128,10 @@ SortPlan sort_plan(uint32_t bits);          // fewest passes for `bits` key bits
 uint32_t key_bits_for(uint64_t max_key_value);
 size_t sort_workspace_bytes(uint32_t n);
 uint32_t sort_tiles(uint32_t n);
+// tile_keys: keys per onesweep tile, 6144 (default, 0) or 4096
 uint64_t* onesweep_sort(uint64_t* buf0, uint64_t* buf1, uint32_t n, uint32_t lo_bit, SortPlan plan,
-                        void* ws, uint32_t* d_err, cudaStream_t st, bool counts_ready = false);
+                        void* ws, uint32_t* d_err, cudaStream_t st, bool counts_ready = false,
+                        uint32_t tile_keys = 0);
 // digit counts [pass][512] in the sort workspace, for producers that count
 // the digits of the keys they write (sort_prepare zeroes them first)
 uint32_t* sort_hist_counts(void* ws);

@@ -361,7 +361,7 @@ void launch_pass(const uint64_t* src, uint64_t* dst, uint32_t n, uint32_t shift,
 // before producing the keys and its producer added every key's digits to
 // sort_hist_counts(ws) ([pass][512]).
 uint64_t* onesweep_sort(uint64_t* buf0, uint64_t* buf1, uint32_t n, uint32_t lo_bit, SortPlan plan, void* ws,
-                        uint32_t* d_err, cudaStream_t st, bool counts_ready) {
+                        uint32_t* d_err, cudaStream_t st, bool counts_ready, uint32_t tile_keys) {
   if (n <= 1 || plan.passes == 0) return buf0;
   uint32_t* hist = (uint32_t*)ws;
   uint32_t* tickets = hist + 4 * kMaxBins;
@@ -378,11 +378,15 @@ uint64_t* onesweep_sort(uint64_t* buf0, uint64_t* buf1, uint32_t n, uint32_t lo_
     const uint32_t shift = lo_bit + plan.width * p;
     const uint32_t w = std::min(plan.width, plan.bits - plan.width * p);
     const uint32_t mask = (1u << w) - 1u;
-    if (plan.width == 9)
-      launch_pass<kPassItems, 2, 9>(src, dst, n, shift, mask, hist + p * kMaxBins, status, tickets + p, d_err, st);
-    else
-      launch_pass<kPassItems, 2, 8>(src, dst, n, shift, mask, hist + p * kMaxBins, status, tickets + p, d_err,
-                                    st);
+    // 4096-key tiles (8 per thread) are the autotuner's alternative tile shape
+    const bool t4k = tile_keys == 4096u;
+    if (plan.width == 9) {
+      if (t4k) launch_pass<8, 2, 9>(src, dst, n, shift, mask, hist + p * kMaxBins, status, tickets + p, d_err, st);
+      else launch_pass<kPassItems, 2, 9>(src, dst, n, shift, mask, hist + p * kMaxBins, status, tickets + p, d_err, st);
+    } else {
+      if (t4k) launch_pass<8, 2, 8>(src, dst, n, shift, mask, hist + p * kMaxBins, status, tickets + p, d_err, st);
+      else launch_pass<kPassItems, 2, 8>(src, dst, n, shift, mask, hist + p * kMaxBins, status, tickets + p, d_err, st);
+    }
     std::swap(src, dst);
   }
   return src;

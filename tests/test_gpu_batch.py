@@ -105,11 +105,12 @@ def test_batch_autotune_sah_and_block_shapes(gpu):
     bt = shn.Batch(scs)
     cands = np.array([0.5, 1.0, 3.0, 8.0], np.float32)
     chosen, sah, rep = bt.autotune_ex(cands, expected_rays=[100000] * 4, sample_rays=8192, sah_keep=2,
-                                      blocks_per_sm=(0, 4, 6))
+                                      blocks_per_sm=(0, 4, 6), sort_tiles=(6144, 4096))
     assert set(chosen.tolist()) <= set(cands.tolist())
     nonempty = sum(1 for sc in scs if sc.num_triangles)
     assert rep["timed_candidates"] == 2 * nonempty
     assert rep["blocks_per_sm"] in (0, 4, 6) and all(ms > 0 for ms in rep["shape_ms"])
+    assert rep["sort_tile_keys"] in (4096, 6144) and all(ms > 0 for ms in rep["sort_tile_ms"])
     # the chosen candidate is one of the two of least SAH cost, and its cost is the oracle's
     for s, sc in enumerate(scs):
         if not sc.num_triangles:
