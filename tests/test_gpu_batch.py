@@ -125,3 +125,19 @@ def test_batch_autotune_sah_and_block_shapes(gpu):
     for s, og in enumerate(_oracle_grids(scs, chosen)):
         ex = bt.export_scene(s, og.cells.shape[0], og.indices.size)
         assert np.array_equal(ex["cells"], og.cells)
+
+
+def test_batch_build_with_4096_key_sort_tiles(gpu):
+    """The autotuner's other onesweep tile shape gives the same grids."""
+    import shinobi_b200 as shn
+    scs = _scenes()
+    bt = shn.Batch(scs)
+    cands = np.array([1.5], np.float32)
+    chosen, _, rep = bt.autotune_ex(cands, expected_rays=[100000] * len(scs), sample_rays=4096,
+                                    sort_tiles=(4096,))
+    assert rep["sort_tile_keys"] == 4096
+    bt.build()
+    for s, og in enumerate(_oracle_grids(scs, chosen)):
+        ex = bt.export_scene(s, og.cells.shape[0], og.indices.size)
+        assert np.array_equal(ex["cells"], og.cells)
+        assert np.array_equal(ex["indices"], og.indices)
