@@ -288,26 +288,47 @@ class GridBuilderT {
   void rebuild(Grid& oGrid, FaceSoup& oFaceSoup, cudaStream_t aStream) {
     check(shn_grid_build(oGrid.handle(), oFaceSoup.handle(), &mParams, aStream), "grid build",
           oGrid.context().get());
-    mLast = oGrid.info();
+    mLastGrid = &oGrid;  // statistics are read when asked for (the build's last stage runs on)
   }
 
   void cleanup() {}
 
   void outputStats(std::ostream& os) const {
-    os << "Grid resolution: " << mLast.res[0] << " " << mLast.res[1] << " " << mLast.res[2] << "\n"
-       << "Number of references: " << mLast.num_refs << "\n";
-    if (KIND == SHN_GRID_TWO_LEVEL) os << "Number of leaf cells: " << mLast.num_leaves << "\n";
-    os << "Build time (ms): " << mLast.build_ms << "\n";
+    const shn_grid_info last = mLastGrid ? mLastGrid->info() : shn_grid_info{};
+    os << "Grid resolution: " << last.res[0] << " " << last.res[1] << " " << last.res[2] << "\n"
+       << "Number of references: " << last.num_refs << "\n";
+    if (KIND == SHN_GRID_TWO_LEVEL) os << "Number of leaf cells: " << last.num_leaves << "\n";
+    os << "Build time (ms): " << last.build_ms << "\n";
   }
 
- private:
+ protected:
   uint32_t mNumPrimitives = 0;
   shn_grid_params mParams;
-  shn_grid_info mLast{};
+  const Grid* mLastGrid = nullptr;
 };
 
 typedef GridBuilderT<SimpleGrid, SHN_GRID_UNIFORM> FastSimpleGridBuilder;
 typedef GridBuilderT<TwoLevelGrid, SHN_GRID_TWO_LEVEL> FastTwoLevelGridBuilder;
+
+// SAHGridBuilder (src/Control/Algorithm/SAHGridBuilder.h:38-202): the uniform
+// sort-based build at the resolution of least SAH cost in the window 0.75 ..
+// 1.25 around the lambda = 5 estimate (computeResolution), counted on the
+// device in one launch.
+class SAHGridBuilder : public GridBuilderT<SimpleGrid, SHN_GRID_UNIFORM> {
+ public:
+  // computeResolution: fixes params().res for the builds that follow.
+  shn_sah_result computeResolution(FaceSoup& oFaceSoup, cudaStream_t aStream = nullptr) {
+    shn_sah_result r{};
+    check(shn_grid_sah_resolution(oFaceSoup.handle(), 5.f, 0.75f, 1.25f, nullptr, 0, &r, aStream),
+          "SAH resolution", oFaceSoup.context().get());
+    for (int k = 0; k < 3; ++k) mParams.res[k] = r.res[k];
+    return r;
+  }
+  void build(SimpleGrid& oGrid, FaceSoup& oFaceSoup) {
+    computeResolution(oFaceSoup);
+    rebuild(oGrid, oFaceSoup, nullptr);
+  }
+};
 
 // ---- traversers (SimpleGridTraverser.h:249-469, TwoLevelGridTraverser.h:430-828) ------
 // The reference's traverser + SimpleIntersector pair, fused: closest hit for
