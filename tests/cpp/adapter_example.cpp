@@ -1,8 +1,10 @@
 // Drives the C++ adapters (include/shinobi/shinobi.hpp) the way an engine
 // written against the reference's host interface would: FWObject ->
-// FaceSoup::upload -> Fast*GridBuilder::init/build -> StaticRTEngine::renderImage
-// (DirectIlluminationIntegrator::tracePrimary + shade).  Usage:
-//   adapter_example <scene.bin> <out.bin> <kind 0|1> <res_x> <res_y>
+// FaceSoup::upload -> Fast*GridBuilder / SAHGridBuilder::init/build ->
+// StaticRTEngine::renderImage (DirectIlluminationIntegrator::tracePrimary +
+// shade).  Usage:
+//   adapter_example <scene.bin> <out.bin> <kind 0|1|2> <res_x> <res_y>
+// kind 0: uniform grid, 1: two-level grid, 2: uniform grid at the SAH resolution.
 // scene.bin: uint32 nv, uint32 nt, nv*3 float, nt*3 uint32.
 // out.bin:   res_x*res_y uint32 triangle ids, res_x*res_y float t, then the
 //            res_x*res_y*3 float direct-illumination frame.
@@ -96,6 +98,7 @@ int main(int argc, char** argv) {
   const uint32_t rx = (uint32_t)atoi(argv[4]), ry = (uint32_t)atoi(argv[5]);
   try {
     if (kind == 0) return run<shinobi::FastSimpleGridBuilder, shinobi::SimpleGrid>(obj, argv[2], rx, ry);
+    if (kind == 2) return run<shinobi::SAHGridBuilder, shinobi::SimpleGrid>(obj, argv[2], rx, ry);
     return run<shinobi::FastTwoLevelGridBuilder, shinobi::TwoLevelGrid>(obj, argv[2], rx, ry);
   } catch (const shinobi::Error& e) {
     if (e.status == SHN_ERR_CUDA) {

@@ -55,7 +55,7 @@ def test_adapter_compiles_and_fails_cleanly_without_device(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kind", [0, 1])
+@pytest.mark.parametrize("kind", [0, 1, 2])
 def test_adapter_primary_hits_match_oracle(tmp_path, gpu, kind):
     exe = _compile(tmp_path)
     sc = scenes.uniform_soup(20000, seed=7, offset_scale=0.02)
@@ -70,6 +70,8 @@ def test_adapter_primary_hits_match_oracle(tmp_path, gpu, kind):
     b = oracle.bounds(sc.vertices, sc.indices)
     if kind == 0:
         g = oracle.build_uniform(sc.vertices, sc.indices, b, oracle.resolution(sc.num_triangles, b, 5.0))
+    elif kind == 2:  # SAHGridBuilder: the resolution of least SAH cost
+        g = oracle.build_uniform(sc.vertices, sc.indices, b, oracle.sah_resolution(sc.vertices, sc.indices, b)["res"])
     else:
         g = oracle.build_two_level(sc.vertices, sc.indices, b,
                                    oracle.resolution(sc.num_triangles, b, 1.0 / 16.0, 1, 2), 4.0, 16)
