@@ -117,7 +117,7 @@ struct AoParams {
 };
 
 template <int KIND, bool STATS>
-__global__ void __launch_bounds__(kTraceBlock, 9) k_trace_ao(GridView G, AoParams A,
+__global__ void __launch_bounds__(kTraceBlock, 6) k_trace_ao(GridView G, AoParams A,
                                                           const uint32_t* __restrict__ ptri,
                                                           const float* __restrict__ pt,
                                                           const uint32_t* __restrict__ hit_idx,
@@ -218,7 +218,7 @@ SHN_D void di_segment(const DiParams& P, uint32_t p, uint32_t s, float t, V3& o,
 }
 
 template <int KIND, bool STATS>
-__global__ void __launch_bounds__(kTraceBlock, 9) k_trace_direct(GridView G, DiParams P,
+__global__ void __launch_bounds__(kTraceBlock, 6) k_trace_direct(GridView G, DiParams P,
                                                               const float* __restrict__ pt,
                                                               const uint32_t* __restrict__ hit_idx,
                                                               const uint32_t* d_m, uint32_t* counter,
