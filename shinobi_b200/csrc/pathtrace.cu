@@ -73,7 +73,7 @@ __global__ void k_pt_camera(PtView P, uint64_t g0, uint32_t count, PathRec* __re
 }
 
 template <int KIND>
-__global__ void __launch_bounds__(kPtBlock, 8) k_pt_bounce(GridView G, PtView P, PathRec* __restrict__ paths,
+__global__ void __launch_bounds__(kPtBlock, 10) k_pt_bounce(GridView G, PtView P, PathRec* __restrict__ paths,
                                                         const uint32_t* d_n, uint32_t depth,
                                                         uint32_t* counter, uint32_t* __restrict__ alive,
                                                         float4* __restrict__ slots, uint64_t g0,
