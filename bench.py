@@ -407,7 +407,7 @@ def run_shinobi(args):
             g.shade_direct(cam, hits, dip, frame=ao, final=final, num_rays=nao)
         else:
             g.trace_ao(cam, hits, AO_SPP, AO_LEN, AO_OFFSET, AO_SEED, out=ao, num_rays=nao)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")  # 256 MiB, twice the L2
 
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
 
