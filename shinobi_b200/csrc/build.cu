@@ -680,16 +680,7 @@ __global__ void k_leaf_dist(const uint2* __restrict__ cells, uint32_t C, uint2* 
   for (uint32_t li = blockIdx.x * blockDim.x + threadIdx.x; li < L; li += gridDim.x * blockDim.x) {
     uint32_t c;
     if (AXIS == 0) {
-      // the warp's leaves are consecutive and nearly always share one top
-      // cell: one search for the warp, a search per lane only past its end
-      const unsigned am = __activemask();
-      const int leader = __ffs(am) - 1;
-      uint32_t c0 = 0;
-      if ((int)(threadIdx.x & 31) == leader) c0 = leaf_owner(cells, C, li);
-      c0 = __shfl_sync(am, c0, leader);
-      const uint2 w0 = __ldg(cells + c0);
-      const uint32_t n0 = (w0.y & kNotEmpty) ? (w0.y & 0xFFu) * ((w0.y >> 8) & 0xFFu) * ((w0.y >> 16) & 0xFFu) : 0u;
-      c = (li >= w0.x && li - w0.x < n0) ? c0 : leaf_owner(cells, C, li);
+      c = leaf_owner(cells, C, li);
       owner[li] = c;
     } else {
       c = __ldg(owner + li);
