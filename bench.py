@@ -659,10 +659,13 @@ def serve_summary(sv):
 
 def launches_per_step(P, R, C0, L):
     def sort_launches(n, cells):
+        # the emission counts the digits: a digit-offset scan + one launch per
+        # 8- or 9-bit pass (whichever takes fewer passes)
         if n <= 1:
             return 0
-        passes = (max(1, (cells - 1).bit_length()) + 7) // 8
-        return 2 + passes
+        bits = max(1, (cells - 1).bit_length())
+        p8, p9 = (bits + 7) // 8, (bits + 8) // 9
+        return 1 + min(p8, p9)
     build = (2 + 1 + sort_launches(P, C0) + 1      # count + scan, emit, sort, top ranges
              + 1 + 2 + 1 + sort_launches(R, L) + 1)  # leaf cells scan, leaf count + scan, emit, sort, ranges
     # Morton order of the triangles (keys, two 4-pass sorts, second keys, permute)
