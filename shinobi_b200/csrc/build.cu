@@ -658,7 +658,7 @@ __global__ void k_super_boxes(const float4* __restrict__ box, uint32_t nblocks, 
 // passes (x, then y, then z).  An empty leaf stores [D, D): its range stays
 // empty, and a DDA that fetched it may take its next D - 1 steps without
 // fetching, since every cell within those steps lies closer than D.
-constexpr uint32_t kLeafDistCap = 15;
+constexpr uint32_t kLeafDistCap = 7;
 
 // top cell owning leaf li: the last cell whose leaf offset is <= li (offsets
 // are the exclusive scan of the leaf counts, so empty cells never match last)
