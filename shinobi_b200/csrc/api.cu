@@ -147,6 +147,41 @@ void ctx_release(shn_ctx* c) {
 }
 }  // namespace shn
 
+namespace shn {
+shn_status scene_reload(shn_scene* s, const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                        cudaStream_t st) {
+  if (!s || (nv && !vtx) || (nt && !idx)) return SHN_ERR_INVALID;
+  shn_ctx* ctx = s->ctx;
+  if (nt >= (1u << 30) || nv >= (1u << 30)) return set_error(ctx, SHN_ERR_INVALID, "scene larger than 2^30 elements");
+  shn_status rc = validate_host(ctx, vtx, nv, idx, nt);
+  if (rc) return rc;
+  struct Buf {
+    void** p;
+    size_t* cap;
+    size_t need;
+  } bufs[3] = {{(void**)&s->vtx, &s->cap_v, std::max<size_t>(12 * (size_t)nv, 16)},
+               {(void**)&s->idx, &s->cap_i, std::max<size_t>(12 * (size_t)nt, 16)},
+               {(void**)&s->tri, &s->cap_t, std::max<size_t>(48 * (size_t)nt, 16)}};
+  for (Buf& b : bufs) {
+    if (*b.cap >= b.need) continue;
+    dev_free(ctx, *b.p, *b.cap, st);
+    *b.p = nullptr;
+    *b.cap = 0;
+    const cudaError_t e = dev_alloc(ctx, b.p, b.need, st);
+    if (e != cudaSuccess) return alloc_status(ctx, e, "scene");
+    *b.cap = b.need;
+  }
+  s->nv = nv;
+  s->nt = nt;
+  s->bytes = s->cap_v + s->cap_i + s->cap_t;
+  if (nv) rc = copy_in(ctx, s->vtx, vtx, 12 * (size_t)nv, SHN_MEM_HOST, st);
+  if (!rc && nt) rc = copy_in(ctx, s->idx, idx, 12 * (size_t)nt, SHN_MEM_HOST, st);
+  if (rc) return rc;
+  launch_pack_triangles(s->vtx, s->idx, nt, s->tri, st);
+  return refresh_bounds(s, st);
+}
+}  // namespace shn
+
 extern "C" {
 
 uint32_t shn_abi_version(void) { return SHN_ABI_VERSION; }
@@ -226,12 +261,19 @@ shn_status shn_scene_create(shn_ctx* ctx, const float* vtx, uint32_t nv, const u
   const size_t bv = std::max<size_t>(12 * (size_t)nv, 16), bi = std::max<size_t>(12 * (size_t)nt, 16),
                bt = std::max<size_t>(48 * (size_t)nt, 16);
   cudaError_t e = dev_alloc(ctx, (void**)&s->vtx, bv, st);
-  if (e == cudaSuccess) e = dev_alloc(ctx, (void**)&s->idx, bi, st);
-  if (e == cudaSuccess) e = dev_alloc(ctx, (void**)&s->tri, bt, st);
+  if (e == cudaSuccess) {
+    s->cap_v = bv;
+    e = dev_alloc(ctx, (void**)&s->idx, bi, st);
+  }
+  if (e == cudaSuccess) {
+    s->cap_i = bi;
+    e = dev_alloc(ctx, (void**)&s->tri, bt, st);
+  }
   if (e != cudaSuccess) {
     shn_scene_destroy(s);
     return alloc_status(ctx, e, "scene");
   }
+  s->cap_t = bt;
   s->bytes = bv + bi + bt;
   shn_status rc = SHN_OK;
   if (nv) rc = copy_in(ctx, s->vtx, vtx, 12 * (size_t)nv, mem, st);
@@ -319,13 +361,14 @@ uint32_t shn_scene_num_triangles(const shn_scene* s) { return s ? s->nt : 0; }
 void shn_scene_destroy(shn_scene* s) {
   if (!s) return;
   cudaStream_t st = 0;
-  dev_free(s->ctx, s->vtx, std::max<size_t>(12 * (size_t)s->nv, 16), st);
-  dev_free(s->ctx, s->idx, std::max<size_t>(12 * (size_t)s->nt, 16), st);
-  dev_free(s->ctx, s->tri, std::max<size_t>(48 * (size_t)s->nt, 16), st);
+  dev_free(s->ctx, s->vtx, s->cap_v, st);
+  dev_free(s->ctx, s->idx, s->cap_i, st);
+  dev_free(s->ctx, s->tri, s->cap_t, st);
   shn_ctx* c = s->ctx;
   delete s;
   ctx_release(c);
 }
+
 
 // ---- grid --------------------------------------------------------------------------
 void shn_grid_params_default(uint32_t kind, shn_grid_params* p) {

@@ -59,6 +59,7 @@ struct shn_scene {
   const float4* ids = nullptr;
   float bounds[6] = {0, 0, 0, 0, 0, 0};
   size_t bytes = 0;
+  size_t cap_v = 0, cap_i = 0, cap_t = 0;  // allocated bytes of vtx, idx, tri
 };
 
 struct shn_grid {
@@ -115,6 +116,11 @@ void dev_free(shn_ctx* ctx, void* p, size_t bytes, cudaStream_t st);
 uint32_t* pinned_take(shn_ctx* ctx);
 void pinned_give(shn_ctx* ctx, uint32_t* p);
 void ctx_retain(shn_ctx* ctx);
+// Replaces a scene's geometry with new host arrays (checked as
+// shn_scene_create checks them), reusing its device buffers when they are
+// large enough.  On an error the scene's contents are undefined.
+shn_status scene_reload(shn_scene* s, const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                        cudaStream_t st);
 void ctx_release(shn_ctx* ctx);
 shn_status set_error(shn_ctx* ctx, shn_status s, const std::string& msg);
 shn_status cuda_status(shn_ctx* ctx, cudaError_t e, const char* where);

@@ -112,10 +112,12 @@ struct ServeSlot {
   uint32_t pending = 0;         // updates of this slot handed to the updater, not yet applied
 };
 
-// A replaced scene/grid pair, freed once every launch issued before the
-// replacement (seq <= after_seq) has completed.
+// A replaced scene/grid pair, released once every launch issued before the
+// replacement (seq <= after_seq) has completed: it becomes its slot's spare,
+// whose buffers the slot's next replacement is built into, or is freed.
 struct ServeRetired {
   ServeSlot pair;
+  uint32_t slot = 0;
   uint64_t after_seq = 0;
 };
 
@@ -141,6 +143,11 @@ struct shn_server {
   std::deque<ServeReq*> upd_q;
   bool stop_upd = false;
   std::vector<ServeRetired> retired;
+  // per slot, one released pair kept for the next replacement: rebuilding
+  // into its buffers avoids allocating and freeing gigabytes of pool memory
+  // per replacement (pool calls of that size block the host for 30-500 ms and
+  // hold up every other thread's CUDA calls meanwhile)
+  std::vector<ServeSlot> spares;
   std::vector<uint8_t> blocked;  // per slot, scratch of one queue scan
   uint64_t work_gen = 0;         // bumped when a request arrives or an update is applied
   uint32_t upd_outstanding = 0;  // updates handed to the updater and not yet applied
@@ -175,14 +182,25 @@ void complete(shn_server* s, ServeReq* r, shn_status st) {
   s->cv_done.notify_all();
 }
 
-// New scene + uniform grid for a slot, built and synchronised on st.
-shn_status build_slot(shn_server* s, const float* vtx, uint32_t nv, const uint32_t* idx, uint32_t nt,
-                      float lambda, cudaStream_t st, ServeSlot* out) {
-  shn_scene* sc = nullptr;
-  shn_status rc = shn_scene_create(s->ctx, vtx, nv, idx, nt, SHN_MEM_HOST, st, &sc);
-  if (rc) return rc;
-  shn_grid* g = nullptr;
-  shn_grid_create(s->ctx, &g);
+void free_pair(const ServeSlot& p) {
+  if (p.grid) shn_grid_destroy(p.grid);
+  if (p.scene) shn_scene_destroy(p.scene);
+}
+
+// New scene + uniform grid for a slot, built and synchronised on st, into the
+// buffers of spare (a released pair of this slot, may be empty) where they
+// are large enough.  The spare is consumed either way.
+shn_status build_slot(shn_server* s, ServeSlot spare, const float* vtx, uint32_t nv, const uint32_t* idx,
+                      uint32_t nt, float lambda, cudaStream_t st, ServeSlot* out) {
+  shn_scene* sc = spare.scene;
+  shn_status rc = sc ? scene_reload(sc, vtx, nv, idx, nt, st)
+                     : shn_scene_create(s->ctx, vtx, nv, idx, nt, SHN_MEM_HOST, st, &sc);
+  if (rc) {
+    free_pair(spare);
+    return rc;
+  }
+  shn_grid* g = spare.grid;
+  if (!g) shn_grid_create(s->ctx, &g);
   shn_grid_params p;
   shn_grid_params_default(SHN_GRID_UNIFORM, &p);
   p.lambda = lambda > 0.f ? lambda : 5.f;
@@ -203,31 +221,86 @@ shn_status build_slot(shn_server* s, const float* vtx, uint32_t nv, const uint32
   return SHN_OK;
 }
 
-void free_pair(const ServeSlot& p) {
-  if (p.grid) shn_grid_destroy(p.grid);
-  if (p.scene) shn_scene_destroy(p.scene);
+// Takes the slot's spare pair (caller holds s->mu).
+ServeSlot take_spare(shn_server* s, uint32_t slot) {
+  ServeSlot p = s->spares[slot];
+  s->spares[slot] = ServeSlot{};
+  return p;
 }
 
-// Replaces the slot's pair immediately (no launch may be using it).
+// Keeps a released pair as the slot's spare if it has none; otherwise
+// returns it to be freed (caller holds s->mu; frees after unlocking).
+void release_pair(shn_server* s, uint32_t slot, const ServeSlot& p, std::vector<ServeSlot>* dead) {
+  if (!p.scene && !p.grid) return;
+  ServeSlot& sp = s->spares[slot];
+  if (!sp.scene && !sp.grid) {
+    sp.scene = p.scene;
+    sp.grid = p.grid;
+  } else {
+    dead->push_back(p);
+  }
+}
+
+// Every spare, to be freed (caller holds s->mu): an allocation that the HBM
+// budget or the device refused is retried once without them.
+std::vector<ServeSlot> take_all_spares(shn_server* s) {
+  std::vector<ServeSlot> out;
+  for (ServeSlot& sp : s->spares)
+    if (sp.scene || sp.grid) {
+      out.push_back(sp);
+      sp = ServeSlot{};
+    }
+  return out;
+}
+
+// build_slot with the slot's spare, retried once from scratch after freeing
+// every spare when the budget or the device refused memory.
+shn_status build_slot_retry(shn_server* s, uint32_t slot, ServeSlot spare, const float* vtx, uint32_t nv,
+                            const uint32_t* idx, uint32_t nt, float lambda, cudaStream_t st, ServeSlot* out) {
+  shn_status rc = build_slot(s, spare, vtx, nv, idx, nt, lambda, st, out);
+  if (rc != SHN_ERR_BUDGET && rc != SHN_ERR_OOM) return rc;
+  std::vector<ServeSlot> all;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    all = take_all_spares(s);
+  }
+  if (all.empty()) return rc;
+  for (const ServeSlot& p : all) free_pair(p);
+  return build_slot(s, ServeSlot{}, vtx, nv, idx, nt, lambda, st, out);
+}
+
+// Replaces the slot's pair immediately (no launch may be using it); the old
+// pair becomes the slot's spare.  Caller holds s->mu.
 shn_status load_slot(shn_server* s, uint32_t slot, const float* vtx, uint32_t nv, const uint32_t* idx,
                      uint32_t nt, float lambda, cudaStream_t st) {
   ServeSlot fresh;
-  shn_status rc = build_slot(s, vtx, nv, idx, nt, lambda, st, &fresh);
+  const ServeSlot spare = take_spare(s, slot);
+  shn_status rc = build_slot(s, spare, vtx, nv, idx, nt, lambda, st, &fresh);
+  if (rc == SHN_ERR_BUDGET || rc == SHN_ERR_OOM) {
+    std::vector<ServeSlot> all = take_all_spares(s);
+    if (!all.empty()) {
+      for (const ServeSlot& p : all) free_pair(p);
+      rc = build_slot(s, ServeSlot{}, vtx, nv, idx, nt, lambda, st, &fresh);
+    }
+  }
   if (rc) return rc;
   ServeSlot old = s->slots[slot];
   s->slots[slot].scene = fresh.scene;
   s->slots[slot].grid = fresh.grid;
-  free_pair(old);
+  std::vector<ServeSlot> dead;
+  release_pair(s, slot, ServeSlot{old.scene, old.grid, 0}, &dead);
+  for (const ServeSlot& p : dead) free_pair(p);
   return SHN_OK;
 }
 
-// Retired pairs whose launches have all completed (caller holds s->mu;
-// free the returned pairs after unlocking).
+// Releases the retired pairs whose launches have all completed (caller
+// holds s->mu): spares where the slot has none, the rest returned to be
+// freed after unlocking.
 std::vector<ServeSlot> take_retired(shn_server* s) {
   std::vector<ServeSlot> out;
   size_t w = 0;
   for (size_t i = 0; i < s->retired.size(); ++i) {
-    if (s->retired[i].after_seq <= s->done_seq) out.push_back(s->retired[i].pair);
+    if (s->retired[i].after_seq <= s->done_seq) release_pair(s, s->retired[i].slot, s->retired[i].pair, &out);
     else s->retired[w++] = s->retired[i];
   }
   s->retired.resize(w);
@@ -251,15 +324,17 @@ void updater_main(shn_server* s, int index) {
     ServeReq* r = s->upd_q.front();
     s->upd_q.pop_front();
     const shn_request q = r->r;
+    const ServeSlot spare = take_spare(s, q.scene);
     lk.unlock();
     ServeSlot fresh;
-    const shn_status rc = build_slot(s, q.vtx, q.nv, q.idx, q.nt, q.lambda, ust, &fresh);
+    const shn_status rc = build_slot_retry(s, q.scene, spare, q.vtx, q.nv, q.idx, q.nt, q.lambda, ust, &fresh);
     lk.lock();
     ServeSlot& sl = s->slots[q.scene];
     if (rc == SHN_OK) {
       ServeRetired old;
       old.pair.scene = sl.scene;
       old.pair.grid = sl.grid;
+      old.slot = q.scene;
       old.after_seq = s->launch_seq;
       s->retired.push_back(old);
       sl.scene = fresh.scene;
@@ -343,9 +418,25 @@ void worker_plain(shn_server* s, std::unique_lock<std::mutex>& lk) {
     }
     if (head->r.kind == SHN_REQ_UPDATE) {
       const shn_request& q = head->r;
+      const ServeSlot spare = take_spare(s, q.scene);
       lk.unlock();
-      const shn_status rc = load_slot(s, q.scene, q.vtx, q.nv, q.idx, q.nt, q.lambda, s->update_st);
+      ServeSlot fresh;
+      const shn_status rc =
+          build_slot_retry(s, q.scene, spare, q.vtx, q.nv, q.idx, q.nt, q.lambda, s->update_st, &fresh);
       lk.lock();
+      if (rc == SHN_OK) {
+        ServeSlot& sl = s->slots[q.scene];
+        const ServeSlot old{sl.scene, sl.grid, 0};
+        sl.scene = fresh.scene;
+        sl.grid = fresh.grid;
+        std::vector<ServeSlot> dead;
+        release_pair(s, q.scene, old, &dead);
+        if (!dead.empty()) {
+          lk.unlock();
+          for (const ServeSlot& p : dead) free_pair(p);
+          lk.lock();
+        }
+      }
       s->updates_done++;
       complete(s, head, rc);
       continue;
@@ -507,6 +598,7 @@ shn_status shn_server_create(shn_ctx* ctx, const shn_server_config* cfg, shn_ser
   s->cfg = *cfg;
   s->slots.resize(cfg->num_slots);
   s->blocked.assign(cfg->num_slots, 0);
+  s->spares.resize(cfg->num_slots);
   cudaStreamCreateWithFlags(&s->update_st, cudaStreamNonBlocking);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_serve_trace, kServeBlock, 0);
@@ -698,6 +790,7 @@ void shn_server_destroy(shn_server* s) {
   for (auto& kv : s->reqs) delete kv.second;
   for (auto& r : s->retired) free_pair(r.pair);
   for (auto& sl : s->slots) free_pair(sl);
+  for (auto& sl : s->spares) free_pair(sl);
   for (int i = 0; i < 2; ++i) {
     ServeLaunch& la = s->L[i];
     dev_free(s->ctx, la.d_rays, 32 * (size_t)s->cfg.max_batch_rays, la.st);

@@ -115,6 +115,40 @@ def test_updates_are_ordered(gpu):
     srv.close()
 
 
+@pytest.mark.parametrize("coalesce", [True, False])
+def test_repeated_replacements_of_one_slot(gpu, coalesce):
+    """A slot replaced again and again, by scenes larger and smaller than the
+    one before (each replacement rebuilds into the buffers the slot released
+    last time, growing them where needed): every request sees the scene of its
+    turn, and the slot left alone keeps its own."""
+    import shinobi_b200 as shn
+    seq = [scenes.uniform_soup(n, seed=70 + i, offset_scale=0.01)
+           for i, n in enumerate([4000, 12000, 2500, 12000, 4000, 9000])]
+    other = scenes.uniform_soup(3000, seed=90, offset_scale=0.02)
+    srv = shn.Server(num_slots=2, coalesce=coalesce)
+    srv.load_scene(0, seq[0])
+    srv.load_scene(1, other)
+    rays = _rays8(6000, 21, 1e30)
+    outs = []
+    for k in range(len(seq)):
+        o = (np.zeros(6000, np.uint32), np.zeros(6000, np.float32))
+        o1 = (np.zeros(6000, np.uint32), np.zeros(6000, np.float32))
+        tk = [srv.submit(srv.ray_request(0, 0, rays, *o)), srv.submit(srv.ray_request(0, 1, rays, *o1))]
+        if k + 1 < len(seq):
+            tk.append(srv.submit(srv.update_request(0, seq[k + 1])))
+        assert all(srv.wait(t) == 0 for t in tk)
+        outs.append((k, o, o1))
+    ref_other, ref_other_t = _oracle(other, rays, 0)
+    for k, o, o1 in outs:
+        ref, ref_t = _oracle(seq[k], rays, 0)
+        assert np.array_equal(o[0], ref), k
+        assert np.array_equal(o[1].view(np.uint32), ref_t.view(np.uint32)), k
+        assert np.array_equal(o1[0], ref_other), k
+        assert np.array_equal(o1[1].view(np.uint32), ref_other_t.view(np.uint32)), k
+    assert srv.stats()["updates"] == len(seq) - 1
+    srv.close()
+
+
 def test_admission_by_memory_budget(gpu):
     import shinobi_b200 as shn
     ctx = shn.Context(0, hbm_budget_bytes=96 << 20)
