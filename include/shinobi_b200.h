@@ -493,7 +493,12 @@ shn_status shn_batch_sync_status(shn_batch* b, void* stream);
  * HBM budget, continuous batching: consecutive ray requests (any scenes,
  * closest or any hit) are packed into one launch while the previous launch
  * runs; scene updates rebuild a slot's grid after the requests queued before
- * them.  coalesce = 0 gives the plain path: one launch per request, no overlap. */
+ * them.  coalesce = 0 gives the plain path: one launch per request, no overlap.
+ * A replaced slot keeps its previous scene and grid (once no launch reads
+ * them) and builds its next replacement into their device buffers, so
+ * replacements of similar size allocate no device memory; that memory counts
+ * against the HBM budget, and an update the budget would refuse releases it
+ * and tries once more. */
 #define SHN_REQ_CLOSEST 0u
 #define SHN_REQ_ANY 1u
 #define SHN_REQ_UPDATE 2u
